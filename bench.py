@@ -1,0 +1,365 @@
+#!/usr/bin/env python
+"""Throughput of the U(1) Monte Carlo hot path: link-updates/s at 32^4.
+
+Workload (one step): one sweep of 1 Metropolis + 4 overrelaxation passes over a
+32^4 lattice at beta = 1.0 (hot start), followed by the fused plaquette
+(spatial/temporal) + Polyakov-loop measurement, FP64 reductions.  One chain per
+GPU (independent chains, no data-path collective: weak scaling).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value` is device time (CUDA events on the lattice's stream, L2 flushed
+between steps), `e2e` runs the same step through the C ABI with host buffers:
+the configuration is imported from pinned host memory (FP64 angles, the
+reference layout), swept, measured, and exported back every step.
+`--impl reference` times the reference's own FP64 CPU update
+(oracle/_ref/libu1ref.so, all host threads) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+L_DEFAULT = 32
+BETA = 1.0
+METROP, OVRN = 1, 4
+DIMS = 4
+METRIC = "link-updates/s at 32^4 (1 Metropolis + 4 OR per sweep)"
+UNIT = "link-updates/s"
+
+
+def algorithmic_bytes_per_link_update(d: int) -> int:
+    """Per (parity, mu) phase: read+write the V/2 updated links, read the V/2
+    opposite-parity mu links and all V(d-1) nu != mu links, 8 B per link:
+    8Vd + 4V bytes for V/2 link updates = 16d + 8 B per link update."""
+    return 16 * d + 8
+
+
+def workload_config(L: int) -> dict:
+    return {
+        "workload": f"U(1) Wilson 4D {L}^4 beta={BETA} hot start; step = 1 Metropolis + 4 OR sweep "
+                    "+ fused plaquette(SS/ST)+Polyakov measurement",
+        "lattice": f"{L}^4", "beta": BETA, "metrop": METROP, "ovrn": OVRN,
+        "links": "float2 (cos,sin) even/odd SoA, 8 B/link",
+        "l2": "flushed between timed steps (512 MiB device write)",
+        "rng": "Philox4x32-10 keyed by (seed, site, mu, pass)",
+    }
+
+
+def link_updates_per_step(L: int) -> int:
+    return (L ** DIMS) * DIMS * (METROP + OVRN)
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: str):
+        self.gpu = gpu
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peak() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def ncu_traffic_per_launch(L: int):
+    """DRAM bytes per k_update launch from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / f"k_update_{L}x4_traffic.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("dram_bytes_per_launch:"):
+            return float(line.split(":", 1)[1].split()[0])
+    return None
+
+
+# ------------------------------------------------------------------ CPU baselines
+def cpu_reference_rate(L: int, budget_s: float, min_sweeps: int = 1) -> dict:
+    """The reference's own FP64 CPU metropolis + overrelaxation (oracle/_ref),
+    OpenMP over all host threads, on the 32^4 workload; bounded by budget_s.
+    Falls back to the oracle port (oracle/u1_oracle.cpp) if _ref is absent."""
+    import numpy as np
+    from oracle.oracle import Oracle, Ref
+    threads = os.cpu_count() or 1
+    lat = np.random.default_rng(1).uniform(0, 2 * np.pi, (L ** 4) * 4)
+    if Ref.available():
+        ref = Ref(4, (L, L, L, L), BETA, 1.0, METROP, OVRN)
+        ref.seed_cpu(threads, 1234)
+        kind = "reference"
+
+        def sweep():
+            ref.metropolis(lat)
+            for _ in range(OVRN):
+                ref.overrelax(lat)
+    else:
+        o = Oracle(4, (L, L, L, L), BETA)
+        kind = "port"
+        state = {"p": 0}
+
+        def sweep():
+            state["p"] = o.update_philox(lat, 1234, state["p"], METROP, OVRN)
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        sweep()
+        n += 1
+        el = time.perf_counter() - t0
+        if n >= min_sweeps and el >= budget_s:
+            break
+        if el + el / n > 3 * budget_s:
+            break
+    rate = n * link_updates_per_step(L) / el
+    return {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"{n} full sweeps (1 Metropolis + 4 OR) of the {L}^4 lattice, {el:.1f} s, FP64"}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    L = args.L
+    import numpy as np
+    from oracle.oracle import Oracle, Ref
+    threads = os.cpu_count() or 1
+    lat = np.random.default_rng(1).uniform(0, 2 * np.pi, (L ** 4) * 4)
+    if Ref.available():
+        ref = Ref(4, (L, L, L, L), BETA, 1.0, METROP, OVRN)
+        ref.seed_cpu(threads, 1234)
+        kind = "reference"
+
+        def step():
+            ref.metropolis(lat)
+            for _ in range(OVRN):
+                ref.overrelax(lat)
+            ref.plaquette(lat)
+            ref.polyakov(lat)
+    else:
+        o = Oracle(4, (L, L, L, L), BETA)
+        kind = "port"
+        st = {"p": 0}
+
+        def step():
+            st["p"] = o.update_philox(lat, 1234, st["p"], METROP, OVRN)
+            o.plaquette(lat)
+            o.polyakov(lat)
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    el = time.perf_counter() - t0
+    rate = args.steps * link_updates_per_step(L) / el
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(L),
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": f"{args.steps} timed full sweeps of {L}^4 (1 Met + 4 OR) + CPU plaquette "
+                                   "and Polyakov, FP64, OpenMP"},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args) -> None:
+    import numpy as np
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    from latticeu1_b200 import Context, Lattice, Rng, launch_count
+
+    L = args.L
+    ctx = Context(local)
+    lat = Lattice(ctx, DIMS, (L, L, L, L), BETA)
+    stream = torch.cuda.Stream()
+    lat.set_stream(stream.cuda_stream)
+    rng = Rng(ctx, 1234 + 7919 * rank)
+    flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    obs = torch.zeros((args.steps + args.warmup, 6), dtype=torch.float64, device="cuda")
+    lu = link_updates_per_step(L)
+
+    with torch.cuda.stream(stream):
+        lat.hot_start(rng)
+        for w in range(args.warmup):
+            flush.zero_()
+            lat.update(rng, METROP, OVRN)
+            lat.measure_async(obs[w].data_ptr())
+        stream.synchronize()
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        props = torch.cuda.get_device_properties(local)
+        uuid = str(getattr(props, "uuid", ""))
+        clocks = ClockSampler(("GPU-" + uuid) if uuid and not uuid.startswith("GPU-") else (uuid or str(local)))
+        clocks.start()
+        n0 = launch_count()
+        t_wall = time.perf_counter()
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record(stream)
+            lat.update(rng, METROP, OVRN)
+            ev[k][1].record(stream)
+            lat.measure_async(obs[args.warmup + k].data_ptr())
+            ev[k][2].record(stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t_wall = time.perf_counter() - t_wall
+        launches = launch_count() - n0
+        clk = clocks.stop()
+    upd_ms = sum(e[0].elapsed_time(e[1]) for e in ev)
+    step_ms = sum(e[0].elapsed_time(e[2]) for e in ev)
+    tot = torch.tensor([step_ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
+    step_ms_max = float(tot.item())
+    value = world * args.steps * lu / (step_ms_max * 1e-3)
+
+    # e2e: C ABI with host buffers (configuration in pinned host memory)
+    host = torch.empty(lat.nlinks, dtype=torch.float64, pin_memory=True)
+    lat.export_angles(host.numpy())
+    e2e_steps = max(3, min(args.steps, 10))
+    with torch.cuda.stream(stream):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            lat.import_angles(host.numpy())
+            lat.update(rng, METROP, OVRN)
+            m = lat.measure()
+            lat.export_angles(host.numpy())
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = world * e2e_steps * lu / float(e2e_t.item())
+    bytes_cfg = lat.nlinks * 8
+
+    ob = obs[args.warmup:].cpu().numpy()
+    if rank == 0:
+        peak, peak_kind = measured_peak()
+        upd_launches = 2 * DIMS * (METROP + OVRN)
+        avg_launch_s = upd_ms * 1e-3 / (args.steps * upd_launches)
+        alg_bytes = algorithmic_bytes_per_link_update(DIMS) * (L ** DIMS) // 2
+        achieved = alg_bytes / avg_launch_s / 1e9
+        traffic = ncu_traffic_per_launch(L)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_config(L),
+            "roofline": {"bound": "hbm", "kernel": "k_update (one (parity,mu) phase)",
+                         "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": alg_bytes,
+                         "avg_launch_us": avg_launch_s * 1e6},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_cfg,
+                    "d2h_bytes_per_step": bytes_cfg + 48,
+                    "path": "u1_lattice_import_angles(pinned host FP64) + u1_update + u1_measure + "
+                            "u1_lattice_export_angles(pinned host FP64) per step"},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+            "wall_s_timed_region": t_wall,
+            "update_ms_per_step": upd_ms / args.steps,
+            "observables": {"plaq_ss_re": float(ob[:, 0].mean()), "plaq_st_re": float(ob[:, 2].mean()),
+                            "abs_L": float(np.abs(ob[:, 4] + 1j * ob[:, 5]).mean())},
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_reference_rate(L, args.cpu_budget)
+        print(json.dumps(line), flush=True)
+    lat.close()
+    rng.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--L", type=int, default=L_DEFAULT)
+    ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU baseline sampling")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

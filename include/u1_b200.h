@@ -1,0 +1,154 @@
+/*
+ * u1_b200.h -- C ABI of the B200 (sm_100a) U(1) lattice-gauge Monte Carlo hot path.
+ *
+ * Every entry point returns an int status (U1_OK == 0).  Handles are opaque,
+ * there is no process-global lattice state, nothing calls exit(), and every
+ * device operation runs on the stream attached to the lattice (default: the
+ * legacy stream 0).  On failure u1_last_error() returns a thread-local message.
+ *
+ * Link layout at the boundary (import/export): the reference's FP64 angle
+ * array theta[id + parity*V/2 + mu*V], id = even/odd site index
+ * (reference include/index.h:114-153, u1.cpp:99, src/update.cu:188).
+ * Internally a link is a float2 (cos theta, sin theta) stored at the same index.
+ *
+ * Geometry follows reference src/parameters.cu:146-208: N = {Nx, Ny, Nz, Nt}
+ * is given in the reference's argument order and mapped onto Grid[] the way
+ * SetupLatticeParameters does (2D: Grid = {Nx, Nt}; 3D: {Nx, Ny, Nt}).
+ */
+#ifndef U1_B200_H
+#define U1_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  U1_OK = 0,
+  U1_ERR_INVALID = -1,     /* bad argument (odd extent, null pointer, ...) */
+  U1_ERR_CUDA = -2,        /* a CUDA runtime call failed */
+  U1_ERR_UNSUPPORTED = -3, /* valid request outside what this build supports */
+  U1_ERR_NOMEM = -4,       /* device or host allocation failed */
+  U1_ERR_STATE = -5        /* object in the wrong state (e.g. replay stream exhausted) */
+};
+
+typedef struct u1_ctx u1_ctx;
+typedef struct u1_lattice u1_lattice;
+typedef struct u1_rng u1_rng;
+
+typedef struct u1_geom {
+  int dims;       /* 2, 3 or 4 (reference "dirs") */
+  int N[4];       /* Nx, Ny, Nz, Nt in the reference's argument order; unused entries ignored */
+  double beta;    /* reference "beta" */
+  double aniso;   /* reference "aniso" (xi): spatial plaquettes weighted 1/xi, temporal xi */
+} u1_geom;
+
+/* Last error message of the calling thread ("" if none). */
+const char *u1_last_error(void);
+/* Library version string. */
+const char *u1_version(void);
+
+/* Replaces Start(gpuid, ...) (reference src/cuda_error_check.cpp:24-45):
+ * selects the device; no tune-cache side effects. */
+int u1_ctx_create(int device, u1_ctx **out);
+/* Replaces Finalize (reference src/cuda_error_check.cpp:47-72) without exit(). */
+int u1_ctx_destroy(u1_ctx *ctx);
+/* Stream used by lattices created after this call (cudaStream_t as void*). */
+int u1_ctx_set_stream(u1_ctx *ctx, void *stream);
+
+/* Host-only geometry check and sizes, no device needed (reference
+ * SetupLatticeParameters' Grid/volume logic, src/parameters.cu:150-166):
+ * out[0]=V, out[1]=V/2, out[2]=V_s, out[3]=dims, out[4..7]=Grid[0..3].
+ * Odd or non-positive extents return U1_ERR_INVALID. */
+int u1_geom_validate(const u1_geom *geom, int64_t out[8]);
+
+/* Replaces SetupLatticeParameters (reference src/parameters.cu:146-208) plus
+ * new Array<double>(Device, Volume()*Dirs()) (reference u1.cpp:99): allocates
+ * a cold (theta = 0) lattice, as the reference's zero-filled dev_malloc does
+ * (reference src/alloc.cpp:193).  Odd extents return U1_ERR_INVALID
+ * (reference src/parameters.cu:164-168 exits instead). */
+int u1_lattice_create(u1_ctx *ctx, const u1_geom *geom, u1_lattice **out);
+int u1_lattice_destroy(u1_lattice *lat);
+/* Attach a stream (cudaStream_t as void*; NULL = legacy default stream). */
+int u1_lattice_set_stream(u1_lattice *lat, void *stream);
+/* Sizes: out[0]=V, out[1]=V/2, out[2]=V_s, out[3]=dims, out[4..7]=Grid[0..3]. */
+int u1_lattice_info(const u1_lattice *lat, int64_t out[8]);
+/* Change beta / aniso of an existing lattice (no reallocation). */
+int u1_lattice_set_coupling(u1_lattice *lat, double beta, double aniso);
+/* Device pointer of the float2 link array (V*dims float2). */
+int u1_lattice_links(u1_lattice *lat, void **dev_ptr);
+/* Copy all links of src into dst (same geometry). */
+int u1_lattice_copy(u1_lattice *dst, const u1_lattice *src);
+
+/* Import/export in the reference layout theta[id + p*V/2 + mu*V] (FP64).
+ * on_device != 0: the pointer is a device pointer on the lattice's device. */
+int u1_lattice_import_angles(u1_lattice *lat, const double *angles, int on_device);
+int u1_lattice_export_angles(const u1_lattice *lat, double *angles, int on_device);
+/* Cold start: every theta = 0. */
+int u1_cold_start(u1_lattice *lat);
+
+/* Counter-based RNG (Philox4x32-10).  Replaces CudaRNG(seed, V/2)
+ * (reference include/random.h:31-58, src/random.cu:28-36): the state is
+ * (seed, pass counter) only, so it is free to checkpoint and any thread or
+ * tile order draws the same numbers. */
+int u1_rng_create(u1_ctx *ctx, uint64_t seed, u1_rng **out);
+int u1_rng_destroy(u1_rng *rng);
+int u1_rng_get_state(const u1_rng *rng, uint64_t *seed, uint64_t *pass);
+int u1_rng_set_state(u1_rng *rng, uint64_t seed, uint64_t pass);
+/* Test-only shared-stream mode: Metropolis passes read (new_theta, b) pairs
+ * from `pairs` (host FP64, 2 values per link) in the reference's draw order
+ * pass -> parity -> mu -> id (reference src/update.cu:51-79, 305-308).
+ * n_pairs must be a multiple of V*dims (one pass).  NULL/0 switches back
+ * to Philox. */
+int u1_rng_set_replay(u1_rng *rng, const double *pairs, size_t n_pairs);
+/* The uniforms Philox gives link (parity, mu, id) in Metropolis pass `pass`
+ * for the lattice's geometry: out[2*id], out[2*id+1] (float, as drawn). */
+int u1_rng_debug_uniforms(u1_lattice *lat, const u1_rng *rng, uint64_t pass,
+                          int parity, int mu, float *out_host);
+
+/* Replaces HotStart (reference src/update.cu:30-48): theta uniform in
+ * [0, 2 pi) for every link, drawn from the rng (tag "hot start"). */
+int u1_hot_start(u1_lattice *lat, u1_rng *rng);
+
+/* Replaces UpdateLattice (reference src/update.cu:449-456): metrop
+ * Metropolis passes, then ovrn overrelaxation passes; each pass visits
+ * parity 0,1 and mu = 0..dims-1 in order (reference src/update.cu:305-308,
+ * 383-386).  Asynchronous on the lattice's stream. */
+int u1_update(u1_lattice *lat, u1_rng *rng, int metrop, int ovrn);
+
+/* Replaces Plaquette (reference src/plaquette.cu:222-228):
+ * out = {SS re, SS im, ST re, ST im} of mean(1 - exp(i theta_P)).  In 2D the
+ * SS mean has no plaquettes and is NaN, as in the reference. Synchronous. */
+int u1_plaquette(u1_lattice *lat, double out[4]);
+/* Replaces Polyakov (reference src/polyakov.cu:169-174): out = {re, im} of
+ * (1/V_s) sum_x exp(i sum_t theta_t(x,t)).  Synchronous. */
+int u1_polyakov(u1_lattice *lat, double out[2]);
+/* Fused plaquette + Polyakov pass: out = {SS re, SS im, ST re, ST im, L re, L im}. */
+int u1_measure(u1_lattice *lat, double out[6]);
+/* Asynchronous form: the 6 doubles land in device memory dev_out. */
+int u1_measure_async(u1_lattice *lat, double *dev_out);
+
+/* Replaces Poly2 (reference src/polyakov.cu:618-654):
+ * out[2*(r-1)], out[2*(r-1)+1] = re, im of C(r) for r = 1..R, R = Grid[0]/2,
+ * C(r) = 1/(V_s (d-1)) sum_x sum_i P(x) conj(P(x + r e_i)).  multihit != 0
+ * replaces each temporal link by its analytic multihit mean
+ * (reference include/lattice_functions.h:92-105). */
+int u1_poly_corr(u1_lattice *lat, int multihit, double *out, int out_len);
+
+/* Replaces MultiLevel (reference src/multilevel.cu:639-732).  Works on an
+ * internal copy of the lattice (the caller's links are unchanged) and
+ * advances the rng.  Requires dims == 4 and Nt % 4 == 0 (else U1_ERR_INVALID;
+ * the reference exits).  out as for u1_poly_corr. */
+int u1_multilevel(u1_lattice *lat, u1_rng *rng, int n4, int k4, int n2, int k2,
+                  int metrop, int ovrn, double *out, int out_len);
+
+/* Number of kernels this library has launched in the calling process. */
+int u1_kernel_launch_count(uint64_t *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* U1_B200_H */

@@ -1,0 +1,101 @@
+"""ctypes binding of the C ABI declared in include/u1_b200.h.
+
+The shared library is latticeu1_b200/lib/libu1b200.so, built in-tree by
+latticeu1_b200/build.py.  There is no fallback: if the library is missing
+or cannot be loaded, importing this module raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libu1b200.so"
+
+U1_OK = 0
+U1_ERR_INVALID = -1
+U1_ERR_CUDA = -2
+U1_ERR_UNSUPPORTED = -3
+U1_ERR_NOMEM = -4
+U1_ERR_STATE = -5
+
+
+class U1Error(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class u1_geom(C.Structure):
+    _fields_ = [("dims", C.c_int), ("N", C.c_int * 4), ("beta", C.c_double), ("aniso", C.c_double)]
+
+
+_vp = C.c_void_p
+_i = C.c_int
+_dp = C.POINTER(C.c_double)
+
+# name -> argtypes (all return int status unless listed in _RET)
+SIGNATURES = {
+    "u1_ctx_create": [_i, C.POINTER(_vp)],
+    "u1_ctx_destroy": [_vp],
+    "u1_ctx_set_stream": [_vp, _vp],
+    "u1_geom_validate": [C.POINTER(u1_geom), C.POINTER(C.c_int64)],
+    "u1_lattice_create": [_vp, C.POINTER(u1_geom), C.POINTER(_vp)],
+    "u1_lattice_destroy": [_vp],
+    "u1_lattice_set_stream": [_vp, _vp],
+    "u1_lattice_info": [_vp, C.POINTER(C.c_int64)],
+    "u1_lattice_set_coupling": [_vp, C.c_double, C.c_double],
+    "u1_lattice_links": [_vp, C.POINTER(_vp)],
+    "u1_lattice_copy": [_vp, _vp],
+    "u1_lattice_import_angles": [_vp, _vp, _i],
+    "u1_lattice_export_angles": [_vp, _vp, _i],
+    "u1_cold_start": [_vp],
+    "u1_rng_create": [_vp, C.c_uint64, C.POINTER(_vp)],
+    "u1_rng_destroy": [_vp],
+    "u1_rng_get_state": [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)],
+    "u1_rng_set_state": [_vp, C.c_uint64, C.c_uint64],
+    "u1_rng_set_replay": [_vp, _vp, C.c_size_t],
+    "u1_rng_debug_uniforms": [_vp, _vp, C.c_uint64, _i, _i, _vp],
+    "u1_hot_start": [_vp, _vp],
+    "u1_update": [_vp, _vp, _i, _i],
+    "u1_plaquette": [_vp, _dp],
+    "u1_polyakov": [_vp, _dp],
+    "u1_measure": [_vp, _dp],
+    "u1_measure_async": [_vp, _vp],
+    "u1_poly_corr": [_vp, _i, _dp, _i],
+    "u1_multilevel": [_vp, _vp, _i, _i, _i, _i, _i, _i, _dp, _i],
+    "u1_kernel_launch_count": [C.POINTER(C.c_uint64)],
+    "u1_last_error": [],
+    "u1_version": [],
+}
+_RET = {"u1_last_error": C.c_char_p, "u1_version": C.c_char_p}
+
+
+def load(path: Path = LIB_PATH) -> C.CDLL:
+    if not path.exists():
+        raise ImportError(
+            f"{path} is missing: build it with `python latticeu1_b200/build.py` "
+            "(the CUDA path has no CPU fallback)")
+    lib = C.CDLL(str(path))
+    for name, argtypes in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = argtypes
+        fn.restype = _RET.get(name, C.c_int)
+    return lib
+
+
+lib = load()
+
+
+def last_error() -> str:
+    return (lib.u1_last_error() or b"").decode()
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != U1_OK:
+        raise U1Error(rc, f"{what}: {last_error()}" if what else last_error())
+
+
+def launch_count() -> int:
+    v = C.c_uint64(0)
+    check(lib.u1_kernel_launch_count(C.byref(v)), "u1_kernel_launch_count")
+    return int(v.value)

@@ -1,0 +1,745 @@
+// C ABI implementation (include/u1_b200.h): context, lattice, RNG, update,
+// measurements, Polyakov correlator and multilevel orchestration.
+//
+// Host orchestration being replaced:
+//   SetupLatticeParameters  reference src/parameters.cu:146-208
+//   UpdateLattice           reference src/update.cu:449-456 (+ :301-316, :379-394)
+//   Plaquette / Polyakov    reference src/plaquette.cu:169-187,222-228; src/polyakov.cu:124-139,169-174
+//   Poly2                   reference src/polyakov.cu:618-654
+//   MultiLevel              reference src/multilevel.cu:639-732
+// Differences by design: no globals (geometry lives in the lattice handle),
+// status codes instead of exit(), explicit streams, no per-op device
+// synchronisation except where a host result is returned, and whole sweeps
+// replayed as CUDA graphs.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "u1_internal.h"
+#include "u1_multilevel.cuh"
+
+using namespace u1b;
+
+namespace u1i {
+static thread_local std::string g_err;
+std::atomic<unsigned long long> g_launches{0};
+static std::atomic<unsigned long long> g_rng_ids{1};
+
+void set_error(const std::string &msg) { g_err = msg; }
+int cuda_fail(cudaError_t e, const char *what) {
+  set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return U1_ERR_CUDA;
+}
+static int fail(int code, const std::string &msg) {
+  set_error(msg);
+  return code;
+}
+
+int ensure_scratch(u1_lattice *lat, size_t partial_doubles, size_t out_doubles) {
+  if (partial_doubles > lat->partials_cap) {
+    if (lat->partials) cudaFree(lat->partials);
+    lat->partials = nullptr;
+    lat->partials_cap = 0;
+    U1_CUDA_TRY(cudaMalloc(&lat->partials, partial_doubles * sizeof(double)));
+    lat->partials_cap = partial_doubles;
+  }
+  if (!lat->counter) {
+    U1_CUDA_TRY(cudaMalloc(&lat->counter, sizeof(unsigned int)));
+    U1_CUDA_TRY(cudaMemset(lat->counter, 0, sizeof(unsigned int)));
+  }
+  if (out_doubles > lat->d_out_cap) {
+    if (lat->d_out) cudaFree(lat->d_out);
+    if (lat->h_out) cudaFreeHost(lat->h_out);
+    lat->d_out = nullptr;
+    lat->h_out = nullptr;
+    lat->d_out_cap = lat->h_out_cap = 0;
+    U1_CUDA_TRY(cudaMalloc(&lat->d_out, out_doubles * sizeof(double)));
+    U1_CUDA_TRY(cudaMallocHost(&lat->h_out, out_doubles * sizeof(double)));
+    lat->d_out_cap = lat->h_out_cap = out_doubles;
+  }
+  return U1_OK;
+}
+
+static inline int blocks_for(long long n, int threads) { return (int)((n + threads - 1) / threads); }
+
+}  // namespace u1i
+
+using u1i::fail;
+
+extern "C" const char *u1_last_error(void) { return u1i::g_err.c_str(); }
+extern "C" const char *u1_version(void) { return "latticeu1_b200 0.1 (sm_100a)"; }
+
+extern "C" int u1_kernel_launch_count(uint64_t *out) {
+  if (!out) return fail(U1_ERR_INVALID, "u1_kernel_launch_count: null out");
+  *out = u1i::g_launches.load();
+  return U1_OK;
+}
+
+// ---------------------------------------------------------------- context
+extern "C" int u1_ctx_create(int device, u1_ctx **out) {
+  if (!out) return fail(U1_ERR_INVALID, "u1_ctx_create: null out");
+  *out = nullptr;
+  int n = 0;
+  U1_CUDA_TRY(cudaGetDeviceCount(&n));
+  if (device < 0 || device >= n)
+    return fail(U1_ERR_INVALID, "u1_ctx_create: device " + std::to_string(device) + " out of range (" +
+                                    std::to_string(n) + " devices)");
+  U1_CUDA_TRY(cudaSetDevice(device));
+  u1_ctx *ctx = new u1_ctx;
+  ctx->device = device;
+  cudaError_t e = cudaGetDeviceProperties(&ctx->prop, device);
+  if (e != cudaSuccess) {
+    delete ctx;
+    return u1i::cuda_fail(e, "cudaGetDeviceProperties");
+  }
+  if (ctx->prop.major != 10) {
+    std::string msg = std::string("u1_ctx_create: this library is built for sm_100a (B200); device is ") +
+                      ctx->prop.name + " sm_" + std::to_string(ctx->prop.major) + std::to_string(ctx->prop.minor);
+    delete ctx;
+    return fail(U1_ERR_UNSUPPORTED, msg);
+  }
+  *out = ctx;
+  return U1_OK;
+}
+
+extern "C" int u1_ctx_destroy(u1_ctx *ctx) {
+  if (!ctx) return U1_OK;
+  delete ctx;
+  return U1_OK;
+}
+
+extern "C" int u1_ctx_set_stream(u1_ctx *ctx, void *stream) {
+  if (!ctx) return fail(U1_ERR_INVALID, "u1_ctx_set_stream: null ctx");
+  ctx->stream = (cudaStream_t)stream;
+  return U1_OK;
+}
+
+// ---------------------------------------------------------------- lattice
+static int make_geom(const u1_geom *gm, GeomK &g) {
+  if (!gm) return fail(U1_ERR_INVALID, "geometry: null");
+  const int d = gm->dims;
+  if (d < 2 || d > 4) return fail(U1_ERR_INVALID, "geometry: dims must be 2, 3 or 4");
+  int Grid[4] = {1, 1, 1, 1};
+  const int Nx = gm->N[0], Ny = gm->N[1], Nz = gm->N[2], Nt = gm->N[3];
+  Grid[0] = Nx;
+  if (d == 2) Grid[1] = Nt;
+  else Grid[1] = Ny;
+  if (d == 3) Grid[2] = Nt;
+  else if (d > 3) Grid[2] = Nz;
+  if (d == 4) Grid[3] = Nt;
+  long long V = 1;
+  for (int k = 0; k < d; ++k) {
+    if (Grid[k] < 2 || (Grid[k] % 2) != 0)
+      return fail(U1_ERR_INVALID, "geometry: every extent must be even and >= 2 (got " +
+                                      std::to_string(Grid[k]) + " in direction " + std::to_string(k) + ")");
+    V *= Grid[k];
+  }
+  if (V * d > (1LL << 31)) return fail(U1_ERR_UNSUPPORTED, "geometry: V*dims exceeds 2^31 links");
+  g.dims = d;
+  g.tdir = d - 1;
+  for (int k = 0; k < 4; ++k) g.N[k] = Grid[k];
+  g.hN0 = Grid[0] / 2;
+  g.es[0] = 0;
+  g.es[1] = g.hN0;
+  g.es[2] = g.hN0 * Grid[1];
+  g.es[3] = g.hN0 * Grid[1] * Grid[2];
+  g.V = (int)V;
+  g.Vh = (int)(V / 2);
+  g.Vs = 1;
+  for (int k = 0; k < g.tdir; ++k) g.Vs *= Grid[k];
+  return U1_OK;
+}
+
+extern "C" int u1_geom_validate(const u1_geom *geom, int64_t out[8]) {
+  GeomK g{};
+  int rc = make_geom(geom, g);
+  if (rc) return rc;
+  if (!(geom->aniso > 0.0)) return fail(U1_ERR_INVALID, "geometry: aniso must be > 0");
+  if (out) {
+    out[0] = g.V;
+    out[1] = g.Vh;
+    out[2] = g.Vs;
+    out[3] = g.dims;
+    for (int k = 0; k < 4; ++k) out[4 + k] = g.N[k];
+  }
+  return U1_OK;
+}
+
+static void set_coupling(u1_lattice *lat, double beta, double aniso) {
+  lat->beta = beta;
+  lat->aniso = aniso;
+  lat->c.beta = (float)beta;
+  lat->c.w_ss = (float)(1.0 / aniso);
+  lat->c.w_st = (float)aniso;
+}
+
+static void drop_graphs(u1_lattice *lat) {
+  for (auto &kv : lat->graphs) cudaGraphExecDestroy(kv.second);
+  lat->graphs.clear();
+}
+
+extern "C" int u1_lattice_create(u1_ctx *ctx, const u1_geom *geom, u1_lattice **out) {
+  if (!ctx || !out) return fail(U1_ERR_INVALID, "u1_lattice_create: null argument");
+  *out = nullptr;
+  GeomK g{};
+  int rc = make_geom(geom, g);
+  if (rc) return rc;
+  if (!(geom->aniso > 0.0)) return fail(U1_ERR_INVALID, "u1_lattice_create: aniso must be > 0");
+  U1_CUDA_TRY(cudaSetDevice(ctx->device));
+  u1_lattice *lat = new u1_lattice;
+  lat->ctx = ctx;
+  lat->g = g;
+  set_coupling(lat, geom->beta, geom->aniso);
+  cudaError_t e = cudaStreamCreate(&lat->own_stream);
+  if (e != cudaSuccess) {
+    delete lat;
+    return u1i::cuda_fail(e, "cudaStreamCreate");
+  }
+  lat->stream = ctx->stream ? ctx->stream : lat->own_stream;
+  const size_t nl = (size_t)g.V * g.dims;
+  e = cudaMalloc(&lat->links, nl * sizeof(float2));
+  if (e != cudaSuccess) {
+    u1_lattice_destroy(lat);
+    u1i::set_error(std::string("u1_lattice_create: cudaMalloc links: ") + cudaGetErrorString(e));
+    return U1_ERR_NOMEM;
+  }
+  rc = u1_cold_start(lat);
+  if (rc) {
+    u1_lattice_destroy(lat);
+    return rc;
+  }
+  *out = lat;
+  return U1_OK;
+}
+
+extern "C" int u1_lattice_destroy(u1_lattice *lat) {
+  if (!lat) return U1_OK;
+  cudaSetDevice(lat->ctx->device);
+  cudaStreamSynchronize(lat->stream);
+  drop_graphs(lat);
+  if (lat->links) cudaFree(lat->links);
+  if (lat->partials) cudaFree(lat->partials);
+  if (lat->counter) cudaFree(lat->counter);
+  if (lat->d_out) cudaFree(lat->d_out);
+  if (lat->h_out) cudaFreeHost(lat->h_out);
+  if (lat->pfield) cudaFree(lat->pfield);
+  if (lat->stage) cudaFree(lat->stage);
+  if (lat->own_stream) cudaStreamDestroy(lat->own_stream);
+  delete lat;
+  return U1_OK;
+}
+
+extern "C" int u1_lattice_set_stream(u1_lattice *lat, void *stream) {
+  if (!lat) return fail(U1_ERR_INVALID, "u1_lattice_set_stream: null lattice");
+  lat->stream = stream ? (cudaStream_t)stream : lat->own_stream;
+  return U1_OK;
+}
+
+extern "C" int u1_lattice_info(const u1_lattice *lat, int64_t out[8]) {
+  if (!lat || !out) return fail(U1_ERR_INVALID, "u1_lattice_info: null argument");
+  out[0] = lat->g.V;
+  out[1] = lat->g.Vh;
+  out[2] = lat->g.Vs;
+  out[3] = lat->g.dims;
+  for (int k = 0; k < 4; ++k) out[4 + k] = lat->g.N[k];
+  return U1_OK;
+}
+
+extern "C" int u1_lattice_set_coupling(u1_lattice *lat, double beta, double aniso) {
+  if (!lat) return fail(U1_ERR_INVALID, "u1_lattice_set_coupling: null lattice");
+  if (!(aniso > 0.0)) return fail(U1_ERR_INVALID, "u1_lattice_set_coupling: aniso must be > 0");
+  set_coupling(lat, beta, aniso);
+  drop_graphs(lat);
+  return U1_OK;
+}
+
+extern "C" int u1_lattice_links(u1_lattice *lat, void **dev_ptr) {
+  if (!lat || !dev_ptr) return fail(U1_ERR_INVALID, "u1_lattice_links: null argument");
+  *dev_ptr = lat->links;
+  return U1_OK;
+}
+
+extern "C" int u1_lattice_copy(u1_lattice *dst, const u1_lattice *src) {
+  if (!dst || !src) return fail(U1_ERR_INVALID, "u1_lattice_copy: null argument");
+  if (memcmp(dst->g.N, src->g.N, sizeof(dst->g.N)) != 0 || dst->g.dims != src->g.dims)
+    return fail(U1_ERR_INVALID, "u1_lattice_copy: geometry mismatch");
+  U1_CUDA_TRY(cudaSetDevice(dst->ctx->device));
+  U1_CUDA_TRY(cudaMemcpyAsync(dst->links, src->links, (size_t)src->g.V * src->g.dims * sizeof(float2),
+                              cudaMemcpyDeviceToDevice, dst->stream));
+  return U1_OK;
+}
+
+extern "C" int u1_cold_start(u1_lattice *lat) {
+  if (!lat) return fail(U1_ERR_INVALID, "u1_cold_start: null lattice");
+  U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
+  const size_t n = (size_t)lat->g.V * lat->g.dims;
+  k_fill_links<<<u1i::blocks_for((long long)n, 256), 256, 0, lat->stream>>>(lat->links, n,
+                                                                            make_float2(1.f, 0.f));
+  U1_LAUNCH_CHECK("k_fill_links");
+  return U1_OK;
+}
+
+static int ensure_stage(u1_lattice *lat) {
+  if (!lat->stage) U1_CUDA_TRY(cudaMalloc(&lat->stage, (size_t)lat->g.V * lat->g.dims * sizeof(double)));
+  return U1_OK;
+}
+
+extern "C" int u1_lattice_import_angles(u1_lattice *lat, const double *angles, int on_device) {
+  if (!lat || !angles) return fail(U1_ERR_INVALID, "u1_lattice_import_angles: null argument");
+  U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
+  const size_t n = (size_t)lat->g.V * lat->g.dims;
+  const double *src = angles;
+  if (!on_device) {
+    int rc = ensure_stage(lat);
+    if (rc) return rc;
+    U1_CUDA_TRY(cudaMemcpyAsync(lat->stage, angles, n * sizeof(double), cudaMemcpyHostToDevice, lat->stream));
+    src = lat->stage;
+  }
+  k_import_angles<<<u1i::blocks_for((long long)n, 256), 256, 0, lat->stream>>>(lat->links, src, n);
+  U1_LAUNCH_CHECK("k_import_angles");
+  U1_CUDA_TRY(cudaStreamSynchronize(lat->stream));
+  return U1_OK;
+}
+
+extern "C" int u1_lattice_export_angles(const u1_lattice *clat, double *angles, int on_device) {
+  if (!clat || !angles) return fail(U1_ERR_INVALID, "u1_lattice_export_angles: null argument");
+  u1_lattice *lat = const_cast<u1_lattice *>(clat);  // the staging buffer is a cache
+  U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
+  const size_t n = (size_t)lat->g.V * lat->g.dims;
+  double *dst = angles;
+  if (!on_device) {
+    int rc = ensure_stage(lat);
+    if (rc) return rc;
+    dst = lat->stage;
+  }
+  k_export_angles<<<u1i::blocks_for((long long)n, 256), 256, 0, lat->stream>>>(lat->links, dst, n);
+  U1_LAUNCH_CHECK("k_export_angles");
+  if (!on_device)
+    U1_CUDA_TRY(cudaMemcpyAsync(angles, lat->stage, n * sizeof(double), cudaMemcpyDeviceToHost, lat->stream));
+  U1_CUDA_TRY(cudaStreamSynchronize(lat->stream));
+  return U1_OK;
+}
+
+// ---------------------------------------------------------------- rng
+extern "C" int u1_rng_create(u1_ctx *ctx, uint64_t seed, u1_rng **out) {
+  if (!ctx || !out) return fail(U1_ERR_INVALID, "u1_rng_create: null argument");
+  *out = nullptr;
+  U1_CUDA_TRY(cudaSetDevice(ctx->device));
+  u1_rng *r = new u1_rng;
+  r->ctx = ctx;
+  r->seed = seed;
+  r->pass = 0;
+  r->chain = 0;
+  r->id = u1i::g_rng_ids.fetch_add(1);
+  cudaError_t e = cudaMalloc(&r->pass_dev, sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemset(r->pass_dev, 0, sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    if (r->pass_dev) cudaFree(r->pass_dev);
+    delete r;
+    return u1i::cuda_fail(e, "u1_rng_create");
+  }
+  *out = r;
+  return U1_OK;
+}
+
+extern "C" int u1_rng_destroy(u1_rng *rng) {
+  if (!rng) return U1_OK;
+  cudaSetDevice(rng->ctx->device);
+  cudaDeviceSynchronize();
+  if (rng->pass_dev) cudaFree(rng->pass_dev);
+  if (rng->replay_dev) cudaFree(rng->replay_dev);
+  delete rng;
+  return U1_OK;
+}
+
+extern "C" int u1_rng_get_state(const u1_rng *rng, uint64_t *seed, uint64_t *pass) {
+  if (!rng) return fail(U1_ERR_INVALID, "u1_rng_get_state: null rng");
+  if (seed) *seed = rng->seed;
+  if (pass) *pass = rng->pass;
+  return U1_OK;
+}
+
+extern "C" int u1_rng_set_state(u1_rng *rng, uint64_t seed, uint64_t pass) {
+  if (!rng) return fail(U1_ERR_INVALID, "u1_rng_set_state: null rng");
+  U1_CUDA_TRY(cudaSetDevice(rng->ctx->device));
+  U1_CUDA_TRY(cudaDeviceSynchronize());
+  unsigned long long v = pass;
+  U1_CUDA_TRY(cudaMemcpy(rng->pass_dev, &v, sizeof(v), cudaMemcpyHostToDevice));
+  rng->seed = seed;
+  rng->pass = pass;
+  return U1_OK;
+}
+
+extern "C" int u1_rng_set_replay(u1_rng *rng, const double *pairs, size_t n_pairs) {
+  if (!rng) return fail(U1_ERR_INVALID, "u1_rng_set_replay: null rng");
+  U1_CUDA_TRY(cudaSetDevice(rng->ctx->device));
+  U1_CUDA_TRY(cudaDeviceSynchronize());
+  if (rng->replay_dev) cudaFree(rng->replay_dev);
+  rng->replay_dev = nullptr;
+  rng->replay_pairs = 0;
+  if (!pairs || n_pairs == 0) return U1_OK;
+  U1_CUDA_TRY(cudaMalloc(&rng->replay_dev, n_pairs * 2 * sizeof(double)));
+  U1_CUDA_TRY(cudaMemcpy(rng->replay_dev, pairs, n_pairs * 2 * sizeof(double), cudaMemcpyHostToDevice));
+  rng->replay_pairs = n_pairs;
+  rng->replay_base = rng->pass;
+  return U1_OK;
+}
+
+extern "C" int u1_rng_debug_uniforms(u1_lattice *lat, const u1_rng *rng, uint64_t pass, int parity,
+                                     int mu, float *out_host) {
+  if (!lat || !rng || !out_host) return fail(U1_ERR_INVALID, "u1_rng_debug_uniforms: null argument");
+  if (parity < 0 || parity > 1 || mu < 0 || mu >= lat->g.dims)
+    return fail(U1_ERR_INVALID, "u1_rng_debug_uniforms: bad parity/mu");
+  U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
+  float *d = nullptr;
+  U1_CUDA_TRY(cudaMalloc(&d, (size_t)lat->g.Vh * 2 * sizeof(float)));
+  k_rng_debug<<<u1i::blocks_for(lat->g.Vh, 256), 256, 0, lat->stream>>>(
+      d, lat->g.Vh, parity, mu, (uint32_t)rng->seed, (uint32_t)(rng->seed >> 32), rng->chain, pass);
+  u1i::g_launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out_host, d, (size_t)lat->g.Vh * 2 * sizeof(float), cudaMemcpyDeviceToHost, lat->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(lat->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return u1i::cuda_fail(e, "k_rng_debug");
+  return U1_OK;
+}
+
+// ---------------------------------------------------------------- updates
+template <int D>
+static int launch_hot(u1_lattice *lat, u1_rng *rng) {
+  k_hot_start<D><<<u1i::blocks_for(lat->g.Vh, 256), 256, 0, lat->stream>>>(
+      lat->links, lat->g, (uint32_t)rng->seed, (uint32_t)(rng->seed >> 32), rng->chain, rng->pass);
+  U1_LAUNCH_CHECK("k_hot_start");
+  k_pass_add<<<1, 1, 0, lat->stream>>>(rng->pass_dev, 1ull);
+  U1_LAUNCH_CHECK("k_pass_add");
+  return U1_OK;
+}
+
+extern "C" int u1_hot_start(u1_lattice *lat, u1_rng *rng) {
+  if (!lat || !rng) return fail(U1_ERR_INVALID, "u1_hot_start: null argument");
+  U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
+  int rc;
+  switch (lat->g.dims) {
+    case 2: rc = launch_hot<2>(lat, rng); break;
+    case 3: rc = launch_hot<3>(lat, rng); break;
+    default: rc = launch_hot<4>(lat, rng); break;
+  }
+  if (rc) return rc;
+  rng->pass += 1;
+  return U1_OK;
+}
+
+template <int D>
+static int launch_phase(const UpdArgs &a, cudaStream_t s, bool met, bool replay) {
+  const int blocks = u1i::blocks_for(a.g.Vh, 256);
+  if (met) {
+    if (replay)
+      k_update<D, true, true><<<blocks, 256, 0, s>>>(a);
+    else
+      k_update<D, true, false><<<blocks, 256, 0, s>>>(a);
+  } else {
+    k_update<D, false, false><<<blocks, 256, 0, s>>>(a);
+  }
+  U1_LAUNCH_CHECK("k_update");
+  return U1_OK;
+}
+
+// Issue one sweep (metrop Metropolis + ovrn overrelaxation passes) on links
+// `links` with freeze period ml.  The device pass counter advances by metrop.
+static int issue_sweep(u1_lattice *lat, float2 *links, u1_rng *rng, int metrop, int ovrn, int ml) {
+  UpdArgs a{};
+  a.lat = links;
+  a.g = lat->g;
+  a.c = lat->c;
+  a.key0 = (uint32_t)rng->seed;
+  a.key1 = (uint32_t)(rng->seed >> 32);
+  a.chain = rng->chain;
+  a.pass_dev = rng->pass_dev;
+  a.replay = rng->replay_dev;
+  a.replay_base = rng->replay_base;
+  a.ml = ml;
+  const bool replay = rng->replay_dev != nullptr;
+  const int D = lat->g.dims;
+  for (int m = 0; m < metrop; ++m)
+    for (int p = 0; p < 2; ++p)
+      for (int mu = 0; mu < D; ++mu) {
+        a.p = p;
+        a.mu = mu;
+        a.hit = m;
+        int rc = D == 2 ? launch_phase<2>(a, lat->stream, true, replay)
+                        : D == 3 ? launch_phase<3>(a, lat->stream, true, replay)
+                                 : launch_phase<4>(a, lat->stream, true, replay);
+        if (rc) return rc;
+      }
+  bool bumped = (metrop == 0);
+  for (int o = 0; o < ovrn; ++o)
+    for (int p = 0; p < 2; ++p)
+      for (int mu = 0; mu < D; ++mu) {
+        a.p = p;
+        a.mu = mu;
+        a.hit = 0;
+        a.bump_ptr = bumped ? nullptr : rng->pass_dev;
+        a.bump_by = (unsigned)metrop;
+        bumped = true;
+        int rc = D == 2 ? launch_phase<2>(a, lat->stream, false, false)
+                        : D == 3 ? launch_phase<3>(a, lat->stream, false, false)
+                                 : launch_phase<4>(a, lat->stream, false, false);
+        if (rc) return rc;
+      }
+  if (!bumped) {
+    k_pass_add<<<1, 1, 0, lat->stream>>>(rng->pass_dev, (unsigned long long)metrop);
+    U1_LAUNCH_CHECK("k_pass_add");
+  }
+  return U1_OK;
+}
+
+static int check_replay(const u1_lattice *lat, const u1_rng *rng, int metrop) {
+  if (!rng->replay_dev) return U1_OK;
+  const size_t per_pass = (size_t)lat->g.V * lat->g.dims;
+  if (rng->replay_pairs % per_pass != 0)
+    return fail(U1_ERR_INVALID, "replay stream length is not a multiple of V*dims pairs");
+  const uint64_t avail = rng->replay_pairs / per_pass;
+  if (rng->pass < rng->replay_base || rng->pass + (uint64_t)metrop - rng->replay_base > avail)
+    return fail(U1_ERR_STATE, "replay stream exhausted");
+  return U1_OK;
+}
+
+// Capture `fn` (which issues work on lat->stream) into an executable graph.
+template <class F>
+static int capture_graph(u1_lattice *lat, F fn, cudaGraphExec_t *exec) {
+  cudaGraph_t graph = nullptr;
+  U1_CUDA_TRY(cudaStreamBeginCapture(lat->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = fn();
+  cudaError_t e = cudaStreamEndCapture(lat->stream, &graph);
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (e != cudaSuccess) return u1i::cuda_fail(e, "cudaStreamEndCapture");
+  e = cudaGraphInstantiate(exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return u1i::cuda_fail(e, "cudaGraphInstantiate");
+  return U1_OK;
+}
+
+extern "C" int u1_update(u1_lattice *lat, u1_rng *rng, int metrop, int ovrn) {
+  if (!lat || !rng) return fail(U1_ERR_INVALID, "u1_update: null argument");
+  if (metrop < 0 || ovrn < 0) return fail(U1_ERR_INVALID, "u1_update: negative pass count");
+  if (metrop == 0 && ovrn == 0) return U1_OK;
+  U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
+  int rc = check_replay(lat, rng, metrop);
+  if (rc) return rc;
+  const bool replay = rng->replay_dev != nullptr;
+  if (lat->use_graphs && !replay) {
+    auto key = std::make_tuple(metrop, ovrn, rng->id, rng->seed);
+    auto it = lat->graphs.find(key);
+    if (it == lat->graphs.end()) {
+      cudaGraphExec_t ex = nullptr;
+      rc = capture_graph(lat, [&]() { return issue_sweep(lat, lat->links, rng, metrop, ovrn, 0); }, &ex);
+      if (rc) return rc;
+      it = lat->graphs.emplace(key, ex).first;
+    }
+    U1_CUDA_TRY(cudaGraphLaunch(it->second, lat->stream));
+    u1i::g_launches += (unsigned long long)(2 * lat->g.dims * (metrop + ovrn) + (ovrn == 0 ? 1 : 0));
+  } else {
+    rc = issue_sweep(lat, lat->links, rng, metrop, ovrn, 0);
+    if (rc) return rc;
+  }
+  rng->pass += (uint64_t)metrop;
+  return U1_OK;
+}
+
+// ---------------------------------------------------------------- measurements
+template <int D>
+static int launch_measure(u1_lattice *lat, double *dev_out) {
+  const GeomK &g = lat->g;
+  const int nb = u1i::blocks_for(g.Vh, kRedThreads);
+  int rc = u1i::ensure_scratch(lat, (size_t)nb * 6, 8);
+  if (rc) return rc;
+  int nSS = 0, nST = 0;
+  for (int mu = 0; mu < D - 1; ++mu)
+    for (int nu = mu + 1; nu < D; ++nu) (nu == g.tdir ? nST : nSS)++;
+  const double normSS = 1.0 / ((double)g.V * nSS);
+  const double normST = 1.0 / ((double)g.V * nST);
+  const double normL = 1.0 / (double)g.Vs;
+  k_measure<D><<<nb, kRedThreads, 0, lat->stream>>>(lat->links, g, lat->partials, lat->counter,
+                                                   dev_out ? dev_out : lat->d_out, normSS, normST, normL);
+  U1_LAUNCH_CHECK("k_measure");
+  return U1_OK;
+}
+
+static int measure_dispatch(u1_lattice *lat, double *dev_out) {
+  switch (lat->g.dims) {
+    case 2: return launch_measure<2>(lat, dev_out);
+    case 3: return launch_measure<3>(lat, dev_out);
+    default: return launch_measure<4>(lat, dev_out);
+  }
+}
+
+extern "C" int u1_measure_async(u1_lattice *lat, double *dev_out) {
+  if (!lat || !dev_out) return fail(U1_ERR_INVALID, "u1_measure_async: null argument");
+  U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
+  return measure_dispatch(lat, dev_out);
+}
+
+extern "C" int u1_measure(u1_lattice *lat, double out[6]) {
+  if (!lat || !out) return fail(U1_ERR_INVALID, "u1_measure: null argument");
+  U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
+  int rc = u1i::ensure_scratch(lat, 0, 8);
+  if (rc) return rc;
+  rc = measure_dispatch(lat, nullptr);
+  if (rc) return rc;
+  U1_CUDA_TRY(cudaMemcpyAsync(lat->h_out, lat->d_out, 6 * sizeof(double), cudaMemcpyDeviceToHost, lat->stream));
+  U1_CUDA_TRY(cudaStreamSynchronize(lat->stream));
+  memcpy(out, lat->h_out, 6 * sizeof(double));
+  return U1_OK;
+}
+
+extern "C" int u1_plaquette(u1_lattice *lat, double out[4]) {
+  if (!out) return fail(U1_ERR_INVALID, "u1_plaquette: null out");
+  double m[6];
+  int rc = u1_measure(lat, m);
+  if (rc) return rc;
+  memcpy(out, m, 4 * sizeof(double));
+  return U1_OK;
+}
+
+extern "C" int u1_polyakov(u1_lattice *lat, double out[2]) {
+  if (!out) return fail(U1_ERR_INVALID, "u1_polyakov: null out");
+  double m[6];
+  int rc = u1_measure(lat, m);
+  if (rc) return rc;
+  out[0] = m[4];
+  out[1] = m[5];
+  return U1_OK;
+}
+
+template <int D>
+static int launch_poly_field(u1_lattice *lat, const float2 *links, int multihit) {
+  const int nb = u1i::blocks_for(lat->g.Vs, 256);
+  if (multihit)
+    k_poly_field<D, true><<<nb, 256, 0, lat->stream>>>(links, lat->g, lat->c, lat->pfield);
+  else
+    k_poly_field<D, false><<<nb, 256, 0, lat->stream>>>(links, lat->g, lat->c, lat->pfield);
+  U1_LAUNCH_CHECK("k_poly_field");
+  return U1_OK;
+}
+
+extern "C" int u1_poly_corr(u1_lattice *lat, int multihit, double *out, int out_len) {
+  if (!lat || !out) return fail(U1_ERR_INVALID, "u1_poly_corr: null argument");
+  const int R = lat->g.N[0] / 2;
+  if (out_len < 2 * R) return fail(U1_ERR_INVALID, "u1_poly_corr: out_len < 2*R (R = Grid[0]/2)");
+  U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
+  if (!lat->pfield) U1_CUDA_TRY(cudaMalloc(&lat->pfield, (size_t)lat->g.Vs * sizeof(double2)));
+  const int nb = u1i::blocks_for(lat->g.Vs, kRedThreads);
+  int rc = u1i::ensure_scratch(lat, (size_t)nb * 2 * R, (size_t)2 * R);
+  if (rc) return rc;
+  switch (lat->g.dims) {
+    case 2: rc = launch_poly_field<2>(lat, lat->links, multihit); break;
+    case 3: rc = launch_poly_field<3>(lat, lat->links, multihit); break;
+    default: rc = launch_poly_field<4>(lat, lat->links, multihit); break;
+  }
+  if (rc) return rc;
+  const double norm = 1.0 / ((double)lat->g.Vs * lat->g.tdir);
+  k_poly_corr<<<nb, kRedThreads, 0, lat->stream>>>(lat->pfield, lat->g, R, lat->partials, lat->counter,
+                                                   lat->d_out, norm);
+  U1_LAUNCH_CHECK("k_poly_corr");
+  U1_CUDA_TRY(cudaMemcpyAsync(lat->h_out, lat->d_out, (size_t)2 * R * sizeof(double), cudaMemcpyDeviceToHost,
+                              lat->stream));
+  U1_CUDA_TRY(cudaStreamSynchronize(lat->stream));
+  memcpy(out, lat->h_out, (size_t)2 * R * sizeof(double));
+  return U1_OK;
+}
+
+// ---------------------------------------------------------------- multilevel
+extern "C" int u1_multilevel(u1_lattice *lat, u1_rng *rng, int n4, int k4, int n2, int k2, int metrop,
+                             int ovrn, double *out, int out_len) {
+  if (!lat || !rng || !out) return fail(U1_ERR_INVALID, "u1_multilevel: null argument");
+  const GeomK &g = lat->g;
+  if (g.dims != 4) return fail(U1_ERR_INVALID, "u1_multilevel: requires a 4D lattice");
+  if (g.N[g.tdir] % 4 != 0)
+    return fail(U1_ERR_INVALID, "u1_multilevel: Nt is not a multiple of 4 (reference src/multilevel.cu:641)");
+  if (n4 < 1 || n2 < 1 || k4 < 0 || k2 < 0 || metrop < 0 || ovrn < 0)
+    return fail(U1_ERR_INVALID, "u1_multilevel: bad iteration counts");
+  const int R = g.N[0] / 2;
+  if (out_len < 2 * R) return fail(U1_ERR_INVALID, "u1_multilevel: out_len < 2*R");
+  U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
+  const size_t size = (size_t)g.Vs * R * g.tdir;
+  const int nl2 = g.N[g.tdir] / 2, nl4 = g.N[g.tdir] / 4;
+  float2 *work = nullptr, *mh = nullptr;
+  double2 *T2 = nullptr, *T4 = nullptr;
+  int rc = U1_OK;
+  auto cleanup = [&]() {
+    cudaStreamSynchronize(lat->stream);
+    if (work) cudaFree(work);
+    if (mh) cudaFree(mh);
+    if (T2) cudaFree(T2);
+    if (T4) cudaFree(T4);
+  };
+  cudaError_t e = cudaMalloc(&work, (size_t)g.V * g.dims * sizeof(float2));
+  if (e == cudaSuccess) e = cudaMalloc(&mh, (size_t)g.V * sizeof(float2));
+  if (e == cudaSuccess) e = cudaMalloc(&T2, size * nl2 * sizeof(double2));
+  if (e == cudaSuccess) e = cudaMalloc(&T4, size * nl4 * sizeof(double2));
+  if (e != cudaSuccess) {
+    cleanup();
+    u1i::set_error(std::string("u1_multilevel: allocation failed: ") + cudaGetErrorString(e));
+    return U1_ERR_NOMEM;
+  }
+  const int nb_ps = u1i::blocks_for((long long)size, 256);
+  const int nb_s = u1i::blocks_for(g.Vs, kRedThreads);
+  rc = u1i::ensure_scratch(lat, (size_t)nb_s * 2 * R, (size_t)2 * R);
+  if (rc) {
+    cleanup();
+    return rc;
+  }
+  auto body = [&]() -> int {
+    U1_CUDA_TRY(cudaMemcpyAsync(work, lat->links, (size_t)g.V * g.dims * sizeof(float2),
+                                cudaMemcpyDeviceToDevice, lat->stream));
+    U1_CUDA_TRY(cudaMemsetAsync(T4, 0, size * nl4 * sizeof(double2), lat->stream));
+    for (int i = 0; i < n4; ++i) {
+      for (int j = 0; j < k4; ++j) {
+        int r = issue_sweep(lat, work, rng, metrop, ovrn, 4);
+        if (r) return r;
+        rng->pass += (uint64_t)metrop;
+      }
+      U1_CUDA_TRY(cudaMemsetAsync(T2, 0, size * nl2 * sizeof(double2), lat->stream));
+      for (int k = 0; k < n2; ++k) {
+        for (int l = 0; l < k2; ++l) {
+          int r = issue_sweep(lat, work, rng, metrop, ovrn, 2);
+          if (r) return r;
+          rng->pass += (uint64_t)metrop;
+        }
+        k_ml_mhit_field<4><<<u1i::blocks_for(g.V, 256), 256, 0, lat->stream>>>(work, g, lat->c, mh);
+        U1_LAUNCH_CHECK("k_ml_mhit_field");
+        k_ml_T2<<<nb_ps, 256, 0, lat->stream>>>(mh, g, R, T2);
+        U1_LAUNCH_CHECK("k_ml_T2");
+      }
+      k_ml_T4<<<nb_ps, 256, 0, lat->stream>>>(T2, g, R, 1.0 / (double)n2, T4);
+      U1_LAUNCH_CHECK("k_ml_T4");
+    }
+    k_ml_final<<<nb_s, kRedThreads, 0, lat->stream>>>(T4, g, R, 1.0 / (double)n4, lat->partials, lat->counter,
+                                                      lat->d_out, 1.0 / ((double)g.Vs * g.tdir));
+    U1_LAUNCH_CHECK("k_ml_final");
+    U1_CUDA_TRY(cudaMemcpyAsync(lat->h_out, lat->d_out, (size_t)2 * R * sizeof(double),
+                                cudaMemcpyDeviceToHost, lat->stream));
+    U1_CUDA_TRY(cudaStreamSynchronize(lat->stream));
+    return U1_OK;
+  };
+  if (rng->replay_dev) {
+    uint64_t need = (uint64_t)metrop * ((uint64_t)n4 * k4 + (uint64_t)n4 * n2 * k2);
+    rc = check_replay(lat, rng, (int)need);
+    if (rc) {
+      cleanup();
+      return rc;
+    }
+  }
+  rc = body();
+  cleanup();
+  if (rc) return rc;
+  memcpy(out, lat->h_out, (size_t)2 * R * sizeof(double));
+  return U1_OK;
+}

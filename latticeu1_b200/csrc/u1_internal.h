@@ -1,0 +1,72 @@
+// Host-side object layout behind the C ABI (include/u1_b200.h).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <map>
+#include <string>
+#include <tuple>
+
+#include "u1_b200.h"
+#include "u1_geom.cuh"
+
+struct u1_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaDeviceProp prop{};
+};
+
+struct u1_rng {
+  u1_ctx *ctx = nullptr;
+  uint64_t seed = 0;
+  uint64_t pass = 0;                        // host mirror of *pass_dev
+  unsigned long long *pass_dev = nullptr;   // device pass counter
+  double *replay_dev = nullptr;             // shared-stream pairs (test mode)
+  size_t replay_pairs = 0;
+  uint64_t replay_base = 0;                 // pass number of the first replay pass
+  uint32_t chain = 0;
+  uint64_t id = 0;                          // unique per rng object (graph cache key)
+};
+
+struct u1_lattice {
+  u1_ctx *ctx = nullptr;
+  cudaStream_t stream = nullptr;
+  u1b::GeomK g{};
+  u1b::CoupK c{};
+  double beta = 0.0, aniso = 1.0;
+  float2 *links = nullptr;          // V*dims
+  // scratch for reductions: per-block partials + ticket counter
+  double *partials = nullptr;
+  size_t partials_cap = 0;          // doubles
+  unsigned int *counter = nullptr;
+  double *d_out = nullptr;          // small device result buffer
+  size_t d_out_cap = 0;
+  double *h_out = nullptr;          // pinned host result buffer
+  size_t h_out_cap = 0;
+  double2 *pfield = nullptr;        // Polyakov-loop field (V_s)
+  double *stage = nullptr;          // FP64 angle staging buffer for host import/export (V*dims)
+  cudaStream_t own_stream = nullptr; // used when no stream is attached
+  // cached CUDA graphs of whole sweeps, keyed by (metrop, ovrn, rng id, seed)
+  std::map<std::tuple<int, int, uint64_t, uint64_t>, cudaGraphExec_t> graphs;
+  bool use_graphs = true;
+};
+
+namespace u1i {
+void set_error(const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+extern std::atomic<unsigned long long> g_launches;
+int ensure_scratch(u1_lattice *lat, size_t partial_doubles, size_t out_doubles);
+}  // namespace u1i
+
+#define U1_CUDA_TRY(call)                                            \
+  do {                                                               \
+    cudaError_t _e = (call);                                         \
+    if (_e != cudaSuccess) return u1i::cuda_fail(_e, #call);         \
+  } while (0)
+
+#define U1_LAUNCH_CHECK(what)                                        \
+  do {                                                               \
+    u1i::g_launches.fetch_add(1, std::memory_order_relaxed);         \
+    cudaError_t _e = cudaGetLastError();                             \
+    if (_e != cudaSuccess) return u1i::cuda_fail(_e, what);          \
+  } while (0)

@@ -1,0 +1,198 @@
+// Checkerboard link update kernels (one launch per (parity, mu) phase).
+//
+// Reference algorithm being replaced:
+//   staple            include/staple.h:79-102 (anisotropic weights 1/xi, xi)
+//   Metropolis        include/lattice_functions.h:68-80, src/update.cu:177-190
+//   overrelaxation    include/lattice_functions.h:83-89, src/update.cu:227-231
+//   multilevel freeze src/multilevel.cu:41 and :141
+// Links are float2 (cos theta, sin theta); the staple is a sum of complex
+// products, Metropolis compares exp(beta*Re(S*(U'-U))) with b (the
+// reference's exp(beta*|S|*(cos(theta'+argS)-cos(theta+argS))) > b), and the
+// overrelaxation reflection theta' = -theta - 2 arg S becomes
+// U' = (conj S / |S|)^2 * conj U, with no transcendental call.
+#pragma once
+#include "u1_cplx.cuh"
+#include "u1_geom.cuh"
+#include "u1_philox.h"
+
+namespace u1b {
+
+__device__ __forceinline__ float2 ldg2(const float2 *p) { return __ldg(p); }
+
+// Staple S of link (x, mu), x of parity p with EO index i_self, so that the
+// local action of the link is beta * Re(S * U_mu(x)).
+template <int D>
+__device__ __forceinline__ float2 staple_at(const float2 *__restrict__ lat, const GeomK &g,
+                                            const CoupK &c, const int x[4], int i_self, int p,
+                                            int mu) {
+  const int q = 1 - p;
+  const size_t offP = (size_t)p * g.Vh, offQ = (size_t)q * g.Vh;
+  const size_t Vmu = (size_t)mu * g.V;
+  int xm[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) xm[k] = (k == mu) ? wrap_inc(x[k], g.N[k]) : x[k];
+  const int i_xm = eo_index(g, xm);  // x + mu, parity q
+  float2 ss = make_float2(0.f, 0.f), st = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int nu = 0; nu < D; ++nu) {
+    if (nu == mu) continue;
+    const size_t Vnu = (size_t)nu * g.V;
+    int xn[4], xd[4], xmd[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      xn[k] = (k == nu) ? wrap_inc(x[k], g.N[k]) : x[k];
+      xd[k] = (k == nu) ? wrap_dec(x[k], g.N[k]) : x[k];
+      xmd[k] = (k == nu) ? wrap_dec(xm[k], g.N[k]) : xm[k];
+    }
+    const int i_xn = eo_index(g, xn);    // x + nu       parity q
+    const int i_xd = eo_index(g, xd);    // x - nu       parity q
+    const int i_xmd = eo_index(g, xmd);  // x + mu - nu  parity p
+    // upper: U_nu(x+mu) conj(U_mu(x+nu)) conj(U_nu(x))
+    float2 a = ldg2(lat + Vnu + offQ + i_xm);
+    float2 b = ldg2(lat + Vmu + offQ + i_xn);
+    float2 cc = ldg2(lat + Vnu + offP + i_self);
+    float2 up = cmulc(cmulc(a, b), cc);
+    // lower: conj(U_nu(x+mu-nu)) conj(U_mu(x-nu)) U_nu(x-nu)
+    float2 d = ldg2(lat + Vnu + offP + i_xmd);
+    float2 e = ldg2(lat + Vmu + offQ + i_xd);
+    float2 f = ldg2(lat + Vnu + offQ + i_xd);
+    float2 lo = cmul(cconjmul(d, e), f);
+    if (mu == g.tdir || nu == g.tdir)
+      st = cadd(st, cadd(up, lo));
+    else
+      ss = cadd(ss, cadd(up, lo));
+  }
+  return cadd(cscale(ss, c.w_ss), cscale(st, c.w_st));
+}
+
+// Overrelaxation of one link: U' = (conj S)^2/|S|^2 * conj U, renormalised.
+// |S| == 0 gives U' = conj U (the reference's atan2(0,0) = 0 case).
+__device__ __forceinline__ float2 overrelax_link(float2 S, float2 U) {
+  float n2 = fmaf(S.x, S.x, S.y * S.y);
+  if (n2 > 0.f) {
+    float inv = 1.0f / n2;
+    float ax = (S.x * S.x - S.y * S.y) * inv;
+    float ay = -2.0f * S.x * S.y * inv;
+    float2 Un = make_float2(fmaf(ax, U.x, ay * U.y), fmaf(ay, U.x, -ax * U.y));
+    float r = rsqrtf(fmaf(Un.x, Un.x, Un.y * Un.y));
+    return make_float2(Un.x * r, Un.y * r);
+  }
+  return make_float2(U.x, -U.y);
+}
+
+struct UpdArgs {
+  float2 *lat;
+  GeomK g;
+  CoupK c;
+  int p;
+  int mu;
+  uint32_t key0, key1;                 // Philox key (seed)
+  uint32_t chain;                      // chain number in the counter
+  const unsigned long long *pass_dev;  // Metropolis pass counter (device)
+  int hit;                             // pass = *pass_dev + hit
+  const double *replay;                // shared-stream pairs (test mode)
+  unsigned long long replay_base;      // pass number of replay[0]
+  unsigned long long *bump_ptr;        // OR kernels: *bump_ptr += bump_by (block 0)
+  unsigned int bump_by;
+  int ml;                              // multilevel freeze period (0 = none)
+};
+
+// One (parity, mu) phase.  MET selects Metropolis vs overrelaxation, REPLAY
+// reads the shared-stream pairs instead of Philox.
+template <int D, bool MET, bool REPLAY>
+__global__ void __launch_bounds__(256) k_update(const UpdArgs a) {
+  if (!MET && a.bump_ptr != nullptr && blockIdx.x == 0 && threadIdx.x == 0)
+    *a.bump_ptr += a.bump_by;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.g.Vh) return;
+  int x[4];
+  eo_decode(a.g, i, a.p, x);
+  // Multilevel freeze rule, reference src/multilevel.cu:41: update unless the
+  // site lies on a frozen time slice and the link is spatial (the reference
+  // tests the literal direction index 3).
+  if (a.ml > 0 && a.mu != 3 && (x[a.g.tdir] % a.ml) == 0) return;
+  const size_t self = (size_t)a.mu * a.g.V + (size_t)a.p * a.g.Vh + i;
+  const float2 S = staple_at<D>(a.lat, a.g, a.c, x, i, a.p, a.mu);
+  const float2 U = a.lat[self];
+  if (MET) {
+    const unsigned long long pass = *a.pass_dev + (unsigned long long)a.hit;
+    float2 Un;
+    float b;
+    if (REPLAY) {
+      const size_t pr = ((((size_t)(pass - a.replay_base) * 2 + a.p) * D + a.mu) * a.g.Vh + i) * 2;
+      double sn, cs;
+      sincos(a.replay[pr], &sn, &cs);
+      Un = make_float2((float)cs, (float)sn);
+      b = (float)a.replay[pr + 1];
+    } else {
+      Philox4 r = philox4x32_10((uint32_t)(a.p * a.g.Vh + i),
+                                u1_rng_word1(a.mu, U1_TAG_METROPOLIS, a.chain),
+                                (uint32_t)pass, (uint32_t)(pass >> 32), a.key0, a.key1);
+      float u1 = u1_uniform_open(r.v[0]);
+      b = u1_uniform_open(r.v[1]);
+      float sn, cs;
+      sincospif(2.0f * u1, &sn, &cs);
+      Un = make_float2(cs, sn);
+    }
+    const float dS = a.c.beta * (cre_mul(S, Un) - cre_mul(S, U));
+    if (expf(dS) > b) a.lat[self] = Un;
+  } else {
+    a.lat[self] = overrelax_link(S, U);
+  }
+}
+
+// Hot start (reference src/update.cu:30-48): every link gets
+// theta = 2 pi u, u from Philox with the hot-start tag.
+template <int D>
+__global__ void __launch_bounds__(256) k_hot_start(float2 *lat, GeomK g, uint32_t key0,
+                                                   uint32_t key1, uint32_t chain,
+                                                   unsigned long long pass) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.Vh) return;
+#pragma unroll
+  for (int p = 0; p < 2; ++p)
+#pragma unroll
+    for (int mu = 0; mu < D; ++mu) {
+      Philox4 r = philox4x32_10((uint32_t)(p * g.Vh + i), u1_rng_word1(mu, U1_TAG_HOTSTART, chain),
+                                (uint32_t)pass, (uint32_t)(pass >> 32), key0, key1);
+      float sn, cs;
+      sincospif(2.0f * u1_uniform_open(r.v[0]), &sn, &cs);
+      lat[(size_t)mu * g.V + (size_t)p * g.Vh + i] = make_float2(cs, sn);
+    }
+}
+
+__global__ void k_import_angles(float2 *lat, const double *ang, size_t n) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s, c;
+  sincos(ang[i], &s, &c);
+  lat[i] = make_float2((float)c, (float)s);
+}
+
+__global__ void k_export_angles(const float2 *lat, double *ang, size_t n) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float2 u = lat[i];
+  double t = atan2((double)u.y, (double)u.x);
+  if (t < 0.0) t += 2.0 * 3.14159265358979323846;
+  ang[i] = t;
+}
+
+__global__ void k_fill_links(float2 *lat, size_t n, float2 v) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) lat[i] = v;
+}
+
+__global__ void k_pass_add(unsigned long long *pass, unsigned long long n) { *pass += n; }
+
+__global__ void k_rng_debug(float *out, int Vh, int p, int mu, uint32_t key0, uint32_t key1,
+                            uint32_t chain, unsigned long long pass) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= Vh) return;
+  Philox4 r = philox4x32_10((uint32_t)(p * Vh + i), u1_rng_word1(mu, U1_TAG_METROPOLIS, chain),
+                            (uint32_t)pass, (uint32_t)(pass >> 32), key0, key1);
+  out[2 * i] = u1_uniform_open(r.v[0]);
+  out[2 * i + 1] = u1_uniform_open(r.v[1]);
+}
+
+}  // namespace u1b

@@ -1,0 +1,227 @@
+"""Python host layer over the C ABI: contexts, lattices and counter-based RNGs.
+
+Names mirror the reference's driver surface (reference u1.cpp:44-149):
+Context ~ Start/Finalize, Lattice ~ SetupLatticeParameters + Array<double>,
+Rng ~ CudaRNG, Lattice.update ~ UpdateLattice, .plaquette ~ Plaquette,
+.polyakov ~ Polyakov, .poly_corr ~ Poly2, .multilevel ~ MultiLevel.
+All compute runs in the sm_100a kernels of libu1b200.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Sequence
+
+import numpy as np
+
+from ._lib import check, lib, u1_geom
+
+
+def _grid(dims: int, N: Sequence[int]) -> list[int]:
+    """Grid[] as the reference's SetupLatticeParameters builds it
+    (reference src/parameters.cu:146-161) from (Nx, Ny, Nz, Nt)."""
+    Nx, Ny, Nz, Nt = N
+    g = [1, 1, 1, 1]
+    g[0] = Nx
+    g[1] = Nt if dims == 2 else Ny
+    if dims == 3:
+        g[2] = Nt
+    elif dims > 3:
+        g[2] = Nz
+    if dims == 4:
+        g[3] = Nt
+    return g
+
+
+class Context:
+    """One CUDA device (reference Start(gpuid, ...), src/cuda_error_check.cpp:24-45)."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        check(lib.u1_ctx_create(int(device), C.byref(h)), "u1_ctx_create")
+        self._h = h
+        self.device = device
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def close(self) -> None:
+        if self._h:
+            lib.u1_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Rng:
+    """Counter-based Philox4x32-10 stream: state = (seed, pass counter)."""
+
+    def __init__(self, ctx: Context, seed: int = 1234):
+        h = C.c_void_p()
+        check(lib.u1_rng_create(ctx.handle, C.c_uint64(seed), C.byref(h)), "u1_rng_create")
+        self._h = h
+        self.ctx = ctx
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    @property
+    def state(self) -> tuple[int, int]:
+        s, p = C.c_uint64(), C.c_uint64()
+        check(lib.u1_rng_get_state(self._h, C.byref(s), C.byref(p)), "u1_rng_get_state")
+        return int(s.value), int(p.value)
+
+    def set_state(self, seed: int, pass_: int) -> None:
+        check(lib.u1_rng_set_state(self._h, C.c_uint64(seed), C.c_uint64(pass_)), "u1_rng_set_state")
+
+    def set_replay(self, pairs: np.ndarray | None) -> None:
+        """Shared-stream test mode: pairs[..., 2] = (new theta, b) per link in
+        the reference's draw order pass -> parity -> mu -> id."""
+        if pairs is None:
+            check(lib.u1_rng_set_replay(self._h, None, 0), "u1_rng_set_replay")
+            self._replay = None
+            return
+        arr = np.ascontiguousarray(pairs, dtype=np.float64).reshape(-1, 2)
+        self._replay = arr
+        check(lib.u1_rng_set_replay(self._h, arr.ctypes.data_as(C.c_void_p), arr.shape[0]), "u1_rng_set_replay")
+
+    def debug_uniforms(self, lat: "Lattice", pass_: int, parity: int, mu: int) -> np.ndarray:
+        out = np.empty((lat.Vh, 2), dtype=np.float32)
+        check(lib.u1_rng_debug_uniforms(lat.handle, self._h, C.c_uint64(pass_), parity, mu,
+                                        out.ctypes.data_as(C.c_void_p)), "u1_rng_debug_uniforms")
+        return out
+
+    def close(self) -> None:
+        if self._h:
+            lib.u1_rng_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Lattice:
+    """A U(1) gauge field on the device, float2 links in even/odd SoA order."""
+
+    def __init__(self, ctx: Context, dims: int, N: Sequence[int], beta: float, aniso: float = 1.0):
+        N = list(N) + [0] * (4 - len(N))
+        geom = u1_geom(dims=int(dims), N=(C.c_int * 4)(*[int(n) for n in N[:4]]),
+                       beta=float(beta), aniso=float(aniso))
+        h = C.c_void_p()
+        check(lib.u1_lattice_create(ctx.handle, C.byref(geom), C.byref(h)), "u1_lattice_create")
+        self._h = h
+        self.ctx = ctx
+        self.dims = int(dims)
+        self.beta = float(beta)
+        self.aniso = float(aniso)
+        info = (C.c_int64 * 8)()
+        check(lib.u1_lattice_info(h, info), "u1_lattice_info")
+        self.V, self.Vh, self.Vs = int(info[0]), int(info[1]), int(info[2])
+        self.grid = [int(info[4 + k]) for k in range(4)]
+        self.R = self.grid[0] // 2
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    @property
+    def nlinks(self) -> int:
+        return self.V * self.dims
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        check(lib.u1_lattice_set_stream(self._h, C.c_void_p(stream_ptr or 0)), "u1_lattice_set_stream")
+
+    def set_coupling(self, beta: float, aniso: float | None = None) -> None:
+        aniso = self.aniso if aniso is None else aniso
+        check(lib.u1_lattice_set_coupling(self._h, float(beta), float(aniso)), "u1_lattice_set_coupling")
+        self.beta, self.aniso = float(beta), float(aniso)
+
+    def links_ptr(self) -> int:
+        p = C.c_void_p()
+        check(lib.u1_lattice_links(self._h, C.byref(p)), "u1_lattice_links")
+        return int(p.value)
+
+    def copy_from(self, other: "Lattice") -> None:
+        check(lib.u1_lattice_copy(self._h, other.handle), "u1_lattice_copy")
+
+    # -- data movement (reference layout theta[id + p*V/2 + mu*V]) --------
+    def import_angles(self, theta) -> None:
+        if hasattr(theta, "is_cuda") and theta.is_cuda:
+            assert theta.dtype.__str__() == "torch.float64" and theta.numel() == self.nlinks
+            check(lib.u1_lattice_import_angles(self._h, C.c_void_p(theta.contiguous().data_ptr()), 1),
+                  "u1_lattice_import_angles")
+            return
+        arr = np.ascontiguousarray(theta, dtype=np.float64).reshape(-1)
+        if arr.size != self.nlinks:
+            raise ValueError(f"expected {self.nlinks} angles, got {arr.size}")
+        check(lib.u1_lattice_import_angles(self._h, arr.ctypes.data_as(C.c_void_p), 0), "u1_lattice_import_angles")
+
+    def export_angles(self, out=None) -> np.ndarray:
+        if out is not None and hasattr(out, "is_cuda") and out.is_cuda:
+            check(lib.u1_lattice_export_angles(self._h, C.c_void_p(out.data_ptr()), 1), "u1_lattice_export_angles")
+            return out
+        arr = np.empty(self.nlinks, dtype=np.float64)
+        check(lib.u1_lattice_export_angles(self._h, arr.ctypes.data_as(C.c_void_p), 0), "u1_lattice_export_angles")
+        return arr
+
+    # -- Monte Carlo -----------------------------------------------------
+    def cold_start(self) -> None:
+        check(lib.u1_cold_start(self._h), "u1_cold_start")
+
+    def hot_start(self, rng: Rng) -> None:
+        check(lib.u1_hot_start(self._h, rng.handle), "u1_hot_start")
+
+    def update(self, rng: Rng, metrop: int = 1, ovrn: int = 4) -> None:
+        check(lib.u1_update(self._h, rng.handle, int(metrop), int(ovrn)), "u1_update")
+
+    # -- measurements ------------------------------------------------------
+    def measure(self) -> dict:
+        out = (C.c_double * 6)()
+        check(lib.u1_measure(self._h, out), "u1_measure")
+        return {"plaq_ss": complex(out[0], out[1]), "plaq_st": complex(out[2], out[3]),
+                "poly": complex(out[4], out[5])}
+
+    def measure_async(self, dev_ptr: int) -> None:
+        check(lib.u1_measure_async(self._h, C.c_void_p(dev_ptr)), "u1_measure_async")
+
+    def plaquette(self) -> tuple[complex, complex]:
+        out = (C.c_double * 4)()
+        check(lib.u1_plaquette(self._h, out), "u1_plaquette")
+        return complex(out[0], out[1]), complex(out[2], out[3])
+
+    def polyakov(self) -> complex:
+        out = (C.c_double * 2)()
+        check(lib.u1_polyakov(self._h, out), "u1_polyakov")
+        return complex(out[0], out[1])
+
+    def poly_corr(self, multihit: bool = False) -> np.ndarray:
+        out = (C.c_double * (2 * self.R))()
+        check(lib.u1_poly_corr(self._h, int(bool(multihit)), out, 2 * self.R), "u1_poly_corr")
+        a = np.frombuffer(out, dtype=np.float64).copy()
+        return a[0::2] + 1j * a[1::2]
+
+    def multilevel(self, rng: Rng, n4: int, k4: int, n2: int, k2: int, metrop: int, ovrn: int) -> np.ndarray:
+        out = (C.c_double * (2 * self.R))()
+        check(lib.u1_multilevel(self._h, rng.handle, n4, k4, n2, k2, metrop, ovrn, out, 2 * self.R),
+              "u1_multilevel")
+        a = np.frombuffer(out, dtype=np.float64).copy()
+        return a[0::2] + 1j * a[1::2]
+
+    def close(self) -> None:
+        if self._h:
+            lib.u1_lattice_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
