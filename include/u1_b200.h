@@ -77,6 +77,10 @@ int u1_lattice_set_stream(u1_lattice *lat, void *stream);
 int u1_lattice_info(const u1_lattice *lat, int64_t out[8]);
 /* Change beta / aniso of an existing lattice (no reallocation). */
 int u1_lattice_set_coupling(u1_lattice *lat, double beta, double aniso);
+/* Sweeps issued by u1_update are captured once into a CUDA graph and
+ * replayed (enable = 1, default) or launched kernel by kernel (enable = 0).
+ * Both issue the same kernels with the same arguments. */
+int u1_lattice_set_graphs(u1_lattice *lat, int enable);
 /* Device pointer of the float2 link array (V*dims float2). */
 int u1_lattice_links(u1_lattice *lat, void **dev_ptr);
 /* Copy all links of src into dst (same geometry). */

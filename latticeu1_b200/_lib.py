@@ -44,6 +44,7 @@ SIGNATURES = {
     "u1_lattice_set_stream": [_vp, _vp],
     "u1_lattice_info": [_vp, C.POINTER(C.c_int64)],
     "u1_lattice_set_coupling": [_vp, C.c_double, C.c_double],
+    "u1_lattice_set_graphs": [_vp, _i],
     "u1_lattice_links": [_vp, C.POINTER(_vp)],
     "u1_lattice_copy": [_vp, _vp],
     "u1_lattice_import_angles": [_vp, _vp, _i],

@@ -255,6 +255,13 @@ extern "C" int u1_lattice_set_coupling(u1_lattice *lat, double beta, double anis
   return U1_OK;
 }
 
+extern "C" int u1_lattice_set_graphs(u1_lattice *lat, int enable) {
+  if (!lat) return fail(U1_ERR_INVALID, "u1_lattice_set_graphs: null lattice");
+  lat->use_graphs = enable != 0;
+  if (!lat->use_graphs) drop_graphs(lat);
+  return U1_OK;
+}
+
 extern "C" int u1_lattice_links(u1_lattice *lat, void **dev_ptr) {
   if (!lat || !dev_ptr) return fail(U1_ERR_INVALID, "u1_lattice_links: null argument");
   *dev_ptr = lat->links;

@@ -144,6 +144,9 @@ class Lattice:
         check(lib.u1_lattice_set_coupling(self._h, float(beta), float(aniso)), "u1_lattice_set_coupling")
         self.beta, self.aniso = float(beta), float(aniso)
 
+    def set_graphs(self, enable: bool) -> None:
+        check(lib.u1_lattice_set_graphs(self._h, int(bool(enable))), "u1_lattice_set_graphs")
+
     def links_ptr(self) -> int:
         p = C.c_void_p()
         check(lib.u1_lattice_links(self._h, C.byref(p)), "u1_lattice_links")

@@ -59,6 +59,7 @@ class Oracle:
                 "o_index_eo": (None, [g, C.c_int, C.c_int, C.POINTER(C.c_int)]),
                 "o_index_eo_neg": (C.c_long, [g, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
                 "o_staple": (None, [g, _dp, C.c_int, C.c_int, C.c_int, _dp]),
+                "o_staple_all": (None, [g, _dp, _dp]),
                 "o_metropolis_pairs": (C.c_long, [g, _dp, _dp]),
                 "o_metropolis_philox": (C.c_long, [g, _dp, C.c_uint64, C.c_uint32, C.c_uint64, C.c_int]),
                 "o_philox_uniforms": (None, [g, C.c_uint64, C.c_uint32, C.c_uint64, C.c_int, C.c_int, C.c_int,
@@ -111,6 +112,21 @@ class Oracle:
         o = np.zeros(2)
         self.lib().o_staple(self._g(), _arr(lat), id_, parity, mu, _arr(o))
         return complex(o[0], o[1])
+
+    def staple_all(self, lat) -> np.ndarray:
+        """Complex staple of every link, reference layout."""
+        o = np.zeros(2 * self.nlinks)
+        self.lib().o_staple_all(self._g(), _arr(np.ascontiguousarray(lat)), _arr(o))
+        return o[0::2] + 1j * o[1::2]
+
+    def fp32_angle_tolerance(self, lat, base: float = 1e-5) -> np.ndarray:
+        """Per-link bound for one FP32 pass vs FP64: base + 2*dS/|S| with
+        dS = 12*8 roundings of 2^-24 times the largest staple weight.  The
+        reflection theta' = -theta - 2 arg S amplifies a staple error dS by
+        2/|S|; links with tiny |S| are ill-conditioned in any precision."""
+        w = max(self.g.aniso, 1.0 / self.g.aniso)
+        dS = 12 * 8 * 2.0 ** -24 * w
+        return base + 2.0 * dS / np.maximum(np.abs(self.staple_all(lat)), 1e-30)
 
     def metropolis_pairs(self, lat: np.ndarray, pairs: np.ndarray) -> int:
         pairs = np.ascontiguousarray(pairs, dtype=np.float64)

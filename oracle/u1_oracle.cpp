@@ -122,6 +122,19 @@ void o_staple(const OGeom *g, const double *lat, int id, int parity, int mu, dou
   out[1] = S.imag();
 }
 
+// Staple of every link in the reference layout: out[2*l], out[2*l+1] for
+// l = id + parity*V/2 + mu*V.  Used for conditioning-aware FP32 tolerances.
+void o_staple_all(const OGeom *g, const double *lat, double *out) {
+  for (int mu = 0; mu < g->dims; ++mu)
+    for (int p = 0; p < 2; ++p) {
+#pragma omp parallel for schedule(static)
+      for (int id = 0; id < (int)g->Vh; ++id) {
+        const long l = id + p * g->Vh + mu * g->V;
+        o_staple(g, lat, id, p, mu, out + 2 * l);
+      }
+    }
+}
+
 // One Metropolis pass with externally supplied (new_theta, b) pairs in the
 // reference CPU draw order parity -> mu -> id (reference src/update.cu:51-79).
 // Returns the number of accepted proposals.

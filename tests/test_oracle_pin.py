@@ -109,12 +109,18 @@ def test_bessel_ratio(x):
 
 def exact_2d_plaquette(beta: float, V: int) -> float:
     """<cos theta_P> on a periodic 2D lattice of V plaquettes:
-    sum_n I_n^{V-1} (I_{n-1}+I_{n+1})/2 / sum_n I_n^V (all at beta)."""
-    n = np.arange(-30, 31)
-    In = special.iv(n, beta)
-    num = np.sum(In ** (V - 1) * 0.5 * (special.iv(n - 1, beta) + special.iv(n + 1, beta)))
-    den = np.sum(In ** V)
-    return float(num / den)
+    sum_n I_n^{V-1} (I_{n-1}+I_{n+1})/2 / sum_n I_n^V (all at beta), with every
+    I_n divided by I_0 so the powers stay finite."""
+    n = np.arange(-40, 41)
+    r = special.ive(n, beta) / special.ive(0, beta)
+    rm = special.ive(n - 1, beta) / special.ive(0, beta)
+    rp = special.ive(n + 1, beta) / special.ive(0, beta)
+    return float(np.sum(r ** (V - 1) * 0.5 * (rm + rp)) / np.sum(r ** V))
+
+
+def test_exact_2d_plaquette_large_volume_limit():
+    for beta in (2.0, 4.0, 6.0):
+        assert abs(exact_2d_plaquette(beta, 1024) - special.iv(1, beta) / special.iv(0, beta)) < 1e-10
 
 
 def binned_mean_err(x, nbins=20):
