@@ -134,6 +134,19 @@ int u1_measure(u1_lattice *lat, double out[6]);
 /* Asynchronous form: the 6 doubles land in device memory dev_out. */
 int u1_measure_async(u1_lattice *lat, double *dev_out);
 
+/* No counterpart in the reference.  The u1_measure_async measurement for
+ * callers that cannot allocate device memory (e.g. code confined to memory
+ * handed out by its host framework, or loops where a cudaMalloc that may
+ * synchronise the device is not acceptable).  It allocates nothing: its
+ * scratch is a fixed file-scope device array of about 192 KiB that every GPU
+ * loading the library keeps until exit.  links_dev: the V*dims float2 links
+ * (this library's layout); out_dev: 6 doubles, as u1_measure; stream:
+ * cudaStream_t as void* on the current device.  Lattices with V/2 above
+ * 1,048,576 sites return U1_ERR_INVALID.  The first call on a device looks
+ * up the array's address and should come before any stream capture; calls
+ * that overlap on the GPU race on the shared array. */
+int u1_measure_noalloc(const void *links_dev, const u1_geom *geom, double *out_dev, void *stream);
+
 /* Replaces Poly2 (reference src/polyakov.cu:618-654):
  * out[2*(r-1)], out[2*(r-1)+1] = re, im of C(r) for r = 1..R, R = Grid[0]/2,
  * C(r) = 1/(V_s (d-1)) sum_x sum_i P(x) conj(P(x + r e_i)).  multihit != 0

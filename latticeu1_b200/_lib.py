@@ -62,6 +62,7 @@ SIGNATURES = {
     "u1_polyakov": [_vp, _dp],
     "u1_measure": [_vp, _dp],
     "u1_measure_async": [_vp, _vp],
+    "u1_measure_noalloc": [_vp, C.POINTER(u1_geom), _vp, _vp],
     "u1_poly_corr": [_vp, _i, _dp, _i],
     "u1_multilevel": [_vp, _vp, _i, _i, _i, _i, _i, _i, _dp, _i],
     "u1_kernel_launch_count": [C.POINTER(C.c_uint64)],

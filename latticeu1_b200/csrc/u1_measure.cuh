@@ -83,7 +83,7 @@ __device__ __forceinline__ void partials_finish(double (&v)[NV], double *smem, d
 // out = {SS re, SS im, ST re, ST im, L re, L im}: mean of (1 - e^{i theta_P})
 // per class and (1/V_s) sum_x prod_t U_t.
 template <int D>
-__global__ void __launch_bounds__(kRedThreads)
+static __global__ void __launch_bounds__(kRedThreads)
     k_measure(const float2 *__restrict__ lat, GeomK g, double *partials, unsigned int *counter,
               double *out, double normSS, double normST, double normL) {
   __shared__ double smem[kRedWarps * 6];
@@ -179,7 +179,7 @@ __device__ __forceinline__ void spatial_decode(const GeomK &g, int s, int x[4]) 
 // P(x) = prod_t U_t(x,t) (or of the multihit means) for every spatial site,
 // stored in spatial lexicographic order; products in FP64.
 template <int D, bool MH>
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
     k_poly_field(const float2 *__restrict__ lat, GeomK g, CoupK c, double2 *P) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= g.Vs) return;
@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(256)
 
 // C(r) = norm * sum_x sum_{i<d-1} P(x) conj(P(x + r e_i)), r = 1..R.
 // partials: gridDim.x * 2R doubles; out: 2R doubles.
-__global__ void __launch_bounds__(kRedThreads)
+static __global__ void __launch_bounds__(kRedThreads)
     k_poly_corr(const double2 *__restrict__ P, GeomK g, int R, double *partials,
                 unsigned int *counter, double *out, double norm) {
   __shared__ double smem[kRedWarps * 2];

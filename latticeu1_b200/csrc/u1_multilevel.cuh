@@ -16,7 +16,7 @@ namespace u1b {
 
 // Multihit mean of every temporal link, stored at the 4D lexicographic index.
 template <int D>
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
     k_ml_mhit_field(const float2 *__restrict__ lat, GeomK g, CoupK c, float2 *mh) {
   const int id = blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= g.V) return;
@@ -45,7 +45,7 @@ __device__ __forceinline__ int spatial_shift(const GeomK &g, const int x[4], int
 
 // T2[x, r, i, slab] += prod_{t in slab} mh(x,t) * prod_{t in slab} conj(mh(x + r e_i, t)),
 // slabs of thickness 2.  One thread per (x, r, i).
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
     k_ml_T2(const float2 *__restrict__ mh, GeomK g, int R, double2 *T2) {
   const size_t size = (size_t)g.Vs * R * g.tdir;
   const size_t id = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(256)
 }
 
 // T4[., slab4] += prod_{two level-2 slabs} (T2 * l2norm).  One thread per (x, r, i).
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
     k_ml_T4(const double2 *__restrict__ T2, GeomK g, int R, double l2norm, double2 *T4) {
   const size_t size = (size_t)g.Vs * R * g.tdir;
   const size_t id = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(256)
 }
 
 // C(r) = norm * sum_x sum_i prod_{slab4} (T4 * l4norm), r = 1..R.
-__global__ void __launch_bounds__(kRedThreads)
+static __global__ void __launch_bounds__(kRedThreads)
     k_ml_final(const double2 *__restrict__ T4, GeomK g, int R, double l4norm, double *partials,
                unsigned int *counter, double *out, double norm) {
   __shared__ double smem[kRedWarps * 2];

@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(256) k_hot_start(float2 *lat, GeomK g, uint32_
     }
 }
 
-__global__ void k_import_angles(float2 *lat, const double *ang, size_t n) {
+static __global__ void k_import_angles(float2 *lat, const double *ang, size_t n) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double s, c;
@@ -169,7 +169,7 @@ __global__ void k_import_angles(float2 *lat, const double *ang, size_t n) {
   lat[i] = make_float2((float)c, (float)s);
 }
 
-__global__ void k_export_angles(const float2 *lat, double *ang, size_t n) {
+static __global__ void k_export_angles(const float2 *lat, double *ang, size_t n) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   float2 u = lat[i];
@@ -178,14 +178,14 @@ __global__ void k_export_angles(const float2 *lat, double *ang, size_t n) {
   ang[i] = t;
 }
 
-__global__ void k_fill_links(float2 *lat, size_t n, float2 v) {
+static __global__ void k_fill_links(float2 *lat, size_t n, float2 v) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) lat[i] = v;
 }
 
-__global__ void k_pass_add(unsigned long long *pass, unsigned long long n) { *pass += n; }
+static __global__ void k_pass_add(unsigned long long *pass, unsigned long long n) { *pass += n; }
 
-__global__ void k_rng_debug(float *out, int Vh, int p, int mu, uint32_t key0, uint32_t key1,
+static __global__ void k_rng_debug(float *out, int Vh, int p, int mu, uint32_t key0, uint32_t key1,
                             uint32_t chain, unsigned long long pass) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= Vh) return;
