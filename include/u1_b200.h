@@ -122,6 +122,13 @@ int u1_hot_start(u1_lattice *lat, u1_rng *rng);
  * 383-386).  Asynchronous on the lattice's stream. */
 int u1_update(u1_lattice *lat, u1_rng *rng, int metrop, int ovrn);
 
+/* Test and debugging aid: run exactly one (parity, mu) phase of a
+ * Metropolis (metropolis != 0) or overrelaxation pass, with the Metropolis
+ * numbers of pass (rng pass counter + hit).  The pass counter is not
+ * advanced.  A pass of u1_update is the phases parity 0,1 x mu 0..dims-1 in
+ * that order (reference src/update.cu:305-308). */
+int u1_update_phase(u1_lattice *lat, u1_rng *rng, int metropolis, int parity, int mu, int hit);
+
 /* Replaces Plaquette (reference src/plaquette.cu:222-228):
  * out = {SS re, SS im, ST re, ST im} of mean(1 - exp(i theta_P)).  In 2D the
  * SS mean has no plaquettes and is NaN, as in the reference. Synchronous. */

@@ -58,6 +58,7 @@ SIGNATURES = {
     "u1_rng_debug_uniforms": [_vp, _vp, C.c_uint64, _i, _i, _vp],
     "u1_hot_start": [_vp, _vp],
     "u1_update": [_vp, _vp, _i, _i],
+    "u1_update_phase": [_vp, _vp, _i, _i, _i, _i],
     "u1_plaquette": [_vp, _dp],
     "u1_polyakov": [_vp, _dp],
     "u1_measure": [_vp, _dp],

@@ -117,7 +117,8 @@ extern "C" int u1_ctx_set_stream(u1_ctx *ctx, void *stream) {
 }
 
 // ---------------------------------------------------------------- lattice
-static int make_geom(const u1_geom *gm, GeomK &g) {
+namespace u1i {
+int make_geom(const u1_geom *gm, GeomK &g) {
   if (!gm) return fail(U1_ERR_INVALID, "geometry: null");
   const int d = gm->dims;
   if (d < 2 || d > 4) return fail(U1_ERR_INVALID, "geometry: dims must be 2, 3 or 4");
@@ -137,20 +138,15 @@ static int make_geom(const u1_geom *gm, GeomK &g) {
     V *= Grid[k];
   }
   if (V * d > (1LL << 31)) return fail(U1_ERR_UNSUPPORTED, "geometry: V*dims exceeds 2^31 links");
+  g = GeomK{};
   g.dims = d;
-  g.tdir = d - 1;
   for (int k = 0; k < 4; ++k) g.N[k] = Grid[k];
-  g.hN0 = Grid[0] / 2;
-  g.es[0] = 0;
-  g.es[1] = g.hN0;
-  g.es[2] = g.hN0 * Grid[1];
-  g.es[3] = g.hN0 * Grid[1] * Grid[2];
-  g.V = (int)V;
-  g.Vh = (int)(V / 2);
-  g.Vs = 1;
-  for (int k = 0; k < g.tdir; ++k) g.Vs *= Grid[k];
+  geom_finish(g);
   return U1_OK;
 }
+}  // namespace u1i
+
+using u1i::make_geom;
 
 extern "C" int u1_geom_validate(const u1_geom *geom, int64_t out[8]) {
   GeomK g{};
@@ -440,19 +436,34 @@ extern "C" int u1_hot_start(u1_lattice *lat, u1_rng *rng) {
   return U1_OK;
 }
 
-template <int D>
-static int launch_phase(const UpdArgs &a, cudaStream_t s, bool met, bool replay) {
+template <int D, int MU>
+static int launch_phase_mu(const UpdArgs &a, cudaStream_t s, bool met, bool replay) {
   const int blocks = u1i::blocks_for(a.g.Vh, 256);
   if (met) {
     if (replay)
-      k_update<D, true, true><<<blocks, 256, 0, s>>>(a);
+      k_update<D, MU, true, true><<<blocks, 256, 0, s>>>(a);
     else
-      k_update<D, true, false><<<blocks, 256, 0, s>>>(a);
+      k_update<D, MU, true, false><<<blocks, 256, 0, s>>>(a);
   } else {
-    k_update<D, false, false><<<blocks, 256, 0, s>>>(a);
+    k_update<D, MU, false, false><<<blocks, 256, 0, s>>>(a);
   }
   U1_LAUNCH_CHECK("k_update");
   return U1_OK;
+}
+
+template <int D>
+static int launch_phase(const UpdArgs &a, cudaStream_t s, bool met, bool replay) {
+  switch (a.mu) {
+    case 0: return launch_phase_mu<D, 0>(a, s, met, replay);
+    case 1: return launch_phase_mu<D, 1>(a, s, met, replay);
+    case 2:
+      if constexpr (D > 2) return launch_phase_mu<D, 2>(a, s, met, replay);
+      break;
+    case 3:
+      if constexpr (D > 3) return launch_phase_mu<D, 3>(a, s, met, replay);
+      break;
+  }
+  return fail(U1_ERR_INVALID, "k_update: direction out of range");
 }
 
 // Issue one sweep (metrop Metropolis + ovrn overrelaxation passes) on links
@@ -558,6 +569,37 @@ extern "C" int u1_update(u1_lattice *lat, u1_rng *rng, int metrop, int ovrn) {
   }
   rng->pass += (uint64_t)metrop;
   return U1_OK;
+}
+
+extern "C" int u1_update_phase(u1_lattice *lat, u1_rng *rng, int metropolis, int parity, int mu, int hit) {
+  if (!lat || !rng) return fail(U1_ERR_INVALID, "u1_update_phase: null argument");
+  if (parity < 0 || parity > 1 || mu < 0 || mu >= lat->g.dims || hit < 0)
+    return fail(U1_ERR_INVALID, "u1_update_phase: bad parity/mu/hit");
+  U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
+  const bool met = metropolis != 0;
+  const bool replay = met && rng->replay_dev != nullptr;
+  if (replay) {
+    int rc = check_replay(lat, rng, hit + 1);
+    if (rc) return rc;
+  }
+  UpdArgs a{};
+  a.lat = lat->links;
+  a.g = lat->g;
+  a.c = lat->c;
+  a.p = parity;
+  a.mu = mu;
+  a.key0 = (uint32_t)rng->seed;
+  a.key1 = (uint32_t)(rng->seed >> 32);
+  a.chain = rng->chain;
+  a.pass_dev = rng->pass_dev;
+  a.hit = hit;
+  a.replay = rng->replay_dev;
+  a.replay_base = rng->replay_base;
+  switch (lat->g.dims) {
+    case 2: return launch_phase<2>(a, lat->stream, met, replay);
+    case 3: return launch_phase<3>(a, lat->stream, met, replay);
+    default: return launch_phase<4>(a, lat->stream, met, replay);
+  }
 }
 
 // ---------------------------------------------------------------- measurements

@@ -56,6 +56,9 @@ void set_error(const std::string &msg);
 int cuda_fail(cudaError_t e, const char *what);
 extern std::atomic<unsigned long long> g_launches;
 int ensure_scratch(u1_lattice *lat, size_t partial_doubles, size_t out_doubles);
+// Geometry from the ABI struct (Grid mapping of the reference's
+// SetupLatticeParameters); U1_ERR_INVALID on odd extents.
+int make_geom(const u1_geom *geom, u1b::GeomK &g);
 }  // namespace u1i
 
 #define U1_CUDA_TRY(call)                                            \

@@ -89,28 +89,15 @@ extern "C" int u1_measure_noalloc(const void *links_dev, const u1_geom *geom, do
     u1i::set_error("u1_measure_noalloc: null argument");
     return U1_ERR_INVALID;
   }
-  int64_t info[8];
-  int rc = u1_geom_validate(geom, info);
+  GeomK g{};
+  int rc = u1i::make_geom(geom, g);
   if (rc) return rc;
-  const int64_t Vh = info[1];
-  if (Vh > (int64_t)kNoAllocMaxBlocks * kRedThreads) {
+  if (g.Vh > kNoAllocMaxBlocks * kRedThreads) {
     u1i::set_error("u1_measure_noalloc: lattice too large for the fixed scratch array (V/2 = " +
-                   std::to_string(Vh) + " > maximum " + std::to_string((long long)kNoAllocMaxBlocks * kRedThreads) +
+                   std::to_string(g.Vh) + " > maximum " + std::to_string((long long)kNoAllocMaxBlocks * kRedThreads) +
                    " sites); use u1_measure_async");
     return U1_ERR_INVALID;
   }
-  GeomK g{};
-  g.dims = (int)info[3];
-  g.tdir = g.dims - 1;
-  for (int k = 0; k < 4; ++k) g.N[k] = (int)info[4 + k];
-  g.hN0 = g.N[0] / 2;
-  g.es[0] = 0;
-  g.es[1] = g.hN0;
-  g.es[2] = g.hN0 * g.N[1];
-  g.es[3] = g.hN0 * g.N[1] * g.N[2];
-  g.V = (int)info[0];
-  g.Vh = (int)info[1];
-  g.Vs = (int)info[2];
   double *scratch = nullptr;
   rc = noalloc_scratch(&scratch);
   if (rc) return rc;

@@ -97,47 +97,78 @@ struct UpdArgs {
   int ml;                              // multilevel freeze period (0 = none)
 };
 
-// One (parity, mu) phase.  MET selects Metropolis vs overrelaxation, REPLAY
-// reads the shared-stream pairs instead of Philox.
-template <int D, bool MET, bool REPLAY>
+// Staple of link (x, MU) from precomputed EO steps (eo_steps): all six
+// neighbour indices of each plaquette pair are i plus one or two steps.
+template <int D, int MU>
+__device__ __forceinline__ float2 staple_steps(const float2 *__restrict__ lat, const GeomK &g, const CoupK &c,
+                                               int i, int p, const int fwd[4], const int bwd[4]) {
+  const int q = 1 - p;
+  const float2 *Lq_mu = lat + MU * g.V + q * g.Vh;
+  const int i_xm = i + fwd[MU];
+  float2 ss = make_float2(0.f, 0.f), st = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int nu = 0; nu < D; ++nu) {
+    if (nu == MU) continue;
+    const float2 *Lp_nu = lat + nu * g.V + p * g.Vh;
+    const float2 *Lq_nu = lat + nu * g.V + q * g.Vh;
+    // upper: U_nu(x+mu) conj(U_mu(x+nu)) conj(U_nu(x))
+    const float2 a = __ldg(Lq_nu + i_xm);
+    const float2 b = __ldg(Lq_mu + i + fwd[nu]);
+    const float2 cc = __ldg(Lp_nu + i);
+    // lower: conj(U_nu(x+mu-nu)) conj(U_mu(x-nu)) U_nu(x-nu)
+    const float2 d = __ldg(Lp_nu + i_xm + bwd[nu]);
+    const float2 e = __ldg(Lq_mu + i + bwd[nu]);
+    const float2 f = __ldg(Lq_nu + i + bwd[nu]);
+    const float2 sum = cadd(cmulc(cmulc(a, b), cc), cmul(cconjmul(d, e), f));
+    if (MU == D - 1 || nu == D - 1)
+      st = cadd(st, sum);
+    else
+      ss = cadd(ss, sum);
+  }
+  return cadd(cscale(ss, c.w_ss), cscale(st, c.w_st));
+}
+
+// One (parity, MU) phase, one thread per link.  MET selects Metropolis vs
+// overrelaxation, REPLAY reads the shared-stream pairs instead of Philox.
+template <int D, int MU, bool MET, bool REPLAY>
 __global__ void __launch_bounds__(256) k_update(const UpdArgs a) {
-  if (!MET && a.bump_ptr != nullptr && blockIdx.x == 0 && threadIdx.x == 0)
-    *a.bump_ptr += a.bump_by;
+  if (!MET && a.bump_ptr != nullptr && blockIdx.x == 0 && threadIdx.x == 0) *a.bump_ptr += a.bump_by;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.g.Vh) return;
-  int x[4];
-  eo_decode(a.g, i, a.p, x);
+  int x[4], k;
+  eo_decode_fast<D>(a.g, i, a.p, x, k);
   // Multilevel freeze rule, reference src/multilevel.cu:41: update unless the
-  // site lies on a frozen time slice and the link is spatial (the reference
-  // tests the literal direction index 3).
-  if (a.ml > 0 && a.mu != 3 && (x[a.g.tdir] % a.ml) == 0) return;
-  const size_t self = (size_t)a.mu * a.g.V + (size_t)a.p * a.g.Vh + i;
-  const float2 S = staple_at<D>(a.lat, a.g, a.c, x, i, a.p, a.mu);
-  const float2 U = a.lat[self];
+  // site lies on a frozen time slice (x_t multiple of ml, ml = 2 or 4) and
+  // the link is spatial (the reference tests the literal direction index 3).
+  if (MU != 3 && a.ml > 0 && (x[D - 1] & (a.ml - 1)) == 0) return;
+  int fwd[4], bwd[4];
+  eo_steps<D>(a.g, x, k, fwd, bwd);
+  float2 *own = a.lat + MU * a.g.V + a.p * a.g.Vh + i;
+  const float2 S = staple_steps<D, MU>(a.lat, a.g, a.c, i, a.p, fwd, bwd);
+  const float2 U = *own;
   if (MET) {
     const unsigned long long pass = *a.pass_dev + (unsigned long long)a.hit;
     float2 Un;
     float b;
     if (REPLAY) {
-      const size_t pr = ((((size_t)(pass - a.replay_base) * 2 + a.p) * D + a.mu) * a.g.Vh + i) * 2;
+      const size_t pr = ((((size_t)(pass - a.replay_base) * 2 + a.p) * D + MU) * a.g.Vh + i) * 2;
       double sn, cs;
       sincos(a.replay[pr], &sn, &cs);
       Un = make_float2((float)cs, (float)sn);
       b = (float)a.replay[pr + 1];
     } else {
-      Philox4 r = philox4x32_10((uint32_t)(a.p * a.g.Vh + i),
-                                u1_rng_word1(a.mu, U1_TAG_METROPOLIS, a.chain),
+      Philox4 r = philox4x32_10((uint32_t)(a.p * a.g.Vh + i), u1_rng_word1(MU, U1_TAG_METROPOLIS, a.chain),
                                 (uint32_t)pass, (uint32_t)(pass >> 32), a.key0, a.key1);
-      float u1 = u1_uniform_open(r.v[0]);
+      const float u1 = u1_uniform_open(r.v[0]);
       b = u1_uniform_open(r.v[1]);
       float sn, cs;
       sincospif(2.0f * u1, &sn, &cs);
       Un = make_float2(cs, sn);
     }
     const float dS = a.c.beta * (cre_mul(S, Un) - cre_mul(S, U));
-    if (expf(dS) > b) a.lat[self] = Un;
+    if (expf(dS) > b) *own = Un;
   } else {
-    a.lat[self] = overrelax_link(S, U);
+    *own = overrelax_link(S, U);
   }
 }
 

@@ -185,6 +185,11 @@ class Lattice:
     def update(self, rng: Rng, metrop: int = 1, ovrn: int = 4) -> None:
         check(lib.u1_update(self._h, rng.handle, int(metrop), int(ovrn)), "u1_update")
 
+    def update_phase(self, rng: Rng, metropolis: bool, parity: int, mu: int, hit: int = 0) -> None:
+        """One (parity, mu) phase; the rng's pass counter does not advance."""
+        check(lib.u1_update_phase(self._h, rng.handle, int(bool(metropolis)), int(parity), int(mu), int(hit)),
+              "u1_update_phase")
+
     # -- measurements ------------------------------------------------------
     def measure(self) -> dict:
         out = (C.c_double * 6)()

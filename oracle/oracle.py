@@ -66,10 +66,13 @@ class Oracle:
                                              C.POINTER(C.c_float)]),
                 "o_philox": (None, [C.c_uint32] * 6 + [C.POINTER(C.c_uint32)]),
                 "o_overrelax": (None, [g, _dp, C.c_int]),
+                "o_phase": (None, [g, _dp, C.c_int, C.c_int, C.c_int, _dp, C.c_uint64, C.c_uint32, C.c_uint64,
+                                   C.c_int, _dp, _dp]),
                 "o_hot_start_philox": (None, [g, _dp, C.c_uint64, C.c_uint32, C.c_uint64]),
                 "o_plaquette": (None, [g, _dp, _dp]),
                 "o_polyakov": (None, [g, _dp, _dp]),
                 "o_bessel_ratio": (C.c_double, [C.c_double]),
+                "o_fastdiv": (C.c_uint32, [C.c_uint32, C.c_uint32]),
                 "o_multihit": (None, [g, _dp, C.c_int, C.c_int, _dp]),
                 "o_poly_field": (None, [g, _dp, C.c_int, _dp]),
                 "o_poly_corr": (None, [g, _dp, C.c_int, _dp]),
@@ -149,6 +152,28 @@ class Oracle:
         cls.lib().o_philox(*[int(c) for c in ctr], *[int(k) for k in key], out)
         return [int(v) for v in out]
 
+    def phase(self, lat, met: bool, parity: int, mu: int, pairs=None, seed: int = 0, pass_: int = 0,
+              chain: int = 0, ml: int = 0):
+        """One (parity, mu) phase in place; returns (|S| per site, Metropolis
+        relative margin 1 - b/exp(dS) per site)."""
+        smag = np.zeros(self.Vh)
+        margin = np.zeros(self.Vh)
+        pp = None
+        if pairs is not None:
+            pairs = np.ascontiguousarray(pairs, dtype=np.float64).reshape(-1)
+            assert pairs.size == 2 * self.Vh
+            pp = _arr(pairs)
+        self.lib().o_phase(self._g(), _arr(lat), int(bool(met)), parity, mu, pp, seed, chain, pass_, ml,
+                           _arr(smag), _arr(margin))
+        return smag, margin
+
+    def fp32_staple_error(self) -> float:
+        """Bound on |S_fp32 - S_fp64|: 2(d-1) plaquette terms of weight up to
+        max(xi, 1/xi), each from three float2 links with a few complex
+        products, about 12 roundings of 2^-24 per term."""
+        w = max(self.g.aniso, 1.0 / self.g.aniso)
+        return 2 * (self.dims - 1) * w * 12 * 2.0 ** -24
+
     def overrelax(self, lat, ml=0) -> None:
         self.lib().o_overrelax(self._g(), _arr(lat), ml)
 
@@ -174,6 +199,10 @@ class Oracle:
         o = np.zeros(2)
         self.lib().o_polyakov(self._g(), _arr(lat), _arr(o))
         return complex(o[0], o[1])
+
+    @classmethod
+    def fastdiv(cls, n: int, d: int) -> int:
+        return int(cls.lib().o_fastdiv(n, d))
 
     @classmethod
     def bessel_ratio(cls, x: float) -> float:

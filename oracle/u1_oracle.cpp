@@ -23,6 +23,7 @@
 #include <cstring>
 #include <vector>
 
+#include "../latticeu1_b200/csrc/u1_geom.cuh"
 #include "../latticeu1_b200/csrc/u1_philox.h"
 
 typedef std::complex<double> cd;
@@ -211,6 +212,47 @@ long o_metropolis_philox(const OGeom *g, double *lat, uint64_t seed, uint32_t ch
   return acc;
 }
 
+// Exactly one (parity p, direction mu) phase of a Metropolis (met != 0) or
+// overrelaxation pass.  Metropolis numbers come from `pairs` (V/2 pairs for
+// this phase, reference draw order) when non-null, else from Philox
+// (seed, chain, pass).  For each site id of the phase it records the staple
+// magnitude used (smag[id]) and, for Metropolis, the relative decision
+// margin 1 - b/exp(dS) (margin[id]; 0 for overrelaxation), so a test can
+// tell an FP32 accept flip at the decision boundary from a wrong result.
+void o_phase(const OGeom *g, double *lat, int met, int p, int mu, const double *pairs, uint64_t seed,
+             uint32_t chain, uint64_t pass, int ml, double *smag, double *margin) {
+#pragma omp parallel for schedule(static)
+  for (int id = 0; id < (int)g->Vh; ++id) {
+    smag[id] = 0.0;
+    margin[id] = 0.0;
+    if (frozen(g, id, p, mu, ml)) continue;
+    const long pos = id + p * g->Vh + mu * g->V;
+    double S[2];
+    o_staple(g, lat, id, p, mu, S);
+    smag[id] = std::sqrt(S[0] * S[0] + S[1] * S[1]);
+    if (met) {
+      double th_new, b;
+      if (pairs) {
+        th_new = pairs[2 * id];
+        b = pairs[2 * id + 1];
+      } else {
+        float u[2];
+        o_philox_uniforms(g, seed, chain, pass, p, mu, id, u);
+        th_new = 2.0 * M_PI * (double)u[0];
+        b = (double)u[1];
+      }
+      const double dS = g->beta * (S[0] * (std::cos(th_new) - std::cos(lat[pos])) -
+                                   S[1] * (std::sin(th_new) - std::sin(lat[pos])));
+      const double e = std::exp(dS);
+      margin[id] = 1.0 - b / e;
+      if (e > b) lat[pos] = th_new;
+    } else {
+      const double t2 = std::atan2(S[1], S[0]);
+      lat[pos] = std::fmod(6. * M_PI - lat[pos] - 2. * t2, 2. * M_PI);
+    }
+  }
+}
+
 // One overrelaxation pass (reference src/update.cu:84-98,
 // include/lattice_functions.h:83-89), optional freeze period ml.
 void o_overrelax(const OGeom *g, double *lat, int ml) {
@@ -283,6 +325,10 @@ void o_polyakov(const OGeom *g, const double *lat, double out[2]) {
   out[0] = re / (double)g->Vs;
   out[1] = im / (double)g->Vs;
 }
+
+// The fast division used by the sm_100a kernels' site decode (host build of
+// the same header), checked against '/' by tests/test_oracle_pin.py.
+uint32_t o_fastdiv(uint32_t n, uint32_t d) { return u1b::fast_div(n, u1b::make_fastdiv(d)); }
 
 double o_bessel_ratio(double x) { return std::cyl_bessel_i(1.0, x) / std::cyl_bessel_i(0.0, x); }
 

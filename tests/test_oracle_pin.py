@@ -102,6 +102,14 @@ def test_live_reference_cpu(dims, N, beta, aniso):
                 assert abs(o.multihit(lat_o, i, p) - r.multihit(lat_r, i, p)) < 1e-14
 
 
+@pytest.mark.parametrize("d", [1, 2, 3, 5, 6, 7, 12, 16, 24, 31, 48, 100, 1000, 65535, 123457, 2 ** 20 + 1])
+def test_fast_division_used_by_kernels(d):
+    rs = np.random.default_rng(d)
+    ns = np.concatenate([np.arange(0, 5000), rs.integers(0, 2 ** 31, 5000), [2 ** 31 - 1, 2 ** 31 - 2]])
+    for n in ns:
+        assert Oracle.fastdiv(int(n), d) == int(n) // d
+
+
 @pytest.mark.parametrize("x", [1e-4, 0.3, 1.0, 2.5, 6.0, 12.0, 24.0])
 def test_bessel_ratio(x):
     assert abs(Oracle.bessel_ratio(x) - special.iv(1, x) / special.iv(0, x)) < 1e-13
