@@ -436,19 +436,42 @@ extern "C" int u1_hot_start(u1_lattice *lat, u1_rng *rng) {
   return U1_OK;
 }
 
+// Launch one phase kernel with programmatic stream serialization (PDL): it
+// may be scheduled before the previous kernel on the stream finishes and
+// waits for it in-kernel (griddepcontrol.wait) before reading links.
+template <class K>
+static int launch_pdl(K kernel, int blocks, cudaStream_t s, const UpdArgs &a, const char *what) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)blocks);
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, a);
+  u1i::g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (e != cudaSuccess) return u1i::cuda_fail(e, what);
+  return U1_OK;
+}
+
+// Two sites per thread (k_update_pair) when N0/2 is even, else one.
 template <int D, int MU>
 static int launch_phase_mu(const UpdArgs &a, cudaStream_t s, bool met, bool replay) {
-  const int blocks = u1i::blocks_for(a.g.Vh, 256);
-  if (met) {
-    if (replay)
-      k_update<D, MU, true, true><<<blocks, 256, 0, s>>>(a);
-    else
-      k_update<D, MU, true, false><<<blocks, 256, 0, s>>>(a);
-  } else {
-    k_update<D, MU, false, false><<<blocks, 256, 0, s>>>(a);
+  if ((a.g.hN0 & 1) == 0) {
+    const int blocks = u1i::blocks_for(a.g.Vh / 2, 256);
+    if (met)
+      return replay ? launch_pdl(k_update_pair<D, MU, true, true>, blocks, s, a, "k_update_pair")
+                    : launch_pdl(k_update_pair<D, MU, true, false>, blocks, s, a, "k_update_pair");
+    return launch_pdl(k_update_pair<D, MU, false, false>, blocks, s, a, "k_update_pair");
   }
-  U1_LAUNCH_CHECK("k_update");
-  return U1_OK;
+  const int blocks = u1i::blocks_for(a.g.Vh, 256);
+  if (met)
+    return replay ? launch_pdl(k_update<D, MU, true, true>, blocks, s, a, "k_update")
+                  : launch_pdl(k_update<D, MU, true, false>, blocks, s, a, "k_update");
+  return launch_pdl(k_update<D, MU, false, false>, blocks, s, a, "k_update");
 }
 
 template <int D>

@@ -19,6 +19,15 @@ namespace u1b {
 
 __device__ __forceinline__ float2 ldg2(const float2 *p) { return __ldg(p); }
 
+// Programmatic dependent launch (sm_90+): phase kernels are launched with
+// programmatic stream serialization, so the next phase's CTAs are scheduled
+// while this phase drains.  Every such kernel waits for the previous grid
+// (completion and memory visibility) before touching links or counters, and
+// signals its dependents once its stores are issued.  Without the launch
+// attribute both instructions are no-ops.
+__device__ __forceinline__ void pdl_wait_prior_grid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_release_dependents() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+
 // Staple S of link (x, mu), x of parity p with EO index i_self, so that the
 // local action of the link is beta * Re(S * U_mu(x)).
 template <int D>
@@ -132,11 +141,12 @@ __device__ __forceinline__ float2 staple_steps(const float2 *__restrict__ lat, c
 // overrelaxation, REPLAY reads the shared-stream pairs instead of Philox.
 template <int D, int MU, bool MET, bool REPLAY>
 __global__ void __launch_bounds__(256) k_update(const UpdArgs a) {
-  if (!MET && a.bump_ptr != nullptr && blockIdx.x == 0 && threadIdx.x == 0) *a.bump_ptr += a.bump_by;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.g.Vh) return;
   int x[4], k;
   eo_decode_fast<D>(a.g, i, a.p, x, k);
+  pdl_wait_prior_grid();
+  if (!MET && a.bump_ptr != nullptr && blockIdx.x == 0 && threadIdx.x == 0) *a.bump_ptr += a.bump_by;
+  if (i >= a.g.Vh) return;
   // Multilevel freeze rule, reference src/multilevel.cu:41: update unless the
   // site lies on a frozen time slice (x_t multiple of ml, ml = 2 or 4) and
   // the link is spatial (the reference tests the literal direction index 3).
@@ -170,6 +180,122 @@ __global__ void __launch_bounds__(256) k_update(const UpdArgs a) {
   } else {
     *own = overrelax_link(S, U);
   }
+  pdl_release_dependents();
+}
+
+// ---------------------------------------------------------------------------
+// Two sites per thread.  When N0/2 is even, EO sites 2t and 2t+1 of a phase
+// lie in the same x0-row: their coordinates x1..x3, their x0 parity and
+// every step along x1..x3 are shared, and because those steps are even the
+// two neighbour links sit side by side at a 16-byte aligned address: one
+// 128-bit load serves both sites.  Steps along x0 are odd or differ at the
+// row end, so x0-shifted neighbours are loaded per site.
+struct Pair2 {
+  float2 s0, s1;
+};
+
+__device__ __forceinline__ Pair2 ld_vec2(const float2 *__restrict__ base, int idx) {
+  const float4 t = __ldg(reinterpret_cast<const float4 *>(base + idx));
+  return Pair2{make_float2(t.x, t.y), make_float2(t.z, t.w)};
+}
+__device__ __forceinline__ Pair2 ld_two(const float2 *__restrict__ base, int i0, int i1) {
+  return Pair2{__ldg(base + i0), __ldg(base + i1)};
+}
+
+// upper + lower staple contributions of one nu for both sites
+__device__ __forceinline__ void staple_term2(const Pair2 &a, const Pair2 &b, const Pair2 &c, const Pair2 &d,
+                                             const Pair2 &e, const Pair2 &f, float2 &acc0, float2 &acc1) {
+  acc0 = cadd(acc0, cadd(cmulc(cmulc(a.s0, b.s0), c.s0), cmul(cconjmul(d.s0, e.s0), f.s0)));
+  acc1 = cadd(acc1, cadd(cmulc(cmulc(a.s1, b.s1), c.s1), cmul(cconjmul(d.s1, e.s1), f.s1)));
+}
+
+template <int D, int MU, bool MET, bool REPLAY>
+__device__ __forceinline__ float2 update_one(const UpdArgs &a, int i, float2 S, float2 U) {
+  if (MET) {
+    const unsigned long long pass = *a.pass_dev + (unsigned long long)a.hit;
+    float2 Un;
+    float b;
+    if (REPLAY) {
+      const size_t pr = ((((size_t)(pass - a.replay_base) * 2 + a.p) * D + MU) * a.g.Vh + i) * 2;
+      double sn, cs;
+      sincos(a.replay[pr], &sn, &cs);
+      Un = make_float2((float)cs, (float)sn);
+      b = (float)a.replay[pr + 1];
+    } else {
+      Philox4 r = philox4x32_10((uint32_t)(a.p * a.g.Vh + i), u1_rng_word1(MU, U1_TAG_METROPOLIS, a.chain),
+                                (uint32_t)pass, (uint32_t)(pass >> 32), a.key0, a.key1);
+      const float u1 = u1_uniform_open(r.v[0]);
+      b = u1_uniform_open(r.v[1]);
+      float sn, cs;
+      sincospif(2.0f * u1, &sn, &cs);
+      Un = make_float2(cs, sn);
+    }
+    const float dS = a.c.beta * (cre_mul(S, Un) - cre_mul(S, U));
+    return (expf(dS) > b) ? Un : U;
+  }
+  return overrelax_link(S, U);
+}
+
+template <int D, int MU, bool MET, bool REPLAY>
+__global__ void __launch_bounds__(256, 8) k_update_pair(const UpdArgs a) {
+  const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  int x[4], k;
+  eo_decode_fast<D>(a.g, i, a.p, x, k);
+  pdl_wait_prior_grid();
+  if (!MET && a.bump_ptr != nullptr && blockIdx.x == 0 && threadIdx.x == 0) *a.bump_ptr += a.bump_by;
+  if (i >= a.g.Vh) return;
+  if (MU != 3 && a.ml > 0 && (x[D - 1] & (a.ml - 1)) == 0) return;  // freeze rule, src/multilevel.cu:41
+  int fwd[4], bwd[4];
+  eo_steps<D>(a.g, x, k, fwd, bwd);  // steps of site i; site i+1 shares those along x1..x3
+  // x0 steps of the two sites: x0 = 2k+odd and 2k+2+odd
+  const int odd = x[0] & 1;
+  const int f0a = fwd[0], b0a = bwd[0];
+  const int f0b = odd ? ((k + 1 == a.g.hN0 - 1) ? a.g.wrapf[0] : 1) : 0;
+  const int b0b = odd ? 0 : -1;
+  const int q = 1 - a.p;
+  const int V = a.g.V, Vh = a.g.Vh;
+  const float2 *lat = a.lat;
+  const float2 *Lq_mu = lat + MU * V + q * Vh;
+  float2 ss0 = make_float2(0.f, 0.f), ss1 = ss0, st0 = ss0, st1 = ss0;
+#pragma unroll
+  for (int nu = 0; nu < D; ++nu) {
+    if (nu == MU) continue;
+    const float2 *Lp_nu = lat + nu * V + a.p * Vh;
+    const float2 *Lq_nu = lat + nu * V + q * Vh;
+    Pair2 A, B, C, Dd, E, F;
+    C = ld_vec2(Lp_nu, i);
+    if (MU == 0) {  // nu != 0: steps along nu shared, along x0 per site
+      A = ld_two(Lq_nu, i + f0a, i + 1 + f0b);
+      B = ld_vec2(Lq_mu, i + fwd[nu]);
+      Dd = ld_two(Lp_nu, i + f0a + bwd[nu], i + 1 + f0b + bwd[nu]);
+      E = ld_vec2(Lq_mu, i + bwd[nu]);
+      F = ld_vec2(Lq_nu, i + bwd[nu]);
+    } else if (nu == 0) {  // MU != 0
+      A = ld_vec2(Lq_nu, i + fwd[MU]);
+      B = ld_two(Lq_mu, i + f0a, i + 1 + f0b);
+      Dd = ld_two(Lp_nu, i + fwd[MU] + b0a, i + 1 + fwd[MU] + b0b);
+      E = ld_two(Lq_mu, i + b0a, i + 1 + b0b);
+      F = ld_two(Lq_nu, i + b0a, i + 1 + b0b);
+    } else {  // MU != 0, nu != 0: every step even, all loads 128-bit
+      A = ld_vec2(Lq_nu, i + fwd[MU]);
+      B = ld_vec2(Lq_mu, i + fwd[nu]);
+      Dd = ld_vec2(Lp_nu, i + fwd[MU] + bwd[nu]);
+      E = ld_vec2(Lq_mu, i + bwd[nu]);
+      F = ld_vec2(Lq_nu, i + bwd[nu]);
+    }
+    if (MU == D - 1 || nu == D - 1)
+      staple_term2(A, B, C, Dd, E, F, st0, st1);
+    else
+      staple_term2(A, B, C, Dd, E, F, ss0, ss1);
+  }
+  const float2 S0 = cadd(cscale(ss0, a.c.w_ss), cscale(st0, a.c.w_st));
+  const float2 S1 = cadd(cscale(ss1, a.c.w_ss), cscale(st1, a.c.w_st));
+  float4 *own = reinterpret_cast<float4 *>(a.lat + MU * V + a.p * Vh + i);
+  const float4 U = *own;
+  const float2 N0 = update_one<D, MU, MET, REPLAY>(a, i, S0, make_float2(U.x, U.y));
+  const float2 N1 = update_one<D, MU, MET, REPLAY>(a, i + 1, S1, make_float2(U.z, U.w));
+  *own = make_float4(N0.x, N0.y, N1.x, N1.y);
+  pdl_release_dependents();
 }
 
 // Hot start (reference src/update.cu:30-48): every link gets

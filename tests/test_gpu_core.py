@@ -114,8 +114,11 @@ def test_pass_golden_statistics(ctx, name):
     assert np.median(diff) < 1e-6 and np.mean(diff < ANGLE_TOL) > 0.95 and diff.max() < 5e-3
 
 
+# N0/2 even runs the two-sites-per-thread kernel, N0/2 odd the one-site kernel
 @pytest.mark.parametrize("dims,N,beta,aniso", [(4, (8, 8, 8, 8), 1.0, 1.0), (4, (4, 6, 6, 8), 1.1, 2.0),
-                                                (3, (8, 6, 0, 8), 2.0, 1.5), (2, (16, 0, 0, 16), 4.0, 1.0)])
+                                                (4, (6, 6, 4, 8), 1.0, 1.0), (3, (8, 6, 0, 8), 2.0, 1.5),
+                                                (3, (10, 4, 0, 6), 1.5, 1.0), (2, (16, 0, 0, 16), 4.0, 1.0),
+                                                (2, (14, 0, 0, 10), 3.0, 1.0)])
 @pytest.mark.parametrize("start", ["hot", "thermalised"])
 def test_five_sweeps_every_phase_shared_stream(ctx, dims, N, beta, aniso, start):
     """Five sweeps of 1 Metropolis + 4 OR with a shared (replayed) stream:
