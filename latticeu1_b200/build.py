@@ -42,6 +42,7 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
     """Compile every CUDA source into one shared library; returns its path."""
     LIBDIR.mkdir(exist_ok=True)
     deps = sources() + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + [ROOT / "include" / "u1_b200.h"]
+    deps += sorted((PKG / "shim").rglob("*.cpp")) + sorted((PKG / "shim").rglob("*.h"))
     if not force and not _stale(LIB, deps):
         return LIB
     objdir = LIBDIR / "obj"
@@ -63,7 +64,27 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
+    build_shim(verbose=verbose)
     return LIB
+
+
+SHIM = PKG / "shim"
+SHIM_LIB = LIBDIR / "libu1shim.so"
+
+
+def build_shim(verbose: bool = False) -> Path:
+    """The drop-in C++ API of the reference driver (namespace U1) over the
+    C ABI: latticeu1_b200/lib/libu1shim.so, linked against libu1b200.so."""
+    gxx = shutil.which("g++") if Path("/usr/bin/g++").exists() is False else "/usr/bin/g++"
+    tmp = SHIM_LIB.with_suffix(".so.tmp")
+    cmd = [gxx, "-std=c++17", "-O2", "-fPIC", "-shared", "-I" + str(SHIM / "include"),
+           "-I" + str(ROOT / "include")] + [str(p) for p in sorted(SHIM.glob("*.cpp"))] + [
+           "-L" + str(LIBDIR), "-lu1b200", "-Wl,-rpath,$ORIGIN", "-o", str(tmp)]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, SHIM_LIB)
+    return SHIM_LIB
 
 
 if __name__ == "__main__":

@@ -1,0 +1,116 @@
+"""The reference's OWN CUDA build (compiled in place into oracle/_ref) run on
+the same B200 as the sm_100a kernels: results on identical configurations,
+and throughput of its UpdateLattice on the 32^4 workload.
+
+Deterministic comparisons (no RNG involved): the fused measurement, one
+overrelaxation pass, Poly2 (plain and multihit) and MultiLevel with no
+updates (metrop = ovrn = 0), which pins the multilevel tensor contraction
+to the reference implementation itself.
+"""
+import json
+import os
+import time
+
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle, Ref, wrap_diff
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not Ref.available(), reason="oracle/_ref not built (reference sources absent)")]
+
+
+def _inputs(dims, N, beta, aniso, lat, **kw):
+    return dict(dims=dims, N=np.array(list(N) + [0] * (4 - len(N))), beta=beta, aniso=aniso, lat=lat, **kw)
+
+
+@pytest.fixture(scope="module")
+def ref_gpu():
+    from oracle import ref_gpu
+    return ref_gpu
+
+
+@pytest.mark.parametrize("dims,N,beta,aniso", [(4, (8, 6, 6, 8), 1.0, 1.0), (4, (6, 6, 6, 8), 0.9, 2.0),
+                                                (3, (8, 8, 0, 6), 2.0, 1.0)])
+def test_measure_or_poly2_vs_reference_cuda(ctx, ref_gpu, dims, N, beta, aniso):
+    from latticeu1_b200 import Lattice, Rng
+    lat = Lattice(ctx, dims, N, beta, aniso)
+    o = Oracle(dims, N, beta, aniso)
+    th = np.random.default_rng(dims).uniform(0, 2 * np.pi, lat.nlinks) * 0.5
+    lat.import_angles(th)
+    th = lat.export_angles()  # exactly the configuration the GPU holds
+    r = ref_gpu.run("measure", _inputs(dims, N, beta, aniso, th))["m"]
+    m = lat.measure()
+    got = np.array([m["plaq_ss"].real, m["plaq_ss"].imag, m["plaq_st"].real, m["plaq_st"].imag, m["poly"].real,
+                    m["poly"].imag])
+    if dims == 2:
+        got, r = got[2:], r[2:]
+    np.testing.assert_allclose(got, r, rtol=0, atol=2e-6)
+    ref_or = ref_gpu.run("or_pass", _inputs(dims, N, beta, aniso, th, passes=1))["lat"]
+    lat.update(Rng(ctx, 1), 0, 1)
+    diff = wrap_diff(lat.export_angles(), ref_or)
+    # whole pass: same bound as the golden pass (ill-conditioned links with
+    # tiny |S| spread their FP32 error to links updated later in the pass)
+    assert np.median(diff) < 1e-6 and np.mean(diff < 1e-5) > 0.95 and diff.max() < 5e-3, (diff.max(),
+                                                                                           np.mean(diff < 1e-5))
+    lat.import_angles(th)
+    c = ref_gpu.run("poly2", _inputs(dims, N, beta, aniso, th))
+    for mh in (0, 1):
+        want = c[f"c{mh}"][0::2] + 1j * c[f"c{mh}"][1::2]
+        got = lat.poly_corr(bool(mh))
+        np.testing.assert_allclose(got, want, rtol=0, atol=3e-5 * np.abs(want).max())
+
+
+def test_multilevel_vs_reference_cuda(ctx, ref_gpu):
+    from latticeu1_b200 import Lattice, Rng
+    dims, N, beta = 4, (6, 4, 4, 8), 1.1
+    lat = Lattice(ctx, dims, N, beta)
+    th = np.random.default_rng(3).uniform(0, 2 * np.pi, lat.nlinks) * 0.4
+    lat.import_angles(th)
+    th = lat.export_angles()
+    args = np.array([2, 1, 3, 1, 0, 0])
+    c = ref_gpu.run("multilevel", _inputs(dims, N, beta, 1.0, th, args=args))["c"]
+    want = c[0::2] + 1j * c[1::2]
+    got = lat.multilevel(Rng(ctx, 1), *[int(a) for a in args])
+    np.testing.assert_allclose(got, want, rtol=1e-4, atol=1e-6 * np.abs(want).max())
+
+
+def test_throughput_vs_reference_cuda(ctx, ref_gpu):
+    """UpdateLattice(1 Metropolis + 4 OR) at 32^4 on the same B200: the
+    reference's CUDA build (FP64, after its own autotuning in the warm-up)
+    against the sm_100a path through the Python host layer."""
+    import torch
+
+    from latticeu1_b200 import Lattice, Rng
+    L = 32
+    sweeps = 20
+    lat = Lattice(ctx, 4, (L, L, L, L), 1.0)
+    rng = Rng(ctx, 7)
+    lat.hot_start(rng)
+    th = lat.export_angles()
+    r = ref_gpu.run("timing", _inputs(4, (L, L, L, L), 1.0, 1.0, th, warmup=3, sweeps=sweeps, metrop=1, ovrn=4))
+    ref_ms = float(r["ms"][0]) / sweeps
+    for _ in range(3):
+        lat.update(rng, 1, 4)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s = torch.cuda.Stream()
+    lat.set_stream(s.cuda_stream)
+    with torch.cuda.stream(s):
+        lat.update(rng, 1, 4)
+        e0.record(s)
+        for _ in range(sweeps):
+            lat.update(rng, 1, 4)
+        e1.record(s)
+        s.synchronize()
+    ours_ms = e0.elapsed_time(e1) / sweeps
+    lu = L ** 4 * 4 * 5
+    result = {"workload": "32^4 beta=1 UpdateLattice(1 Metropolis + 4 OR)", "reference_cuda_ms_per_sweep": ref_ms,
+              "reference_cuda_link_updates_per_s": lu / (ref_ms * 1e-3), "ours_ms_per_sweep": ours_ms,
+              "ours_link_updates_per_s": lu / (ours_ms * 1e-3), "speedup": ref_ms / ours_ms}
+    print(json.dumps(result))
+    out = os.environ.get("U1_REF_TIMING_OUT")
+    if out:
+        with open(out, "w") as f:
+            json.dump(result, f, indent=1)
+    assert ours_ms < ref_ms, result
