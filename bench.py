@@ -224,9 +224,8 @@ def run_ours(args) -> None:
     import numpy as np
     import torch
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from latticeu1_b200 import replicas
+    rank, world, local = replicas.world()
     dist = None
     if world > 1:
         import datetime
@@ -243,7 +242,8 @@ def run_ours(args) -> None:
     lat = Lattice(ctx, DIMS, (L, L, L, L), BETA)
     stream = torch.cuda.Stream()
     lat.set_stream(stream.cuda_stream)
-    rng = Rng(ctx, 1234 + 7919 * rank)
+    rng = Rng(ctx, 1234)
+    rng.set_chain(replicas.chain_id(rank))  # independent replica per rank
     flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device="cuda")
     obs = torch.zeros((args.steps + args.warmup, 6), dtype=torch.float64, device="cuda")
     lu = link_updates_per_step(L)
@@ -291,10 +291,7 @@ def run_ours(args) -> None:
             clk["window"] = f"timed region + {CLOCK_WINDOW_S:.1f} s of the same step"
     upd_ms = sum(e[0].elapsed_time(e[1]) for e in ev)
     step_ms = sum(e[0].elapsed_time(e[2]) for e in ev)
-    tot = torch.tensor([step_ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
-    step_ms_max = float(tot.item())
+    step_ms_max = replicas.max_over_ranks(step_ms)
     value = world * args.steps * lu / (step_ms_max * 1e-3)
 
     # e2e: C ABI with host buffers (configuration in pinned host memory)
@@ -311,13 +308,11 @@ def run_ours(args) -> None:
             lat.export_angles(host.numpy())
         torch.cuda.synchronize()
         e2e_s = time.perf_counter() - t0
-    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_value = world * e2e_steps * lu / float(e2e_t.item())
+    e2e_value = world * e2e_steps * lu / replicas.max_over_ranks(e2e_s)
     bytes_cfg = lat.nlinks * 8
 
     ob = obs[args.warmup:].cpu().numpy()
+    per_chain = replicas.gather_observables([float(ob[:, 0].mean()), float(ob[:, 2].mean())])
     if rank == 0:
         peak, peak_kind = measured_peak()
         upd_launches = 2 * DIMS * (METROP + OVRN)
@@ -344,7 +339,8 @@ def run_ours(args) -> None:
             "wall_s_timed_region": t_wall,
             "update_ms_per_step": upd_ms / args.steps,
             "observables": {"plaq_ss_re": float(ob[:, 0].mean()), "plaq_st_re": float(ob[:, 2].mean()),
-                            "abs_L": float(np.abs(ob[:, 4] + 1j * ob[:, 5]).mean())},
+                            "abs_L": float(np.abs(ob[:, 4] + 1j * ob[:, 5]).mean()),
+                            "per_chain_plaq_ss_st": per_chain},
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_reference_rate(L, args.cpu_budget)

@@ -101,6 +101,10 @@ int u1_rng_create(u1_ctx *ctx, uint64_t seed, u1_rng **out);
 int u1_rng_destroy(u1_rng *rng);
 int u1_rng_get_state(const u1_rng *rng, uint64_t *seed, uint64_t *pass);
 int u1_rng_set_state(u1_rng *rng, uint64_t seed, uint64_t pass);
+/* Chain number (0..65535) folded into every Philox counter: independent
+ * chains (one per GPU, or per lattice of a batch) share a seed and still
+ * draw disjoint streams. */
+int u1_rng_set_chain(u1_rng *rng, uint32_t chain);
 /* Test-only shared-stream mode: Metropolis passes read (new_theta, b) pairs
  * from `pairs` (host FP64, 2 values per link) in the reference's draw order
  * pass -> parity -> mu -> id (reference src/update.cu:51-79, 305-308).

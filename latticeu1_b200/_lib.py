@@ -54,6 +54,7 @@ SIGNATURES = {
     "u1_rng_destroy": [_vp],
     "u1_rng_get_state": [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)],
     "u1_rng_set_state": [_vp, C.c_uint64, C.c_uint64],
+    "u1_rng_set_chain": [_vp, C.c_uint32],
     "u1_rng_set_replay": [_vp, _vp, C.c_size_t],
     "u1_rng_debug_uniforms": [_vp, _vp, C.c_uint64, _i, _i, _vp],
     "u1_hot_start": [_vp, _vp],

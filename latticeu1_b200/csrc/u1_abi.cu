@@ -376,6 +376,13 @@ extern "C" int u1_rng_set_state(u1_rng *rng, uint64_t seed, uint64_t pass) {
   return U1_OK;
 }
 
+extern "C" int u1_rng_set_chain(u1_rng *rng, uint32_t chain) {
+  if (!rng) return fail(U1_ERR_INVALID, "u1_rng_set_chain: null rng");
+  if (chain > 0xFFFFu) return fail(U1_ERR_INVALID, "u1_rng_set_chain: chain must be < 65536");
+  rng->chain = chain;
+  return U1_OK;
+}
+
 extern "C" int u1_rng_set_replay(u1_rng *rng, const double *pairs, size_t n_pairs) {
   if (!rng) return fail(U1_ERR_INVALID, "u1_rng_set_replay: null rng");
   U1_CUDA_TRY(cudaSetDevice(rng->ctx->device));
@@ -576,7 +583,7 @@ extern "C" int u1_update(u1_lattice *lat, u1_rng *rng, int metrop, int ovrn) {
   if (rc) return rc;
   const bool replay = rng->replay_dev != nullptr;
   if (lat->use_graphs && !replay) {
-    auto key = std::make_tuple(metrop, ovrn, rng->id, rng->seed);
+    auto key = std::make_tuple(metrop, ovrn, rng->id, rng->seed ^ ((uint64_t)rng->chain << 48));
     auto it = lat->graphs.find(key);
     if (it == lat->graphs.end()) {
       cudaGraphExec_t ex = nullptr;

@@ -79,6 +79,10 @@ class Rng:
     def set_state(self, seed: int, pass_: int) -> None:
         check(lib.u1_rng_set_state(self._h, C.c_uint64(seed), C.c_uint64(pass_)), "u1_rng_set_state")
 
+    def set_chain(self, chain: int) -> None:
+        """Chain number in every Philox counter (independent streams per chain)."""
+        check(lib.u1_rng_set_chain(self._h, C.c_uint32(chain)), "u1_rng_set_chain")
+
     def set_replay(self, pairs: np.ndarray | None) -> None:
         """Shared-stream test mode: pairs[..., 2] = (new theta, b) per link in
         the reference's draw order pass -> parity -> mu -> id."""
