@@ -252,10 +252,9 @@ def run_ours(args) -> None:
         lat.hot_start(rng)
         for w in range(args.warmup):
             flush.zero_()
-            lat.update(rng, METROP, OVRN)
-            lat.measure_async(obs[w].data_ptr())
+            lat.update_measure(rng, METROP, OVRN, obs[w].data_ptr())
         stream.synchronize()
-        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
@@ -268,10 +267,8 @@ def run_ours(args) -> None:
         for k in range(args.steps):
             flush.zero_()
             ev[k][0].record(stream)
-            lat.update(rng, METROP, OVRN)
+            lat.update_measure(rng, METROP, OVRN, obs[args.warmup + k].data_ptr())
             ev[k][1].record(stream)
-            lat.measure_async(obs[args.warmup + k].data_ptr())
-            ev[k][2].record(stream)
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
@@ -283,19 +280,19 @@ def run_ours(args) -> None:
         t1 = time.perf_counter()
         while time.perf_counter() - t1 < CLOCK_WINDOW_S:
             for _ in range(20):
-                lat.update(rng, METROP, OVRN)
-                lat.measure_async(obs[0].data_ptr())
+                lat.update_measure(rng, METROP, OVRN, obs[0].data_ptr())
             stream.synchronize()
         clk = clocks.stop()
         if clk is not None:
             clk["window"] = f"timed region + {CLOCK_WINDOW_S:.1f} s of the same step"
-    upd_ms = sum(e[0].elapsed_time(e[1]) for e in ev)
-    step_ms = sum(e[0].elapsed_time(e[2]) for e in ev)
+    step_ms = sum(e[0].elapsed_time(e[1]) for e in ev)
+    upd_ms = step_ms  # the measurement runs inside the sweep's last phase
     step_ms_max = replicas.max_over_ranks(step_ms)
     value = world * args.steps * lu / (step_ms_max * 1e-3)
 
     # e2e: C ABI with host buffers (configuration in pinned host memory)
     host = torch.empty(lat.nlinks, dtype=torch.float64, pin_memory=True)
+    e2e_obs = torch.zeros(6, dtype=torch.float64, device="cuda")
     lat.export_angles(host.numpy())
     e2e_steps = max(3, min(args.steps, 10))
     with torch.cuda.stream(stream):
@@ -303,8 +300,8 @@ def run_ours(args) -> None:
         t0 = time.perf_counter()
         for _ in range(e2e_steps):
             lat.import_angles(host.numpy())
-            lat.update(rng, METROP, OVRN)
-            m = lat.measure()
+            lat.update_measure(rng, METROP, OVRN, e2e_obs.data_ptr())
+            m = e2e_obs.cpu()  # D2H of the step's observables
             lat.export_angles(host.numpy())
         torch.cuda.synchronize()
         e2e_s = time.perf_counter() - t0
@@ -315,7 +312,7 @@ def run_ours(args) -> None:
     per_chain = replicas.gather_observables([float(ob[:, 0].mean()), float(ob[:, 2].mean())])
     if rank == 0:
         peak, peak_kind = measured_peak()
-        upd_launches = 2 * DIMS * (METROP + OVRN)
+        upd_launches = 2 * DIMS * (METROP + OVRN)  # the last one also measures
         avg_launch_s = upd_ms * 1e-3 / (args.steps * upd_launches)
         alg_bytes = algorithmic_bytes_per_link_update(DIMS) * (L ** DIMS) // 2
         achieved = alg_bytes / avg_launch_s / 1e9
@@ -325,15 +322,15 @@ def run_ours(args) -> None:
             "warmup": args.warmup, "ms_per_step": step_ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": workload_config(L),
-            "roofline": {"bound": "hbm", "kernel": "k_update (one (parity,mu) phase)",
+            "roofline": {"bound": "hbm", "kernel": "k_update_pair (one (parity,mu) phase; step average)",
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "avg_launch_us": avg_launch_s * 1e6},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_cfg,
                     "d2h_bytes_per_step": bytes_cfg + 48,
-                    "path": "u1_lattice_import_angles(pinned host FP64) + u1_update + u1_measure + "
-                            "u1_lattice_export_angles(pinned host FP64) per step"},
+                    "path": "u1_lattice_import_angles(pinned host FP64) + u1_update_measure + D2H of the "
+                            "6 observables + u1_lattice_export_angles(pinned host FP64) per step"},
             "gpu_launches": int(launches),
             "clocks": clk,
             "wall_s_timed_region": t_wall,
@@ -351,6 +348,48 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
+def run_multilevel(args) -> None:
+    """Multilevel Polyakov correlator, 24^3 x 32 at beta = 0.95, level-2
+    slabs of thickness 2 and level-4 slabs of 4, 1 Metropolis + 4 OR per
+    sub-update, analytic multihit on temporal links.  A step is one level-4
+    iteration (k4 = 1 update + n2 level-2 sub-updates + T4 accumulation);
+    the value is level-2 sub-updates per second.  The full configuration
+    (n4 = 100, n2 = 200) is timed by extrapolating the per-step time; the
+    single-level multihit estimator (Poly2) is timed beside it."""
+    import torch
+
+    from latticeu1_b200 import Context, Lattice, Rng
+    ctx = Context(0)
+    lat = Lattice(ctx, 4, (24, 24, 24, 32), 0.95)
+    rng = Rng(ctx, 1234)
+    lat.hot_start(rng)
+    for _ in range(50):
+        lat.update(rng, METROP, OVRN)
+    n2 = args.n2
+    lat.multilevel(rng, 1, 1, 2, 1, METROP, OVRN)  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    c_ml = lat.multilevel(rng, args.steps, 1, n2, 1, METROP, OVRN)
+    el = time.perf_counter() - t0
+    sub = args.steps * n2
+    t1 = time.perf_counter()
+    nsl = 0
+    while time.perf_counter() - t1 < el:
+        lat.update(rng, METROP, OVRN)
+        c_sl = lat.poly_corr(True)
+        nsl += 1
+    line = {"metric": "multilevel level-2 sub-updates/s (24^3x32, beta=0.95)", "value": sub / el,
+            "unit": "sub-updates/s", "n_gpus": 1, "steps": args.steps, "warmup": 1,
+            "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "dtype": "f32+f64 accum",
+            "data": "synthetic", "config": {"workload": "MultiLevel(n4=steps, k4=1, n2, k2=1, metrop=1, ovrn=4)",
+                                           "lattice": "24^3x32", "beta": 0.95, "n2": n2},
+            "full_config_seconds_n4_100_n2_200": el / sub * 100 * 200,
+            "C_r_multilevel": [[float(c.real), float(c.imag)] for c in c_ml[:6]],
+            "single_level_equal_time": {"configs": nsl, "C_r_last": [[float(c.real), float(c.imag)]
+                                                                     for c in c_sl[:6]]}}
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -360,11 +399,15 @@ def main() -> None:
     ap.add_argument("--L", type=int, default=L_DEFAULT)
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU baseline sampling")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["update32", "multilevel"], default="update32")
+    ap.add_argument("--n2", type=int, default=200, help="level-2 sub-updates per step (multilevel)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "multilevel":
+        run_multilevel(args)
     else:
         run_ours(args)
 

@@ -126,6 +126,14 @@ int u1_hot_start(u1_lattice *lat, u1_rng *rng);
  * 383-386).  Asynchronous on the lattice's stream. */
 int u1_update(u1_lattice *lat, u1_rng *rng, int metrop, int ovrn);
 
+/* u1_update followed by the plaquette + Polyakov measurement of the new
+ * configuration (the reference driver's UpdateLattice then Plaquette and
+ * Polyakov, u1.cpp:120-126), with the measurement fused into the sweep's
+ * last phase: dev_out (device, 6 doubles) receives {SS re, SS im, ST re,
+ * ST im, L re, L im} as u1_measure.  The links are bit-identical to
+ * u1_update.  Asynchronous. */
+int u1_update_measure(u1_lattice *lat, u1_rng *rng, int metrop, int ovrn, double *dev_out);
+
 /* Test and debugging aid: run exactly one (parity, mu) phase of a
  * Metropolis (metropolis != 0) or overrelaxation pass, with the Metropolis
  * numbers of pass (rng pass counter + hit).  The pass counter is not
@@ -149,7 +157,7 @@ int u1_measure_async(u1_lattice *lat, double *dev_out);
  * callers that cannot allocate device memory (e.g. code confined to memory
  * handed out by its host framework, or loops where a cudaMalloc that may
  * synchronise the device is not acceptable).  It allocates nothing: its
- * scratch is a fixed file-scope device array of about 192 KiB that every GPU
+ * scratch is a fixed file-scope device array of about 384 KiB that every GPU
  * loading the library keeps until exit.  links_dev: the V*dims float2 links
  * (this library's layout); out_dev: 6 doubles, as u1_measure; stream:
  * cudaStream_t as void* on the current device.  Lattices with V/2 above

@@ -60,6 +60,7 @@ SIGNATURES = {
     "u1_hot_start": [_vp, _vp],
     "u1_update": [_vp, _vp, _i, _i],
     "u1_update_phase": [_vp, _vp, _i, _i, _i, _i],
+    "u1_update_measure": [_vp, _vp, _i, _i, _vp],
     "u1_plaquette": [_vp, _dp],
     "u1_polyakov": [_vp, _dp],
     "u1_measure": [_vp, _dp],

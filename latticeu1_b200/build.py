@@ -47,7 +47,10 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
         return LIB
     objdir = LIBDIR / "obj"
     objdir.mkdir(exist_ok=True)
-    flags = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+    # -fmad=false: no compiler-chosen multiply-add contraction, so the
+    # one-site, two-site and fused-measurement update kernels round every
+    # link update identically (FMAs are written out where wanted).
+    flags = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC",
                     "-I" + str(ROOT / "include"), "-I" + str(CSRC),
                     "--expt-relaxed-constexpr"] + (extra or [])
     objs = []

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "u1_internal.h"
+#include "u1_fused.cuh"
 #include "u1_multilevel.cuh"
 
 using namespace u1b;
@@ -496,9 +497,37 @@ static int launch_phase(const UpdArgs &a, cudaStream_t s, bool met, bool replay)
   return fail(U1_ERR_INVALID, "k_update: direction out of range");
 }
 
+template <int D, bool MET>
+static int launch_fused_last(const UpdArgs &a, cudaStream_t s, u1_lattice *lat, double *out) {
+  const GeomK &g = a.g;
+  int nSS = 0, nST = 0;
+  for (int mu = 0; mu < D - 1; ++mu)
+    for (int nu = mu + 1; nu < D; ++nu) (nu == D - 1 ? nST : nSS)++;
+  const double normSS = 1.0 / ((double)g.V * nSS), normST = 1.0 / ((double)g.V * nST);
+  const double normL = 1.0 / (double)g.Vs;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)fused_blocks(g));
+  cfg.blockDim = dim3(kFusedThreads);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaError_t e = cudaLaunchKernelEx(&cfg, k_update_last_measure<D, MET>, a, fused_chunks(g), lat->partials,
+                                     lat->counter, out, normSS, normST, normL);
+  u1i::g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (e != cudaSuccess) return u1i::cuda_fail(e, "k_update_last_measure");
+  return U1_OK;
+}
+
 // Issue one sweep (metrop Metropolis + ovrn overrelaxation passes) on links
 // `links` with freeze period ml.  The device pass counter advances by metrop.
-static int issue_sweep(u1_lattice *lat, float2 *links, u1_rng *rng, int metrop, int ovrn, int ml) {
+// fused_out != nullptr: the sweep's last phase is the fused update +
+// measurement kernel writing the 6 observables to fused_out (needs the
+// lattice scratch sized by ensure_scratch for fused_blocks).
+static int issue_sweep(u1_lattice *lat, float2 *links, u1_rng *rng, int metrop, int ovrn, int ml,
+                       double *fused_out = nullptr) {
   UpdArgs a{};
   a.lat = links;
   a.g = lat->g;
@@ -512,15 +541,29 @@ static int issue_sweep(u1_lattice *lat, float2 *links, u1_rng *rng, int metrop, 
   a.ml = ml;
   const bool replay = rng->replay_dev != nullptr;
   const int D = lat->g.dims;
+  const int total = 2 * D * (metrop + ovrn);
+  int phase = 0;
+  auto launch = [&](bool met) -> int {
+    ++phase;
+    if (fused_out && phase == total) {
+      if (met) return D == 2 ? launch_fused_last<2, true>(a, lat->stream, lat, fused_out)
+                     : D == 3 ? launch_fused_last<3, true>(a, lat->stream, lat, fused_out)
+                              : launch_fused_last<4, true>(a, lat->stream, lat, fused_out);
+      return D == 2 ? launch_fused_last<2, false>(a, lat->stream, lat, fused_out)
+           : D == 3 ? launch_fused_last<3, false>(a, lat->stream, lat, fused_out)
+                    : launch_fused_last<4, false>(a, lat->stream, lat, fused_out);
+    }
+    return D == 2 ? launch_phase<2>(a, lat->stream, met, met && replay)
+         : D == 3 ? launch_phase<3>(a, lat->stream, met, met && replay)
+                  : launch_phase<4>(a, lat->stream, met, met && replay);
+  };
   for (int m = 0; m < metrop; ++m)
     for (int p = 0; p < 2; ++p)
       for (int mu = 0; mu < D; ++mu) {
         a.p = p;
         a.mu = mu;
         a.hit = m;
-        int rc = D == 2 ? launch_phase<2>(a, lat->stream, true, replay)
-                        : D == 3 ? launch_phase<3>(a, lat->stream, true, replay)
-                                 : launch_phase<4>(a, lat->stream, true, replay);
+        int rc = launch(true);
         if (rc) return rc;
       }
   bool bumped = (metrop == 0);
@@ -533,9 +576,7 @@ static int issue_sweep(u1_lattice *lat, float2 *links, u1_rng *rng, int metrop, 
         a.bump_ptr = bumped ? nullptr : rng->pass_dev;
         a.bump_by = (unsigned)metrop;
         bumped = true;
-        int rc = D == 2 ? launch_phase<2>(a, lat->stream, false, false)
-                        : D == 3 ? launch_phase<3>(a, lat->stream, false, false)
-                                 : launch_phase<4>(a, lat->stream, false, false);
+        int rc = launch(false);
         if (rc) return rc;
       }
   if (!bumped) {
@@ -574,30 +615,58 @@ static int capture_graph(u1_lattice *lat, F fn, cudaGraphExec_t *exec) {
   return U1_OK;
 }
 
-extern "C" int u1_update(u1_lattice *lat, u1_rng *rng, int metrop, int ovrn) {
-  if (!lat || !rng) return fail(U1_ERR_INVALID, "u1_update: null argument");
-  if (metrop < 0 || ovrn < 0) return fail(U1_ERR_INVALID, "u1_update: negative pass count");
-  if (metrop == 0 && ovrn == 0) return U1_OK;
+static int update_impl(u1_lattice *lat, u1_rng *rng, int metrop, int ovrn, double *fused_out) {
   U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
   int rc = check_replay(lat, rng, metrop);
   if (rc) return rc;
   const bool replay = rng->replay_dev != nullptr;
   if (lat->use_graphs && !replay) {
-    auto key = std::make_tuple(metrop, ovrn, rng->id, rng->seed ^ ((uint64_t)rng->chain << 48));
+    // graph key: passes, rng object, seed/chain and whether the last phase is fused
+    auto key = std::make_tuple(metrop * 2 + (fused_out ? 1 : 0), ovrn, rng->id,
+                               rng->seed ^ ((uint64_t)rng->chain << 48));
     auto it = lat->graphs.find(key);
     if (it == lat->graphs.end()) {
       cudaGraphExec_t ex = nullptr;
-      rc = capture_graph(lat, [&]() { return issue_sweep(lat, lat->links, rng, metrop, ovrn, 0); }, &ex);
+      rc = capture_graph(lat, [&]() { return issue_sweep(lat, lat->links, rng, metrop, ovrn, 0, fused_out); },
+                         &ex);
       if (rc) return rc;
       it = lat->graphs.emplace(key, ex).first;
     }
     U1_CUDA_TRY(cudaGraphLaunch(it->second, lat->stream));
     u1i::g_launches += (unsigned long long)(2 * lat->g.dims * (metrop + ovrn) + (ovrn == 0 ? 1 : 0));
   } else {
-    rc = issue_sweep(lat, lat->links, rng, metrop, ovrn, 0);
+    rc = issue_sweep(lat, lat->links, rng, metrop, ovrn, 0, fused_out);
     if (rc) return rc;
   }
   rng->pass += (uint64_t)metrop;
+  return U1_OK;
+}
+
+extern "C" int u1_update(u1_lattice *lat, u1_rng *rng, int metrop, int ovrn) {
+  if (!lat || !rng) return fail(U1_ERR_INVALID, "u1_update: null argument");
+  if (metrop < 0 || ovrn < 0) return fail(U1_ERR_INVALID, "u1_update: negative pass count");
+  if (metrop == 0 && ovrn == 0) return U1_OK;
+  return update_impl(lat, rng, metrop, ovrn, nullptr);
+}
+
+static int measure_dispatch(u1_lattice *lat, double *dev_out);
+
+extern "C" int u1_update_measure(u1_lattice *lat, u1_rng *rng, int metrop, int ovrn, double *dev_out) {
+  if (!lat || !rng || !dev_out) return fail(U1_ERR_INVALID, "u1_update_measure: null argument");
+  if (metrop < 0 || ovrn < 0) return fail(U1_ERR_INVALID, "u1_update_measure: negative pass count");
+  U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
+  if ((metrop == 0 && ovrn == 0) || rng->replay_dev != nullptr) {
+    // nothing to fuse with (or the test-only replay stream): update, then measure
+    int rc = (metrop || ovrn) ? u1_update(lat, rng, metrop, ovrn) : U1_OK;
+    if (rc) return rc;
+    return measure_dispatch(lat, dev_out);
+  }
+  int rc = u1i::ensure_scratch(lat, (size_t)fused_blocks(lat->g) * 6, 8);
+  if (rc) return rc;
+  rc = update_impl(lat, rng, metrop, ovrn, lat->d_out);
+  if (rc) return rc;
+  if (dev_out != lat->d_out)
+    U1_CUDA_TRY(cudaMemcpyAsync(dev_out, lat->d_out, 6 * sizeof(double), cudaMemcpyDeviceToDevice, lat->stream));
   return U1_OK;
 }
 
@@ -636,7 +705,8 @@ extern "C" int u1_update_phase(u1_lattice *lat, u1_rng *rng, int metropolis, int
 template <int D>
 static int launch_measure(u1_lattice *lat, double *dev_out) {
   const GeomK &g = lat->g;
-  const int nb = u1i::blocks_for(g.Vh, kRedThreads);
+  const int nbp = measure_plaq_blocks(g);
+  const int nb = nbp + measure_poly_blocks(g);
   int rc = u1i::ensure_scratch(lat, (size_t)nb * 6, 8);
   if (rc) return rc;
   int nSS = 0, nST = 0;
@@ -645,7 +715,7 @@ static int launch_measure(u1_lattice *lat, double *dev_out) {
   const double normSS = 1.0 / ((double)g.V * nSS);
   const double normST = 1.0 / ((double)g.V * nST);
   const double normL = 1.0 / (double)g.Vs;
-  k_measure<D><<<nb, kRedThreads, 0, lat->stream>>>(lat->links, g, lat->partials, lat->counter,
+  k_measure<D><<<nb, kRedThreads, 0, lat->stream>>>(lat->links, g, nbp, lat->partials, lat->counter,
                                                    dev_out ? dev_out : lat->d_out, normSS, normST, normL);
   U1_LAUNCH_CHECK("k_measure");
   return U1_OK;

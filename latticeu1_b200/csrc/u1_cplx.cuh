@@ -18,6 +18,12 @@ __device__ __forceinline__ float2 cconjmul(float2 a, float2 b) {
 }
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+// wa*a + wb*b with an explicit fused multiply-add, so every kernel that
+// forms a staple rounds it identically (the library is built with
+// -fmad=false: no compiler-chosen contractions).
+__device__ __forceinline__ float2 cweigh(float2 a, float wa, float2 b, float wb) {
+  return make_float2(fmaf(a.x, wa, b.x * wb), fmaf(a.y, wa, b.y * wb));
+}
 __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
 // Re(a * b)
 __device__ __forceinline__ float cre_mul(float2 a, float2 b) { return fmaf(a.x, b.x, -a.y * b.y); }

@@ -77,68 +77,82 @@ __device__ __forceinline__ void partials_finish(double (&v)[NV], double *smem, d
   if (threadIdx.x == 0) *counter = 0u;
 }
 
-// Fused plaquette + Polyakov loop.  Thread i handles the plaquettes mu<nu at
-// EO sites (i, parity 0) and (i, parity 1), and for i < V_s/2 the two
-// Polyakov loops starting at those sites on the t = 0 slice.
+// Fused plaquette + Polyakov loop, one launch of nb_plaq + nb_poly blocks.
+// Blocks [0, nb_plaq): thread i handles the plaquettes mu<nu at EO sites
+// (i, parity 0) and (i, parity 1).  Blocks [nb_plaq, ...): thread j handles
+// the Polyakov loop of spatial site j (EO order on the t = 0 slice), so the
+// Nt-long products are spread over their own blocks.
 // out = {SS re, SS im, ST re, ST im, L re, L im}: mean of (1 - e^{i theta_P})
 // per class and (1/V_s) sum_x prod_t U_t.
 template <int D>
 static __global__ void __launch_bounds__(kRedThreads)
-    k_measure(const float2 *__restrict__ lat, GeomK g, double *partials, unsigned int *counter,
+    k_measure(const float2 *__restrict__ lat, GeomK g, int nb_plaq, double *partials, unsigned int *counter,
               double *out, double normSS, double normST, double normL) {
   __shared__ double smem[kRedWarps * 6];
-  double v[6] = {0, 0, 0, 0, 0, 0};
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < g.Vh) {
+  float vs[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // per-thread partial sums of a few terms
+  if ((int)blockIdx.x < nb_plaq) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < g.Vh) {
+      int x[4], k;
+      eo_decode_fast<D>(g, i, 0, x, k);
 #pragma unroll
-    for (int p = 0; p < 2; ++p) {
-      int x[4];
-      eo_decode(g, i, p, x);
-      const int q = 1 - p;
+      for (int p = 0; p < 2; ++p) {
+        if (p == 1) x[0] = 2 * k + ((x[1] + x[2] + x[3] + 1) & 1);
+        int fwd[4], bwd[4];
+        eo_steps<D>(g, x, k, fwd, bwd);
+        const int q = 1 - p;
+        float2 U[D];
 #pragma unroll
-      for (int mu = 0; mu < D - 1; ++mu) {
-        int xm[4];
+        for (int mu = 0; mu < D; ++mu) U[mu] = __ldg(lat + mu * g.V + p * g.Vh + i);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) xm[k] = (k == mu) ? wrap_inc(x[k], g.N[k]) : x[k];
-        const int i_xm = eo_index(g, xm);
-        const float2 Umu = __ldg(lat + (size_t)mu * g.V + (size_t)p * g.Vh + i);
+        for (int mu = 0; mu < D - 1; ++mu) {
 #pragma unroll
-        for (int nu = mu + 1; nu < D; ++nu) {
-          int xn[4];
-#pragma unroll
-          for (int k = 0; k < 4; ++k) xn[k] = (k == nu) ? wrap_inc(x[k], g.N[k]) : x[k];
-          const float2 a = __ldg(lat + (size_t)nu * g.V + (size_t)q * g.Vh + i_xm);
-          const float2 b = __ldg(lat + (size_t)mu * g.V + (size_t)q * g.Vh + eo_index(g, xn));
-          const float2 c = __ldg(lat + (size_t)nu * g.V + (size_t)p * g.Vh + i);
-          const float2 P = cmulc(cmulc(cmul(Umu, a), b), c);
-          if (nu == g.tdir) {
-            v[2] += 1.0 - (double)P.x;
-            v[3] -= (double)P.y;
-          } else {
-            v[0] += 1.0 - (double)P.x;
-            v[1] -= (double)P.y;
+          for (int nu = mu + 1; nu < D; ++nu) {
+            const float2 a = __ldg(lat + nu * g.V + q * g.Vh + i + fwd[mu]);  // U_nu(x+mu)
+            const float2 b = __ldg(lat + mu * g.V + q * g.Vh + i + fwd[nu]);  // U_mu(x+nu)
+            const float2 P = cmulc(cmulc(cmul(U[mu], a), b), U[nu]);
+            if (nu == D - 1) {
+              vs[2] += 1.f - P.x;
+              vs[3] -= P.y;
+            } else {
+              vs[0] += 1.f - P.x;
+              vs[1] -= P.y;
+            }
           }
         }
       }
     }
-  }
-  if (i < g.Vs / 2) {
-    const int Nt = g.N[g.tdir];
-    const int est = g.es[g.tdir];
-#pragma unroll
-    for (int p = 0; p < 2; ++p) {
-      float2 L = make_float2(1.f, 0.f);
-      for (int t = 0; t < Nt; ++t) {
-        const int pt = (p + t) & 1;
-        L = cmul(L, __ldg(lat + (size_t)g.tdir * g.V + (size_t)pt * g.Vh + i + (size_t)t * est));
+  } else {
+    const int j = ((int)blockIdx.x - nb_plaq) * blockDim.x + threadIdx.x;
+    if (j < g.Vs) {
+      const int hs = g.Vs / 2;
+      const int p = j >= hs ? 1 : 0;
+      const int i = j - p * hs;
+      const int Nt = g.N[D - 1];
+      const int est = g.es[D - 1];
+      const float2 *base = lat + (D - 1) * g.V + i;
+      float2 L0 = make_float2(1.f, 0.f), L1 = L0;  // even / odd t partial products
+      int t = 0;
+#pragma unroll 4
+      for (; t + 1 < Nt; t += 2) {
+        L0 = cmul(L0, __ldg(base + ((p + t) & 1) * g.Vh + t * est));
+        L1 = cmul(L1, __ldg(base + ((p + t + 1) & 1) * g.Vh + (t + 1) * est));
       }
-      v[4] += (double)L.x;
-      v[5] += (double)L.y;
+      const float2 L = cmul(L0, L1);  // Nt is even
+      vs[4] += L.x;
+      vs[5] += L.y;
     }
   }
+  double v[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) v[k] = (double)vs[k];
   const double scale[6] = {normSS, normSS, normST, normST, normL, normL};
   partials_finish<6>(v, smem, partials, counter, out, scale);
 }
+
+// Blocks of the fused measurement: plaquette blocks then Polyakov blocks.
+__host__ inline int measure_plaq_blocks(const GeomK &g) { return (g.Vh + kRedThreads - 1) / kRedThreads; }
+__host__ inline int measure_poly_blocks(const GeomK &g) { return (g.Vs + kRedThreads - 1) / kRedThreads; }
 
 // I1(x)/I0(x) by backward evaluation of the Gauss continued fraction
 // r_k = I_k/I_{k-1} = x / (2k + x r_{k+1}) (from the recurrence

@@ -12,9 +12,9 @@
 // the 6-double result buffer (output), both device pointers.
 //
 // Limits and sharing:
-//  * The array holds kNoAllocMaxBlocks blocks of partials (~192 KiB, kept by
+//  * The array holds kNoAllocMaxBlocks blocks of partials (~384 KiB, kept by
 //    every GPU that loads the library until the process exits), which
-//    bounds the lattice at V/2 <= kNoAllocMaxBlocks * 256 sites
+//    bounds the lattice at V/2 <= kNoAllocMaxPlaqBlocks * 256 sites
 //    (V <= 2,097,152, e.g. 32^4 or 32^3 x 64); larger lattices are rejected
 //    with U1_ERR_INVALID before any device work.
 //  * Every call shares the one array, and it keeps the last call's contents.
@@ -36,7 +36,10 @@ using namespace u1b;
 
 namespace {
 
-constexpr int kNoAllocMaxBlocks = 4096;
+// Room for the measurement's plaquette blocks (V/2 / 256 <= 4096) plus its
+// Polyakov blocks (V_s / 256 <= V/2 / 256).
+constexpr int kNoAllocMaxPlaqBlocks = 4096;
+constexpr int kNoAllocMaxBlocks = 2 * kNoAllocMaxPlaqBlocks;
 constexpr int kNoAllocMaxDevices = 64;
 // partials (6 doubles per block) followed by one 256-byte slot whose first
 // word is the ticket counter.
@@ -68,7 +71,8 @@ int noalloc_scratch(double **out) {
 
 template <int D>
 int launch_noalloc(const float2 *links, const GeomK &g, double *scratch, double *out, cudaStream_t s) {
-  const int nb = (g.Vh + kRedThreads - 1) / kRedThreads;
+  const int nbp = measure_plaq_blocks(g);
+  const int nb = nbp + measure_poly_blocks(g);
   unsigned int *counter = reinterpret_cast<unsigned int *>(scratch + (size_t)kNoAllocMaxBlocks * 6);
   U1_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned int), s));
   int nSS = 0, nST = 0;
@@ -77,7 +81,7 @@ int launch_noalloc(const float2 *links, const GeomK &g, double *scratch, double 
   const double normSS = 1.0 / ((double)g.V * nSS);
   const double normST = 1.0 / ((double)g.V * nST);
   const double normL = 1.0 / (double)g.Vs;
-  k_measure<D><<<nb, kRedThreads, 0, s>>>(links, g, scratch, counter, out, normSS, normST, normL);
+  k_measure<D><<<nb, kRedThreads, 0, s>>>(links, g, nbp, scratch, counter, out, normSS, normST, normL);
   U1_LAUNCH_CHECK("k_measure (noalloc)");
   return U1_OK;
 }
@@ -92,9 +96,9 @@ extern "C" int u1_measure_noalloc(const void *links_dev, const u1_geom *geom, do
   GeomK g{};
   int rc = u1i::make_geom(geom, g);
   if (rc) return rc;
-  if (g.Vh > kNoAllocMaxBlocks * kRedThreads) {
+  if (g.Vh > kNoAllocMaxPlaqBlocks * kRedThreads) {
     u1i::set_error("u1_measure_noalloc: lattice too large for the fixed scratch array (V/2 = " +
-                   std::to_string(g.Vh) + " > maximum " + std::to_string((long long)kNoAllocMaxBlocks * kRedThreads) +
+                   std::to_string(g.Vh) + " > maximum " + std::to_string((long long)kNoAllocMaxPlaqBlocks * kRedThreads) +
                    " sites); use u1_measure_async");
     return U1_ERR_INVALID;
   }

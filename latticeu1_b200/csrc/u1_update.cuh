@@ -71,7 +71,7 @@ __device__ __forceinline__ float2 staple_at(const float2 *__restrict__ lat, cons
     else
       ss = cadd(ss, cadd(up, lo));
   }
-  return cadd(cscale(ss, c.w_ss), cscale(st, c.w_st));
+  return cweigh(ss, c.w_ss, st, c.w_st);
 }
 
 // Overrelaxation of one link: U' = (conj S)^2/|S|^2 * conj U, renormalised.
@@ -80,7 +80,7 @@ __device__ __forceinline__ float2 overrelax_link(float2 S, float2 U) {
   float n2 = fmaf(S.x, S.x, S.y * S.y);
   if (n2 > 0.f) {
     float inv = 1.0f / n2;
-    float ax = (S.x * S.x - S.y * S.y) * inv;
+    float ax = fmaf(S.x, S.x, -(S.y * S.y)) * inv;
     float ay = -2.0f * S.x * S.y * inv;
     float2 Un = make_float2(fmaf(ax, U.x, ay * U.y), fmaf(ay, U.x, -ax * U.y));
     float r = rsqrtf(fmaf(Un.x, Un.x, Un.y * Un.y));
@@ -134,7 +134,7 @@ __device__ __forceinline__ float2 staple_steps(const float2 *__restrict__ lat, c
     else
       ss = cadd(ss, sum);
   }
-  return cadd(cscale(ss, c.w_ss), cscale(st, c.w_st));
+  return cweigh(ss, c.w_ss, st, c.w_st);
 }
 
 // One (parity, MU) phase, one thread per link.  MET selects Metropolis vs
@@ -288,8 +288,8 @@ __global__ void __launch_bounds__(256, 8) k_update_pair(const UpdArgs a) {
     else
       staple_term2(A, B, C, Dd, E, F, ss0, ss1);
   }
-  const float2 S0 = cadd(cscale(ss0, a.c.w_ss), cscale(st0, a.c.w_st));
-  const float2 S1 = cadd(cscale(ss1, a.c.w_ss), cscale(st1, a.c.w_st));
+  const float2 S0 = cweigh(ss0, a.c.w_ss, st0, a.c.w_st);
+  const float2 S1 = cweigh(ss1, a.c.w_ss, st1, a.c.w_st);
   float4 *own = reinterpret_cast<float4 *>(a.lat + MU * V + a.p * Vh + i);
   const float4 U = *own;
   const float2 N0 = update_one<D, MU, MET, REPLAY>(a, i, S0, make_float2(U.x, U.y));

@@ -189,6 +189,12 @@ class Lattice:
     def update(self, rng: Rng, metrop: int = 1, ovrn: int = 4) -> None:
         check(lib.u1_update(self._h, rng.handle, int(metrop), int(ovrn)), "u1_update")
 
+    def update_measure(self, rng: Rng, metrop: int, ovrn: int, dev_ptr: int) -> None:
+        """Sweep with the plaquette + Polyakov measurement fused into its last
+        phase; 6 doubles land at device address dev_ptr (asynchronous)."""
+        check(lib.u1_update_measure(self._h, rng.handle, int(metrop), int(ovrn), C.c_void_p(dev_ptr)),
+              "u1_update_measure")
+
     def update_phase(self, rng: Rng, metropolis: bool, parity: int, mu: int, hit: int = 0) -> None:
         """One (parity, mu) phase; the rng's pass counter does not advance."""
         check(lib.u1_update_phase(self._h, rng.handle, int(bool(metropolis)), int(parity), int(mu), int(hit)),

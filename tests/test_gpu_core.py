@@ -351,3 +351,30 @@ def test_errors_are_status_codes(ctx):
     with pytest.raises(U1Error) as ei:
         lat.update(rng, 1, 0)
     assert ei.value.code == -5
+
+
+@pytest.mark.parametrize("dims,N,beta,aniso,metrop,ovrn", [(4, (8, 8, 8, 8), 1.0, 1.0, 1, 4), (4, (6, 4, 4, 12), 0.9, 1.5, 1, 2),
+                                                           (4, (8, 6, 6, 8), 1.1, 1.0, 2, 0), (3, (8, 6, 0, 10), 2.0, 1.0, 1, 3),
+                                                           (2, (16, 0, 0, 6), 3.0, 1.0, 1, 1)])
+def test_fused_measurement_sweep(ctx, dims, N, beta, aniso, metrop, ovrn):
+    """u1_update_measure: links bit-identical to u1_update, observables equal
+    to u1_measure of the same configuration within the FP32 tolerance."""
+    import torch
+    a = Lattice(ctx, dims, N, beta, aniso)
+    b = Lattice(ctx, dims, N, beta, aniso)
+    ra, rb = Rng(ctx, 17), Rng(ctx, 17)
+    a.hot_start(ra)
+    b.hot_start(rb)
+    out = torch.zeros(6, dtype=torch.float64, device="cuda")
+    for _ in range(3):
+        a.update_measure(ra, metrop, ovrn, out.data_ptr())
+        b.update(rb, metrop, ovrn)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(a.export_angles(), b.export_angles())
+        want = b.measure()
+        got = out.cpu().numpy()
+        if dims > 2:
+            assert abs(complex(got[0], got[1]) - want["plaq_ss"]) < 2e-6
+        assert abs(complex(got[2], got[3]) - want["plaq_st"]) < 2e-6
+        assert abs(complex(got[4], got[5]) - want["poly"]) < 2e-6
+    assert ra.state == rb.state
