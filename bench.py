@@ -332,6 +332,7 @@ def run_ours(args) -> None:
                     "path": "u1_lattice_import_angles(pinned host FP64) + u1_update_measure + D2H of the "
                             "6 observables + u1_lattice_export_angles(pinned host FP64) per step"},
             "gpu_launches": int(launches),
+            "update_variant": Lattice.VARIANTS.get(lat.variant, str(lat.variant)),
             "clocks": clk,
             "wall_s_timed_region": t_wall,
             "update_ms_per_step": upd_ms / args.steps,
@@ -390,6 +391,117 @@ def run_multilevel(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def batched_geoms(seed: int = 20240):
+    """512 chains: 256 x 16^4, 128 x 12^4, 128 x 16^3x32, beta ~ U[0.8, 1.2]
+    from a seeded generator."""
+    import numpy as np
+    r = np.random.default_rng(seed)
+    shapes = [(16, 16, 16, 16)] * 256 + [(12, 12, 12, 12)] * 128 + [(16, 16, 16, 32)] * 128
+    return [(4, s, float(b)) for s, b in zip(shapes, r.uniform(0.8, 1.2, len(shapes)))]
+
+
+def run_batched(args) -> None:
+    """Config: 512 independent chains advanced together (one launch per
+    (parity, mu) phase for all of them, whole sweep + per-chain measurement
+    captured in one CUDA graph).  A step is one sweep (1 Metropolis + 4 OR)
+    of every chain plus its plaquette/Polyakov measurement.  The comparator
+    advances the same chains one by one (one lattice object per chain, its
+    own graph-captured sweep), as a caller of the single-lattice API would."""
+    import numpy as np
+    import torch
+
+    from latticeu1_b200 import Batch, Context, Lattice, Rng, launch_count
+    ctx = Context(0)
+    geoms = batched_geoms()
+    stream = torch.cuda.Stream()
+    b = Batch(ctx, geoms, seed=1234)
+    b.set_stream(stream.cuda_stream)
+    links = b.total_links
+    lu = links * (METROP + OVRN)
+    flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    with torch.cuda.stream(stream):
+        b.hot_start()
+        for _ in range(args.warmup):
+            b.update(METROP, OVRN, measure=True)
+            b.update(METROP, OVRN, measure=False)
+        stream.synchronize()
+
+        def timed(measure: bool, steps: int) -> float:
+            ev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(steps)]
+            for k in range(steps):
+                flush.zero_()
+                ev[k][0].record(stream)
+                b.update(METROP, OVRN, measure=measure)
+                ev[k][1].record(stream)
+            torch.cuda.synchronize()
+            return sum(e[0].elapsed_time(e[1]) for e in ev)
+
+        n0 = launch_count()
+        step_ms = timed(True, args.steps)
+        launches = launch_count() - n0
+        upd_ms = timed(False, args.steps)
+        obs = b.results_raw()
+    value = args.steps * lu / (step_ms * 1e-3)
+    phases = 2 * DIMS * (METROP + OVRN)
+    avg_launch_s = upd_ms * 1e-3 / (args.steps * phases)
+    alg_bytes = algorithmic_bytes_per_link_update(DIMS) * links // (2 * DIMS)
+    achieved = alg_bytes / avg_launch_s / 1e9
+    peak, peak_kind = measured_peak()
+
+    # comparator: the same chains one at a time through the single-lattice API
+    nseq = len(geoms)
+    lats, rngs = [], []
+    for c, (d, N, beta) in enumerate(geoms[:nseq]):
+        lat = Lattice(ctx, d, N, beta)
+        lat.set_stream(stream.cuda_stream)
+        lat.set_variant(1)
+        rng = Rng(ctx, 1234)
+        rng.set_chain(c)
+        lats.append(lat)
+        rngs.append(rng)
+    out = torch.zeros((nseq, 6), dtype=torch.float64, device="cuda")
+    with torch.cuda.stream(stream):
+        for lat, rng in zip(lats, rngs):
+            lat.hot_start(rng)
+            lat.update_measure(rng, METROP, OVRN, out[0].data_ptr())
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        seq_steps = max(1, min(args.steps, 5))
+        e0.record(stream)
+        for _ in range(seq_steps):
+            for k, (lat, rng) in enumerate(zip(lats, rngs)):
+                lat.update_measure(rng, METROP, OVRN, out[k].data_ptr())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        seq_ms = e0.elapsed_time(e1)
+    seq_value = seq_steps * lu / (seq_ms * 1e-3)
+    for lat in lats:
+        lat.close()
+    absL = np.abs(obs[:, 4] + 1j * obs[:, 5])
+    line = {
+        "metric": "link-updates/s, 512-chain batch (1 Metropolis + 4 OR per sweep, per-chain measurement)",
+        "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": step_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "batched: 256x16^4 + 128x12^4 + 128x16^3x32 chains, beta~U[0.8,1.2] "
+                               "(seeded), hot starts, 1 Met + 4 OR sweep + per-chain plaquette/Polyakov",
+                   "chains": len(geoms), "links": links, "bytes": links * 8,
+                   "l2": "flushed between timed steps (512 MiB device write)"},
+        "roofline": {"bound": "hbm", "kernel": "k_batch_update (one (parity,mu) phase over all chains)",
+                     "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "algorithmic_bytes_per_launch": alg_bytes,
+                     "avg_launch_us": avg_launch_s * 1e6},
+        "update_only_ms_per_step": upd_ms / args.steps,
+        "gpu_launches": int(launches),
+        "one_by_one": {"value": seq_value, "unit": UNIT, "steps": seq_steps,
+                       "path": "one Lattice per chain, graph-captured u1_update_measure each, same stream"},
+        "speedup_vs_one_by_one": value / seq_value,
+        "observables": {"plaq_st_re_mean": float(obs[:, 2].mean()), "absL_mean": float(absL.mean())},
+    }
+    print(json.dumps(line), flush=True)
+    b.close()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -399,7 +511,7 @@ def main() -> None:
     ap.add_argument("--L", type=int, default=L_DEFAULT)
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU baseline sampling")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["update32", "multilevel"], default="update32")
+    ap.add_argument("--workload", choices=["update32", "multilevel", "batched"], default="update32")
     ap.add_argument("--n2", type=int, default=200, help="level-2 sub-updates per step (multilevel)")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -408,6 +520,8 @@ def main() -> None:
         run_reference(args)
     elif args.workload == "multilevel":
         run_multilevel(args)
+    elif args.workload == "batched":
+        run_batched(args)
     else:
         run_ours(args)
 

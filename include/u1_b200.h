@@ -37,6 +37,7 @@ enum {
 typedef struct u1_ctx u1_ctx;
 typedef struct u1_lattice u1_lattice;
 typedef struct u1_rng u1_rng;
+typedef struct u1_batch u1_batch;
 
 typedef struct u1_geom {
   int dims;       /* 2, 3 or 4 (reference "dirs") */
@@ -81,6 +82,20 @@ int u1_lattice_set_coupling(u1_lattice *lat, double beta, double aniso);
  * replayed (enable = 1, default) or launched kernel by kernel (enable = 0).
  * Both issue the same kernels with the same arguments. */
 int u1_lattice_set_graphs(u1_lattice *lat, int enable);
+/* Update kernel variants, all giving bit-identical links: 1 = two sites per
+ * thread (32-register cap, 8 CTAs/SM), 2 = two sites per thread (no cap),
+ * 3 = one site per thread; 0 = auto (tuned at the first u1_update).  The
+ * two-site variants need Nx/2 even. */
+int u1_lattice_set_variant(u1_lattice *lat, int variant);
+/* The variant in use: 0 while automatic and not yet tuned. */
+int u1_lattice_get_variant(const u1_lattice *lat, int *variant);
+/* Replaces the reference's autotuner (tuneLaunch, src/tune.cpp:306-416):
+ * times every valid variant on a few sweeps of this lattice from a
+ * backed-up state (links and rng pass restored afterwards), keeps the
+ * fastest and caches it per (device, geometry); with U1_RESOURCE_PATH set
+ * the cache persists in $U1_RESOURCE_PATH/u1b200_tunecache.tsv.
+ * U1_TUNE=0 in the environment turns the automatic first-update tuning off. */
+int u1_tune(u1_lattice *lat, u1_rng *rng, int *variant);
 /* Device pointer of the float2 link array (V*dims float2). */
 int u1_lattice_links(u1_lattice *lat, void **dev_ptr);
 /* Copy all links of src into dst (same geometry). */
@@ -179,6 +194,41 @@ int u1_poly_corr(u1_lattice *lat, int multihit, double *out, int out_len);
  * the reference exits).  out as for u1_poly_corr. */
 int u1_multilevel(u1_lattice *lat, u1_rng *rng, int n4, int k4, int n2, int k2,
                   int metrop, int ovrn, double *out, int out_len);
+
+/* ------------------------------------------------------------------ batches
+ * Many independent chains advanced by shared launches.  The reference runs
+ * one lattice per process (u1.cpp:99-120, one UpdateLattice call per
+ * sweep); a batch advances nchains lattices (same dims, any extents, own
+ * beta and aniso each) with one kernel per (parity, mu) phase for all of
+ * them, and captures each sweep shape once as a CUDA graph.  All chains
+ * share the Philox key `seed`; chain c uses chain number first_chain + c in
+ * the counter, so it follows exactly the trajectory of a single lattice
+ * driven by u1_update with an rng of the same seed, u1_rng_set_chain(
+ * first_chain + c), and the same sequence of hot starts and updates.
+ * first_chain + nchains <= 65536.  Chains start cold. */
+int u1_batch_create(u1_ctx *ctx, int nchains, const u1_geom *geoms, uint64_t seed, uint32_t first_chain,
+                    u1_batch **out);
+int u1_batch_destroy(u1_batch *b);
+int u1_batch_set_stream(u1_batch *b, void *stream);
+/* out = {nchains, dims, total links, two-sites-per-thread kernels in use}. */
+int u1_batch_info(const u1_batch *b, int64_t out[4]);
+/* Hot start of every chain (as u1_hot_start); advances the pass counter by 1. */
+int u1_batch_hot_start(u1_batch *b);
+/* One sweep of every chain: metrop Metropolis then ovrn overrelaxation
+ * passes (as u1_update).  measure != 0 appends the plaquette + Polyakov
+ * measurement of every chain; read it with u1_batch_results.  Asynchronous. */
+int u1_batch_update(u1_batch *b, int metrop, int ovrn, int measure);
+/* Measure every chain now: out_host = 6 doubles per chain (as u1_measure). */
+int u1_batch_measure(u1_batch *b, double *out_host);
+/* The last measurement (6 doubles per chain), waiting for the batch's stream. */
+int u1_batch_results(u1_batch *b, double *out_host);
+/* Device address of the 6*nchains result doubles (valid until destroy). */
+int u1_batch_results_device(u1_batch *b, double **dev_ptr);
+/* Per-chain FP64 angles in the reference's EO layout (as u1_lattice_*_angles). */
+int u1_batch_import_angles(u1_batch *b, int chain, const double *angles_host);
+int u1_batch_export_angles(u1_batch *b, int chain, double *angles_host);
+/* Metropolis passes done so far (the rng pass counter of the batch). */
+int u1_batch_get_pass(const u1_batch *b, uint64_t *pass);
 
 /* Number of kernels this library has launched in the calling process. */
 int u1_kernel_launch_count(uint64_t *out);

@@ -45,6 +45,9 @@ SIGNATURES = {
     "u1_lattice_info": [_vp, C.POINTER(C.c_int64)],
     "u1_lattice_set_coupling": [_vp, C.c_double, C.c_double],
     "u1_lattice_set_graphs": [_vp, _i],
+    "u1_lattice_set_variant": [_vp, _i],
+    "u1_lattice_get_variant": [_vp, C.POINTER(_i)],
+    "u1_tune": [_vp, _vp, C.POINTER(_i)],
     "u1_lattice_links": [_vp, C.POINTER(_vp)],
     "u1_lattice_copy": [_vp, _vp],
     "u1_lattice_import_angles": [_vp, _vp, _i],
@@ -68,6 +71,18 @@ SIGNATURES = {
     "u1_measure_noalloc": [_vp, C.POINTER(u1_geom), _vp, _vp],
     "u1_poly_corr": [_vp, _i, _dp, _i],
     "u1_multilevel": [_vp, _vp, _i, _i, _i, _i, _i, _i, _dp, _i],
+    "u1_batch_create": [_vp, _i, C.POINTER(u1_geom), C.c_uint64, C.c_uint32, C.POINTER(_vp)],
+    "u1_batch_destroy": [_vp],
+    "u1_batch_set_stream": [_vp, _vp],
+    "u1_batch_info": [_vp, C.POINTER(C.c_int64)],
+    "u1_batch_hot_start": [_vp],
+    "u1_batch_update": [_vp, _i, _i, _i],
+    "u1_batch_measure": [_vp, _dp],
+    "u1_batch_results": [_vp, _dp],
+    "u1_batch_results_device": [_vp, C.POINTER(_vp)],
+    "u1_batch_import_angles": [_vp, _i, _vp],
+    "u1_batch_export_angles": [_vp, _i, _vp],
+    "u1_batch_get_pass": [_vp, C.POINTER(C.c_uint64)],
     "u1_kernel_launch_count": [C.POINTER(C.c_uint64)],
     "u1_last_error": [],
     "u1_version": [],

@@ -13,7 +13,11 @@
 // replayed as CUDA graphs.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <fstream>
+#include <mutex>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -223,6 +227,7 @@ extern "C" int u1_lattice_destroy(u1_lattice *lat) {
   if (lat->h_out) cudaFreeHost(lat->h_out);
   if (lat->pfield) cudaFree(lat->pfield);
   if (lat->stage) cudaFree(lat->stage);
+  if (lat->backup) cudaFree(lat->backup);
   if (lat->own_stream) cudaStreamDestroy(lat->own_stream);
   delete lat;
   return U1_OK;
@@ -465,15 +470,21 @@ static int launch_pdl(K kernel, int blocks, cudaStream_t s, const UpdArgs &a, co
   return U1_OK;
 }
 
-// Two sites per thread (k_update_pair) when N0/2 is even, else one.
+// The phase kernel of the chosen variant.
 template <int D, int MU>
-static int launch_phase_mu(const UpdArgs &a, cudaStream_t s, bool met, bool replay) {
-  if ((a.g.hN0 & 1) == 0) {
+static int launch_phase_mu(const UpdArgs &a, cudaStream_t s, bool met, bool replay, int variant) {
+  if (variant == U1V_PAIR32 || variant == U1V_PAIR) {
     const int blocks = u1i::blocks_for(a.g.Vh / 2, 256);
+    if (variant == U1V_PAIR32) {
+      if (met)
+        return replay ? launch_pdl(k_update_pair<D, MU, true, true>, blocks, s, a, "k_update_pair")
+                      : launch_pdl(k_update_pair<D, MU, true, false>, blocks, s, a, "k_update_pair");
+      return launch_pdl(k_update_pair<D, MU, false, false>, blocks, s, a, "k_update_pair");
+    }
     if (met)
-      return replay ? launch_pdl(k_update_pair<D, MU, true, true>, blocks, s, a, "k_update_pair")
-                    : launch_pdl(k_update_pair<D, MU, true, false>, blocks, s, a, "k_update_pair");
-    return launch_pdl(k_update_pair<D, MU, false, false>, blocks, s, a, "k_update_pair");
+      return replay ? launch_pdl(k_update_pair_free<D, MU, true, true>, blocks, s, a, "k_update_pair_free")
+                    : launch_pdl(k_update_pair_free<D, MU, true, false>, blocks, s, a, "k_update_pair_free");
+    return launch_pdl(k_update_pair_free<D, MU, false, false>, blocks, s, a, "k_update_pair_free");
   }
   const int blocks = u1i::blocks_for(a.g.Vh, 256);
   if (met)
@@ -483,18 +494,27 @@ static int launch_phase_mu(const UpdArgs &a, cudaStream_t s, bool met, bool repl
 }
 
 template <int D>
-static int launch_phase(const UpdArgs &a, cudaStream_t s, bool met, bool replay) {
+static int launch_phase(const UpdArgs &a, cudaStream_t s, bool met, bool replay, int variant) {
   switch (a.mu) {
-    case 0: return launch_phase_mu<D, 0>(a, s, met, replay);
-    case 1: return launch_phase_mu<D, 1>(a, s, met, replay);
+    case 0: return launch_phase_mu<D, 0>(a, s, met, replay, variant);
+    case 1: return launch_phase_mu<D, 1>(a, s, met, replay, variant);
     case 2:
-      if constexpr (D > 2) return launch_phase_mu<D, 2>(a, s, met, replay);
+      if constexpr (D > 2) return launch_phase_mu<D, 2>(a, s, met, replay, variant);
       break;
     case 3:
-      if constexpr (D > 3) return launch_phase_mu<D, 3>(a, s, met, replay);
+      if constexpr (D > 3) return launch_phase_mu<D, 3>(a, s, met, replay, variant);
       break;
   }
   return fail(U1_ERR_INVALID, "k_update: direction out of range");
+}
+
+// Variant used when the tuner has not chosen one.
+static int default_variant(const GeomK &g) { return (g.hN0 & 1) ? U1V_SINGLE : U1V_PAIR32; }
+static bool variant_valid(const GeomK &g, int v) {
+  return v == U1V_SINGLE || ((v == U1V_PAIR32 || v == U1V_PAIR) && (g.hN0 & 1) == 0);
+}
+static int effective_variant(const u1_lattice *lat) {
+  return lat->variant == U1V_AUTO ? default_variant(lat->g) : lat->variant;
 }
 
 template <int D, bool MET>
@@ -553,9 +573,10 @@ static int issue_sweep(u1_lattice *lat, float2 *links, u1_rng *rng, int metrop, 
            : D == 3 ? launch_fused_last<3, false>(a, lat->stream, lat, fused_out)
                     : launch_fused_last<4, false>(a, lat->stream, lat, fused_out);
     }
-    return D == 2 ? launch_phase<2>(a, lat->stream, met, met && replay)
-         : D == 3 ? launch_phase<3>(a, lat->stream, met, met && replay)
-                  : launch_phase<4>(a, lat->stream, met, met && replay);
+    const int var = effective_variant(lat);
+    return D == 2 ? launch_phase<2>(a, lat->stream, met, met && replay, var)
+         : D == 3 ? launch_phase<3>(a, lat->stream, met, met && replay, var)
+                  : launch_phase<4>(a, lat->stream, met, met && replay, var);
   };
   for (int m = 0; m < metrop; ++m)
     for (int p = 0; p < 2; ++p)
@@ -602,7 +623,9 @@ template <class F>
 static int capture_graph(u1_lattice *lat, F fn, cudaGraphExec_t *exec) {
   cudaGraph_t graph = nullptr;
   U1_CUDA_TRY(cudaStreamBeginCapture(lat->stream, cudaStreamCaptureModeThreadLocal));
+  const unsigned long long launches0 = u1i::g_launches.load();
   int rc = fn();
+  u1i::g_launches.store(launches0);  // captured kernels run (and count) at graph launch
   cudaError_t e = cudaStreamEndCapture(lat->stream, &graph);
   if (rc) {
     if (graph) cudaGraphDestroy(graph);
@@ -615,11 +638,166 @@ static int capture_graph(u1_lattice *lat, F fn, cudaGraphExec_t *exec) {
   return U1_OK;
 }
 
+// ---------------------------------------------------------------- tuner
+// Replaces the reference's block-size search (src/tune.cpp:306-416,
+// include/tune.h:143-260): the candidates are the compiled update-kernel
+// variants (two sites per thread with a 32-register cap, two sites
+// uncapped, one site), which give bit-identical links, so a trial never
+// changes the Markov chain.  Trials run real sweeps from a backed-up state
+// (links and pass counter restored afterwards, as the reference's
+// preTune/postTune do); the winner is cached per (device, geometry) in
+// memory and, when U1_RESOURCE_PATH names a directory, in
+// $U1_RESOURCE_PATH/u1b200_tunecache.tsv (the reference's tunecache.csv
+// location rule, src/tune.cpp:160-232).  U1_TUNE=0 disables tuning.
+namespace {
+struct TuneCache {
+  std::mutex mu;
+  bool loaded = false;
+  std::map<std::string, int> best;
+};
+TuneCache &tune_cache() {
+  static TuneCache c;
+  return c;
+}
+std::string tune_file() {
+  const char *p = std::getenv("U1_RESOURCE_PATH");
+  return (p && *p) ? std::string(p) + "/u1b200_tunecache.tsv" : std::string();
+}
+bool tuning_enabled() {
+  const char *e = std::getenv("U1_TUNE");
+  return !(e && e[0] == '0');
+}
+std::string tune_key(const u1_lattice *lat) {
+  std::ostringstream k;
+  k << lat->ctx->prop.name << "|update|" << lat->g.dims << "|" << lat->g.N[0] << "x" << lat->g.N[1] << "x"
+    << lat->g.N[2] << "x" << lat->g.N[3];
+  return k.str();
+}
+void tune_load_locked(TuneCache &c) {
+  if (c.loaded) return;
+  c.loaded = true;
+  const std::string f = tune_file();
+  if (f.empty()) return;
+  std::ifstream in(f);
+  std::string line;
+  while (std::getline(in, line)) {
+    if (line.empty() || line[0] == '#') continue;
+    const size_t t1 = line.find('\t');
+    if (t1 == std::string::npos) continue;
+    const size_t t2 = line.find('\t', t1 + 1);
+    const std::string key = line.substr(0, t1);
+    const int v = std::atoi(line.substr(t1 + 1, t2 == std::string::npos ? std::string::npos : t2 - t1 - 1).c_str());
+    if (v >= U1V_PAIR32 && v <= U1V_SINGLE) c.best[key] = v;
+  }
+}
+void tune_save(const std::string &key, int v, double us) {
+  const std::string f = tune_file();
+  if (f.empty()) return;
+  std::ofstream out(f, std::ios::app);
+  if (out) out << key << '\t' << v << '\t' << us << '\n';
+}
+}  // namespace
+
+static int tune_update(u1_lattice *lat, u1_rng *rng, bool use_cache) {
+  const std::string key = tune_key(lat);
+  TuneCache &c = tune_cache();
+  if (use_cache) {
+    std::lock_guard<std::mutex> lock(c.mu);
+    tune_load_locked(c);
+    auto it = c.best.find(key);
+    if (it != c.best.end() && variant_valid(lat->g, it->second)) {
+      lat->variant = it->second;
+      drop_graphs(lat);
+      return U1_OK;
+    }
+  }
+  std::vector<int> cand;
+  for (int v : {U1V_PAIR32, U1V_PAIR, U1V_SINGLE})
+    if (variant_valid(lat->g, v)) cand.push_back(v);
+  int best = cand[0];
+  double best_us = -1.0;
+  if (cand.size() > 1) {
+    const size_t n = (size_t)lat->g.V * lat->g.dims;
+    if (!lat->backup) U1_CUDA_TRY(cudaMalloc(&lat->backup, n * sizeof(float2)));
+    U1_CUDA_TRY(cudaMemcpyAsync(lat->backup, lat->links, n * sizeof(float2), cudaMemcpyDeviceToDevice, lat->stream));
+    const unsigned long long pass0 = rng->pass;
+    cudaEvent_t e0, e1;
+    U1_CUDA_TRY(cudaEventCreate(&e0));
+    U1_CUDA_TRY(cudaEventCreate(&e1));
+    int rc = U1_OK;
+    for (int v : cand) {
+      lat->variant = v;
+      rc = issue_sweep(lat, lat->links, rng, 1, 4, 0);
+      if (!rc) {
+        const cudaError_t er = cudaEventRecord(e0, lat->stream);
+        if (er != cudaSuccess) rc = u1i::cuda_fail(er, "cudaEventRecord");
+      }
+      for (int k = 0; k < 3 && !rc; ++k) rc = issue_sweep(lat, lat->links, rng, 1, 4, 0);
+      cudaEventRecord(e1, lat->stream);
+      cudaError_t e = cudaEventSynchronize(e1);
+      if (!rc && e != cudaSuccess) rc = u1i::cuda_fail(e, "tuning sweep");
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      cudaMemcpyAsync(lat->links, lat->backup, n * sizeof(float2), cudaMemcpyDeviceToDevice, lat->stream);
+      cudaMemcpyAsync(rng->pass_dev, &pass0, sizeof(pass0), cudaMemcpyHostToDevice, lat->stream);
+      cudaStreamSynchronize(lat->stream);
+      if (rc) break;
+      const double us = 1e3 * ms / 3.0;
+      if (best_us < 0.0 || us < best_us) {
+        best_us = us;
+        best = v;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) {
+      lat->variant = U1V_AUTO;
+      return rc;
+    }
+  }
+  lat->variant = best;
+  drop_graphs(lat);
+  std::lock_guard<std::mutex> lock(c.mu);
+  tune_load_locked(c);
+  c.best[key] = best;
+  tune_save(key, best, best_us);
+  return U1_OK;
+}
+
+extern "C" int u1_tune(u1_lattice *lat, u1_rng *rng, int *variant) {
+  if (!lat || !rng) return fail(U1_ERR_INVALID, "u1_tune: null argument");
+  if (rng->replay_dev) return fail(U1_ERR_STATE, "u1_tune: not available while a replay stream is set");
+  U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
+  int rc = tune_update(lat, rng, false);
+  if (rc) return rc;
+  if (variant) *variant = lat->variant;
+  return U1_OK;
+}
+
+extern "C" int u1_lattice_set_variant(u1_lattice *lat, int variant) {
+  if (!lat) return fail(U1_ERR_INVALID, "u1_lattice_set_variant: null lattice");
+  if (variant != U1V_AUTO && !variant_valid(lat->g, variant))
+    return fail(U1_ERR_INVALID, "u1_lattice_set_variant: variant not valid for this geometry (pair variants need Nx/2 even)");
+  lat->variant = variant;
+  drop_graphs(lat);
+  return U1_OK;
+}
+
+extern "C" int u1_lattice_get_variant(const u1_lattice *lat, int *variant) {
+  if (!lat || !variant) return fail(U1_ERR_INVALID, "u1_lattice_get_variant: null argument");
+  *variant = lat->variant;
+  return U1_OK;
+}
+
 static int update_impl(u1_lattice *lat, u1_rng *rng, int metrop, int ovrn, double *fused_out) {
   U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
   int rc = check_replay(lat, rng, metrop);
   if (rc) return rc;
   const bool replay = rng->replay_dev != nullptr;
+  if (lat->variant == U1V_AUTO && !replay && tuning_enabled()) {
+    rc = tune_update(lat, rng, true);
+    if (rc) return rc;
+  }
   if (lat->use_graphs && !replay) {
     // graph key: passes, rng object, seed/chain and whether the last phase is fused
     auto key = std::make_tuple(metrop * 2 + (fused_out ? 1 : 0), ovrn, rng->id,
@@ -694,10 +872,11 @@ extern "C" int u1_update_phase(u1_lattice *lat, u1_rng *rng, int metropolis, int
   a.hit = hit;
   a.replay = rng->replay_dev;
   a.replay_base = rng->replay_base;
+  const int var = effective_variant(lat);
   switch (lat->g.dims) {
-    case 2: return launch_phase<2>(a, lat->stream, met, replay);
-    case 3: return launch_phase<3>(a, lat->stream, met, replay);
-    default: return launch_phase<4>(a, lat->stream, met, replay);
+    case 2: return launch_phase<2>(a, lat->stream, met, replay, var);
+    case 3: return launch_phase<3>(a, lat->stream, met, replay, var);
+    default: return launch_phase<4>(a, lat->stream, met, replay, var);
   }
 }
 

@@ -28,6 +28,9 @@ struct u1_rng {
   uint64_t id = 0;                          // unique per rng object (graph cache key)
 };
 
+// Update kernel variants (all bit-identical; the tuner picks the fastest).
+enum : int { U1V_AUTO = 0, U1V_PAIR32 = 1, U1V_PAIR = 2, U1V_SINGLE = 3 };
+
 struct u1_lattice {
   u1_ctx *ctx = nullptr;
   cudaStream_t stream = nullptr;
@@ -49,6 +52,8 @@ struct u1_lattice {
   // cached CUDA graphs of whole sweeps, keyed by (metrop, ovrn, rng id, seed)
   std::map<std::tuple<int, int, uint64_t, uint64_t>, cudaGraphExec_t> graphs;
   bool use_graphs = true;
+  int variant = U1V_AUTO;          // update kernel variant (U1V_AUTO: tune on first update)
+  float2 *backup = nullptr;        // link backup used while tuning
 };
 
 namespace u1i {

@@ -77,21 +77,14 @@ __device__ __forceinline__ void partials_finish(double (&v)[NV], double *smem, d
   if (threadIdx.x == 0) *counter = 0u;
 }
 
-// Fused plaquette + Polyakov loop, one launch of nb_plaq + nb_poly blocks.
-// Blocks [0, nb_plaq): thread i handles the plaquettes mu<nu at EO sites
-// (i, parity 0) and (i, parity 1).  Blocks [nb_plaq, ...): thread j handles
-// the Polyakov loop of spatial site j (EO order on the t = 0 slice), so the
-// Nt-long products are spread over their own blocks.
-// out = {SS re, SS im, ST re, ST im, L re, L im}: mean of (1 - e^{i theta_P})
-// per class and (1/V_s) sum_x prod_t U_t.
+// Per-thread terms of measurement block `block` (layout as k_measure below):
+// vs[0..3] += (1 - Re P, -Im P) of the SS and ST plaquettes, vs[4..5] += the
+// Polyakov loop.  Shared by the single-lattice and batched measurements.
 template <int D>
-static __global__ void __launch_bounds__(kRedThreads)
-    k_measure(const float2 *__restrict__ lat, GeomK g, int nb_plaq, double *partials, unsigned int *counter,
-              double *out, double normSS, double normST, double normL) {
-  __shared__ double smem[kRedWarps * 6];
-  float vs[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // per-thread partial sums of a few terms
-  if ((int)blockIdx.x < nb_plaq) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void measure_block_values(const float2 *__restrict__ lat, const GeomK &g, int block,
+                                                     int nb_plaq, float (&vs)[6]) {
+  if (block < nb_plaq) {
+    const int i = block * blockDim.x + threadIdx.x;
     if (i < g.Vh) {
       int x[4], k;
       eo_decode_fast<D>(g, i, 0, x, k);
@@ -123,7 +116,7 @@ static __global__ void __launch_bounds__(kRedThreads)
       }
     }
   } else {
-    const int j = ((int)blockIdx.x - nb_plaq) * blockDim.x + threadIdx.x;
+    const int j = (block - nb_plaq) * blockDim.x + threadIdx.x;
     if (j < g.Vs) {
       const int hs = g.Vs / 2;
       const int p = j >= hs ? 1 : 0;
@@ -132,9 +125,8 @@ static __global__ void __launch_bounds__(kRedThreads)
       const int est = g.es[D - 1];
       const float2 *base = lat + (D - 1) * g.V + i;
       float2 L0 = make_float2(1.f, 0.f), L1 = L0;  // even / odd t partial products
-      int t = 0;
 #pragma unroll 4
-      for (; t + 1 < Nt; t += 2) {
+      for (int t = 0; t + 1 < Nt; t += 2) {
         L0 = cmul(L0, __ldg(base + ((p + t) & 1) * g.Vh + t * est));
         L1 = cmul(L1, __ldg(base + ((p + t + 1) & 1) * g.Vh + (t + 1) * est));
       }
@@ -143,6 +135,22 @@ static __global__ void __launch_bounds__(kRedThreads)
       vs[5] += L.y;
     }
   }
+}
+
+// Fused plaquette + Polyakov loop, one launch of nb_plaq + nb_poly blocks.
+// Blocks [0, nb_plaq): thread i handles the plaquettes mu<nu at EO sites
+// (i, parity 0) and (i, parity 1).  Blocks [nb_plaq, ...): thread j handles
+// the Polyakov loop of spatial site j (EO order on the t = 0 slice), so the
+// Nt-long products are spread over their own blocks.
+// out = {SS re, SS im, ST re, ST im, L re, L im}: mean of (1 - e^{i theta_P})
+// per class and (1/V_s) sum_x prod_t U_t.
+template <int D>
+static __global__ void __launch_bounds__(kRedThreads)
+    k_measure(const float2 *__restrict__ lat, GeomK g, int nb_plaq, double *partials, unsigned int *counter,
+              double *out, double normSS, double normST, double normL) {
+  __shared__ double smem[kRedWarps * 6];
+  float vs[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // per-thread partial sums of a few terms
+  measure_block_values<D>(lat, g, (int)blockIdx.x, nb_plaq, vs);
   double v[6];
 #pragma unroll
   for (int k = 0; k < 6; ++k) v[k] = (double)vs[k];

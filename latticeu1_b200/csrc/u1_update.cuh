@@ -137,25 +137,10 @@ __device__ __forceinline__ float2 staple_steps(const float2 *__restrict__ lat, c
   return cweigh(ss, c.w_ss, st, c.w_st);
 }
 
-// One (parity, MU) phase, one thread per link.  MET selects Metropolis vs
-// overrelaxation, REPLAY reads the shared-stream pairs instead of Philox.
+// One link update (Metropolis with Philox or replayed numbers, or
+// overrelaxation) given its staple S and current value U.
 template <int D, int MU, bool MET, bool REPLAY>
-__global__ void __launch_bounds__(256) k_update(const UpdArgs a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int x[4], k;
-  eo_decode_fast<D>(a.g, i, a.p, x, k);
-  pdl_wait_prior_grid();
-  if (!MET && a.bump_ptr != nullptr && blockIdx.x == 0 && threadIdx.x == 0) *a.bump_ptr += a.bump_by;
-  if (i >= a.g.Vh) return;
-  // Multilevel freeze rule, reference src/multilevel.cu:41: update unless the
-  // site lies on a frozen time slice (x_t multiple of ml, ml = 2 or 4) and
-  // the link is spatial (the reference tests the literal direction index 3).
-  if (MU != 3 && a.ml > 0 && (x[D - 1] & (a.ml - 1)) == 0) return;
-  int fwd[4], bwd[4];
-  eo_steps<D>(a.g, x, k, fwd, bwd);
-  float2 *own = a.lat + MU * a.g.V + a.p * a.g.Vh + i;
-  const float2 S = staple_steps<D, MU>(a.lat, a.g, a.c, i, a.p, fwd, bwd);
-  const float2 U = *own;
+__device__ __forceinline__ float2 update_one(const UpdArgs &a, int i, float2 S, float2 U) {
   if (MET) {
     const unsigned long long pass = *a.pass_dev + (unsigned long long)a.hit;
     float2 Un;
@@ -176,11 +161,26 @@ __global__ void __launch_bounds__(256) k_update(const UpdArgs a) {
       Un = make_float2(cs, sn);
     }
     const float dS = a.c.beta * (cre_mul(S, Un) - cre_mul(S, U));
-    if (expf(dS) > b) *own = Un;
-  } else {
-    *own = overrelax_link(S, U);
+    return (expf(dS) > b) ? Un : U;
   }
-  pdl_release_dependents();
+  return overrelax_link(S, U);
+}
+
+// Body of the one-site-per-thread update of EO site i of phase (a.p, MU);
+// shared by the single-lattice and batched kernels.
+template <int D, int MU, bool MET, bool REPLAY>
+__device__ __forceinline__ void update_single_body(const UpdArgs &a, int i) {
+  int x[4], k;
+  eo_decode_fast<D>(a.g, i, a.p, x, k);
+  // Multilevel freeze rule, reference src/multilevel.cu:41: update unless the
+  // site lies on a frozen time slice (x_t multiple of ml, ml = 2 or 4) and
+  // the link is spatial (the reference tests the literal direction index 3).
+  if (MU != 3 && a.ml > 0 && (x[D - 1] & (a.ml - 1)) == 0) return;
+  int fwd[4], bwd[4];
+  eo_steps<D>(a.g, x, k, fwd, bwd);
+  float2 *own = a.lat + MU * a.g.V + a.p * a.g.Vh + i;
+  const float2 S = staple_steps<D, MU>(a.lat, a.g, a.c, i, a.p, fwd, bwd);
+  *own = update_one<D, MU, MET, REPLAY>(a, i, S, *own);
 }
 
 // ---------------------------------------------------------------------------
@@ -209,41 +209,14 @@ __device__ __forceinline__ void staple_term2(const Pair2 &a, const Pair2 &b, con
   acc1 = cadd(acc1, cadd(cmulc(cmulc(a.s1, b.s1), c.s1), cmul(cconjmul(d.s1, e.s1), f.s1)));
 }
 
+// Body of the two-sites-per-thread update for EO sites i, i+1 (i even) of
+// the phase (a.p, MU); shared by the single-lattice and batched kernels.
+// Every variant forms the staple and the update with the same operations in
+// the same order, so all of them give bit-identical links.
 template <int D, int MU, bool MET, bool REPLAY>
-__device__ __forceinline__ float2 update_one(const UpdArgs &a, int i, float2 S, float2 U) {
-  if (MET) {
-    const unsigned long long pass = *a.pass_dev + (unsigned long long)a.hit;
-    float2 Un;
-    float b;
-    if (REPLAY) {
-      const size_t pr = ((((size_t)(pass - a.replay_base) * 2 + a.p) * D + MU) * a.g.Vh + i) * 2;
-      double sn, cs;
-      sincos(a.replay[pr], &sn, &cs);
-      Un = make_float2((float)cs, (float)sn);
-      b = (float)a.replay[pr + 1];
-    } else {
-      Philox4 r = philox4x32_10((uint32_t)(a.p * a.g.Vh + i), u1_rng_word1(MU, U1_TAG_METROPOLIS, a.chain),
-                                (uint32_t)pass, (uint32_t)(pass >> 32), a.key0, a.key1);
-      const float u1 = u1_uniform_open(r.v[0]);
-      b = u1_uniform_open(r.v[1]);
-      float sn, cs;
-      sincospif(2.0f * u1, &sn, &cs);
-      Un = make_float2(cs, sn);
-    }
-    const float dS = a.c.beta * (cre_mul(S, Un) - cre_mul(S, U));
-    return (expf(dS) > b) ? Un : U;
-  }
-  return overrelax_link(S, U);
-}
-
-template <int D, int MU, bool MET, bool REPLAY>
-__global__ void __launch_bounds__(256, 8) k_update_pair(const UpdArgs a) {
-  const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+__device__ __forceinline__ void update_pair_body(const UpdArgs &a, int i) {
   int x[4], k;
   eo_decode_fast<D>(a.g, i, a.p, x, k);
-  pdl_wait_prior_grid();
-  if (!MET && a.bump_ptr != nullptr && blockIdx.x == 0 && threadIdx.x == 0) *a.bump_ptr += a.bump_by;
-  if (i >= a.g.Vh) return;
   if (MU != 3 && a.ml > 0 && (x[D - 1] & (a.ml - 1)) == 0) return;  // freeze rule, src/multilevel.cu:41
   int fwd[4], bwd[4];
   eo_steps<D>(a.g, x, k, fwd, bwd);  // steps of site i; site i+1 shares those along x1..x3
@@ -295,6 +268,36 @@ __global__ void __launch_bounds__(256, 8) k_update_pair(const UpdArgs a) {
   const float2 N0 = update_one<D, MU, MET, REPLAY>(a, i, S0, make_float2(U.x, U.y));
   const float2 N1 = update_one<D, MU, MET, REPLAY>(a, i + 1, S1, make_float2(U.z, U.w));
   *own = make_float4(N0.x, N0.y, N1.x, N1.y);
+}
+
+// Two sites per thread, register budget capped at 32 so 8 CTAs of 256
+// threads fit an SM (a 32^4 phase is then a single wave).
+template <int D, int MU, bool MET, bool REPLAY>
+__global__ void __launch_bounds__(256, 8) k_update_pair(const UpdArgs a) {
+  const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  pdl_wait_prior_grid();
+  if (!MET && a.bump_ptr != nullptr && blockIdx.x == 0 && threadIdx.x == 0) *a.bump_ptr += a.bump_by;
+  if (i < a.g.Vh) update_pair_body<D, MU, MET, REPLAY>(a, i);
+  pdl_release_dependents();
+}
+
+// The same with no register cap (fewer CTAs per SM, no spills).
+template <int D, int MU, bool MET, bool REPLAY>
+__global__ void __launch_bounds__(256) k_update_pair_free(const UpdArgs a) {
+  const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  pdl_wait_prior_grid();
+  if (!MET && a.bump_ptr != nullptr && blockIdx.x == 0 && threadIdx.x == 0) *a.bump_ptr += a.bump_by;
+  if (i < a.g.Vh) update_pair_body<D, MU, MET, REPLAY>(a, i);
+  pdl_release_dependents();
+}
+
+// One site per thread (any geometry, N0/2 odd included).
+template <int D, int MU, bool MET, bool REPLAY>
+__global__ void __launch_bounds__(256) k_update(const UpdArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  pdl_wait_prior_grid();
+  if (!MET && a.bump_ptr != nullptr && blockIdx.x == 0 && threadIdx.x == 0) *a.bump_ptr += a.bump_by;
+  if (i < a.g.Vh) update_single_body<D, MU, MET, REPLAY>(a, i);
   pdl_release_dependents();
 }
 

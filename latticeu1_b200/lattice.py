@@ -151,6 +151,22 @@ class Lattice:
     def set_graphs(self, enable: bool) -> None:
         check(lib.u1_lattice_set_graphs(self._h, int(bool(enable))), "u1_lattice_set_graphs")
 
+    VARIANTS = {0: "auto", 1: "pair32", 2: "pair", 3: "single"}
+
+    @property
+    def variant(self) -> int:
+        v = C.c_int()
+        check(lib.u1_lattice_get_variant(self._h, C.byref(v)), "u1_lattice_get_variant")
+        return int(v.value)
+
+    def set_variant(self, variant: int) -> None:
+        check(lib.u1_lattice_set_variant(self._h, int(variant)), "u1_lattice_set_variant")
+
+    def tune(self, rng: "Rng") -> int:
+        v = C.c_int()
+        check(lib.u1_tune(self._h, rng.handle, C.byref(v)), "u1_tune")
+        return int(v.value)
+
     def links_ptr(self) -> int:
         p = C.c_void_p()
         check(lib.u1_lattice_links(self._h, C.byref(p)), "u1_lattice_links")
@@ -236,6 +252,109 @@ class Lattice:
     def close(self) -> None:
         if self._h:
             lib.u1_lattice_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many independent chains advanced by shared phase launches.
+
+    Chain c follows exactly the trajectory of a single :class:`Lattice`
+    driven by an :class:`Rng` with the same seed and ``set_chain(first_chain
+    + c)`` through the same hot starts and updates.  ``geoms`` is a list of
+    ``(dims, N, beta[, aniso])``; every chain must have the same dims.
+    """
+
+    def __init__(self, ctx: Context, geoms: Sequence, seed: int = 1234, first_chain: int = 0):
+        n = len(geoms)
+        arr = (u1_geom * n)()
+        self.shapes = []
+        for k, gspec in enumerate(geoms):
+            dims, N, beta = int(gspec[0]), list(gspec[1]), float(gspec[2])
+            aniso = float(gspec[3]) if len(gspec) > 3 else 1.0
+            N = N + [0] * (4 - len(N))
+            arr[k] = u1_geom(dims=dims, N=(C.c_int * 4)(*[int(x) for x in N[:4]]), beta=beta, aniso=aniso)
+            info = (C.c_int64 * 8)()
+            check(lib.u1_geom_validate(C.byref(arr[k]), info), f"u1_geom_validate (chain {k})")
+            self.shapes.append((dims, int(info[0])))
+        h = C.c_void_p()
+        check(lib.u1_batch_create(ctx.handle, n, arr, C.c_uint64(seed), C.c_uint32(first_chain), C.byref(h)),
+              "u1_batch_create")
+        self._h = h
+        self.ctx = ctx
+        self.n = n
+        self.seed = int(seed)
+        self.first_chain = int(first_chain)
+        info = (C.c_int64 * 4)()
+        check(lib.u1_batch_info(h, info), "u1_batch_info")
+        self.dims, self.total_links, self.pair_kernels = int(info[1]), int(info[2]), bool(info[3])
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def nlinks(self, chain: int) -> int:
+        dims, V = self.shapes[chain]
+        return dims * V
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        check(lib.u1_batch_set_stream(self._h, C.c_void_p(stream_ptr or 0)), "u1_batch_set_stream")
+
+    def hot_start(self) -> None:
+        check(lib.u1_batch_hot_start(self._h), "u1_batch_hot_start")
+
+    def update(self, metrop: int = 1, ovrn: int = 4, measure: bool = False) -> None:
+        check(lib.u1_batch_update(self._h, int(metrop), int(ovrn), int(bool(measure))), "u1_batch_update")
+
+    @staticmethod
+    def _unpack(a: np.ndarray) -> list[dict]:
+        return [{"plaq_ss": complex(r[0], r[1]), "plaq_st": complex(r[2], r[3]), "poly": complex(r[4], r[5])}
+                for r in a.reshape(-1, 6)]
+
+    def measure_raw(self) -> np.ndarray:
+        out = np.empty(6 * self.n, dtype=np.float64)
+        check(lib.u1_batch_measure(self._h, out.ctypes.data_as(C.POINTER(C.c_double))), "u1_batch_measure")
+        return out.reshape(self.n, 6)
+
+    def measure(self) -> list[dict]:
+        return self._unpack(self.measure_raw())
+
+    def results_raw(self) -> np.ndarray:
+        out = np.empty(6 * self.n, dtype=np.float64)
+        check(lib.u1_batch_results(self._h, out.ctypes.data_as(C.POINTER(C.c_double))), "u1_batch_results")
+        return out.reshape(self.n, 6)
+
+    def results_ptr(self) -> int:
+        p = C.c_void_p()
+        check(lib.u1_batch_results_device(self._h, C.byref(p)), "u1_batch_results_device")
+        return int(p.value)
+
+    def pass_count(self) -> int:
+        v = C.c_uint64()
+        check(lib.u1_batch_get_pass(self._h, C.byref(v)), "u1_batch_get_pass")
+        return int(v.value)
+
+    def import_angles(self, chain: int, theta) -> None:
+        arr = np.ascontiguousarray(theta, dtype=np.float64).reshape(-1)
+        if arr.size != self.nlinks(chain):
+            raise ValueError(f"expected {self.nlinks(chain)} angles, got {arr.size}")
+        check(lib.u1_batch_import_angles(self._h, int(chain), arr.ctypes.data_as(C.c_void_p)),
+              "u1_batch_import_angles")
+
+    def export_angles(self, chain: int) -> np.ndarray:
+        arr = np.empty(self.nlinks(chain), dtype=np.float64)
+        check(lib.u1_batch_export_angles(self._h, int(chain), arr.ctypes.data_as(C.c_void_p)),
+              "u1_batch_export_angles")
+        return arr
+
+    def close(self) -> None:
+        if self._h:
+            lib.u1_batch_destroy(self._h)
             self._h = C.c_void_p()
 
     def __del__(self):

@@ -1,0 +1,176 @@
+"""Update-kernel variants, the autotuner and batched chains (GPU).
+
+* every update variant (two sites per thread with and without the register
+  cap, one site per thread) gives bit-identical links;
+* tuning restores the lattice and the rng pass counter, and caches its pick
+  in $U1_RESOURCE_PATH/u1b200_tunecache.tsv;
+* chain c of a batch is bit-identical to a single lattice driven by an rng
+  with the same seed and chain number first_chain + c, and its measurement
+  agrees with the FP64 oracle to 2e-6.
+"""
+import numpy as np
+import pytest
+
+from latticeu1_b200 import Batch, Lattice, Rng, U1Error
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+# (dims, N, beta, aniso); Nx = 6 gives Nx/2 odd (two-site kernels invalid)
+VARIANT_GEOMS = [
+    (4, (8, 8, 8, 8), 1.0, 1.0),
+    (4, (12, 8, 4, 6), 0.9, 1.3),
+    (4, (6, 4, 4, 8), 1.1, 1.0),
+    (3, (8, 8, 0, 12), 1.2, 0.8),
+    (2, (16, 0, 0, 8), 2.0, 1.0),
+]
+
+
+def _run(ctx, geom, variant, seed=77, chain=0, sweeps=((1, 4), (2, 0), (0, 3))):
+    dims, N, beta, aniso = geom
+    lat = Lattice(ctx, dims, N, beta, aniso)
+    lat.set_variant(variant)
+    rng = Rng(ctx, seed)
+    rng.set_chain(chain)
+    lat.hot_start(rng)
+    for m, o in sweeps:
+        lat.update(rng, m, o)
+    return lat, rng
+
+
+@pytest.mark.parametrize("geom", VARIANT_GEOMS, ids=lambda g: f"{g[0]}d-{'x'.join(map(str, g[1]))}")
+def test_variants_bit_identical(ctx, geom):
+    pair_ok = (geom[1][0] // 2) % 2 == 0
+    results = {}
+    for v in (1, 2, 3):
+        if not pair_ok and v in (1, 2):
+            with pytest.raises(U1Error):
+                Lattice(ctx, *geom[:2], geom[2], geom[3]).set_variant(v)
+            continue
+        lat, _ = _run(ctx, geom, v)
+        results[v] = lat.export_angles()
+    base = results[3]
+    for v, th in results.items():
+        assert np.array_equal(th, base), f"variant {v} differs from the one-site kernel"
+
+
+def test_graphs_and_variants_agree(ctx):
+    geom = (4, (8, 8, 8, 8), 1.0, 1.0)
+    a, _ = _run(ctx, geom, 1)
+    dims, N, beta, aniso = geom
+    b = Lattice(ctx, dims, N, beta, aniso)
+    b.set_graphs(False)
+    b.set_variant(3)
+    rng = Rng(ctx, 77)
+    b.hot_start(rng)
+    for m, o in ((1, 4), (2, 0), (0, 3)):
+        b.update(rng, m, o)
+    assert np.array_equal(a.export_angles(), b.export_angles())
+
+
+def test_tune_restores_state_and_caches(ctx, tmp_path, monkeypatch):
+    monkeypatch.setenv("U1_RESOURCE_PATH", str(tmp_path))
+    lat = Lattice(ctx, 4, (8, 8, 8, 12), 1.0)
+    rng = Rng(ctx, 5)
+    lat.hot_start(rng)
+    lat.set_variant(3)
+    lat.update(rng, 1, 2)
+    th0 = lat.export_angles()
+    st0 = rng.state
+    best = lat.tune(rng)
+    assert best in (1, 2, 3)
+    assert lat.variant == best
+    assert np.array_equal(lat.export_angles(), th0)
+    assert rng.state == st0
+    cache = tmp_path / "u1b200_tunecache.tsv"
+    assert cache.exists()
+    lines = [ln.split("\t") for ln in cache.read_text().splitlines()]
+    assert any(ln[0].endswith("|update|4|8x8x8x12") and int(ln[1]) == best for ln in lines)
+    # the tuned lattice continues the same chain as an untuned one
+    ref = Lattice(ctx, 4, (8, 8, 8, 12), 1.0)
+    ref.set_variant(3)
+    rng2 = Rng(ctx, 5)
+    ref.hot_start(rng2)
+    ref.update(rng2, 1, 2)
+    lat.update(rng, 1, 4)
+    ref.update(rng2, 1, 4)
+    assert np.array_equal(lat.export_angles(), ref.export_angles())
+
+
+def test_auto_variant_tunes_on_first_update(ctx, monkeypatch, tmp_path):
+    monkeypatch.setenv("U1_RESOURCE_PATH", str(tmp_path))
+    monkeypatch.delenv("U1_TUNE", raising=False)
+    lat = Lattice(ctx, 4, (8, 8, 8, 8), 1.0)
+    assert lat.variant == 0
+    rng = Rng(ctx, 9)
+    lat.hot_start(rng)
+    lat.update(rng, 1, 1)
+    assert lat.variant in (1, 2, 3)
+    ref, _ = _run(ctx, (4, (8, 8, 8, 8), 1.0, 1.0), 3, seed=9, sweeps=((1, 1),))
+    assert np.array_equal(lat.export_angles(), ref.export_angles())
+
+
+BATCH_SETS = {
+    "4d-mixed": [(4, (8, 8, 8, 8), 1.0), (4, (12, 8, 4, 8), 0.85, 1.2), (4, (8, 4, 4, 16), 1.15)],
+    "4d-odd-row": [(4, (6, 6, 4, 4), 1.0), (4, (8, 8, 8, 8), 0.9)],
+    "3d": [(3, (8, 8, 0, 8), 1.2), (3, (16, 12, 0, 8), 1.6, 0.9)],
+    "2d": [(2, (16, 0, 0, 16), 2.0), (2, (8, 0, 0, 32), 3.0)],
+}
+
+
+@pytest.mark.parametrize("name", list(BATCH_SETS))
+def test_batch_matches_single_lattices(ctx, name):
+    geoms = BATCH_SETS[name]
+    seed, first = 2024, 17
+    b = Batch(ctx, geoms, seed=seed, first_chain=first)
+    b.hot_start()
+    plan = ((1, 4, False), (2, 0, False), (1, 2, True))
+    for m, o, meas in plan:
+        b.update(m, o, measure=meas)
+    fused = b.results_raw()
+    now = b.measure_raw()
+    assert np.array_equal(fused, now, equal_nan=True)  # 2D: no SS plaquettes (NaN)
+    assert b.pass_count() == 1 + 1 + 2 + 1
+    for c, g in enumerate(geoms):
+        dims, N, beta = g[0], g[1], g[2]
+        aniso = g[3] if len(g) > 3 else 1.0
+        lat = Lattice(ctx, dims, N, beta, aniso)
+        rng = Rng(ctx, seed)
+        rng.set_chain(first + c)
+        lat.hot_start(rng)
+        for m, o, _ in plan:
+            lat.update(rng, m, o)
+        th = b.export_angles(c)
+        assert np.array_equal(th, lat.export_angles()), f"chain {c} differs from its single lattice"
+        single = lat.measure()
+        row = now[c]
+        if dims > 2:
+            assert row[0] == single["plaq_ss"].real and row[1] == single["plaq_ss"].imag
+        assert row[2] == single["plaq_st"].real and row[3] == single["plaq_st"].imag
+        assert row[4] == single["poly"].real and row[5] == single["poly"].imag
+        o = Oracle(dims, N, beta, aniso)
+        ss, st = o.plaquette(th)
+        poly = o.polyakov(th)
+        if dims > 2:
+            assert abs(row[0] - ss.real) < 2e-6 and abs(row[1] - ss.imag) < 2e-6
+        assert abs(row[2] - st.real) < 2e-6 and abs(row[3] - st.imag) < 2e-6
+        assert abs(row[4] - poly.real) < 2e-6 and abs(row[5] - poly.imag) < 2e-6
+
+
+def test_batch_import_export_and_errors(ctx):
+    geoms = [(4, (8, 8, 8, 8), 1.0), (4, (8, 8, 8, 4), 1.0)]
+    b = Batch(ctx, geoms, seed=3)
+    th = np.random.default_rng(1).uniform(0, 2 * np.pi, b.nlinks(1))
+    b.import_angles(1, th)
+    back = b.export_angles(1)
+    d = np.abs(np.angle(np.exp(1j * (back - th))))
+    assert d.max() < 2e-7
+    assert np.all(b.export_angles(0) == 0.0)  # cold
+    with pytest.raises(U1Error):
+        Batch(ctx, [(4, (8, 8, 8, 8), 1.0), (3, (8, 8, 0, 8), 1.0)])
+    with pytest.raises(U1Error):
+        Batch(ctx, [(4, (8, 8, 8, 8), 1.0)] * 2, first_chain=65535)
+    with pytest.raises(U1Error):
+        Batch(ctx, [(4, (7, 8, 8, 8), 1.0)])
+    with pytest.raises(ValueError):
+        b.import_angles(0, th[:10])
