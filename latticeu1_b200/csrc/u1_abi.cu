@@ -884,8 +884,8 @@ extern "C" int u1_update_phase(u1_lattice *lat, u1_rng *rng, int metropolis, int
 template <int D>
 static int launch_measure(u1_lattice *lat, double *dev_out) {
   const GeomK &g = lat->g;
-  const int nbp = measure_plaq_blocks(g);
-  const int nb = nbp + measure_poly_blocks(g);
+  const MeasK m = measure_layout(g);
+  const int nb = m.nb_plaq + m.nb_poly;
   int rc = u1i::ensure_scratch(lat, (size_t)nb * 6, 8);
   if (rc) return rc;
   int nSS = 0, nST = 0;
@@ -894,7 +894,7 @@ static int launch_measure(u1_lattice *lat, double *dev_out) {
   const double normSS = 1.0 / ((double)g.V * nSS);
   const double normST = 1.0 / ((double)g.V * nST);
   const double normL = 1.0 / (double)g.Vs;
-  k_measure<D><<<nb, kRedThreads, 0, lat->stream>>>(lat->links, g, nbp, lat->partials, lat->counter,
+  k_measure<D><<<nb, kRedThreads, 0, lat->stream>>>(lat->links, g, m, lat->partials, lat->counter,
                                                    dev_out ? dev_out : lat->d_out, normSS, normST, normL);
   U1_LAUNCH_CHECK("k_measure");
   return U1_OK;

@@ -32,7 +32,7 @@ struct BatchChain {
   int first_pair;   // first block in the pair (two sites / thread) table
   int first_site;   // first block in the site (one site / thread) table
   int first_meas;   // first block in the measurement table
-  int nb_plaq;      // measurement plaquette blocks (then the Polyakov blocks)
+  MeasK meas;       // measurement layout (plaquette blocks, then Polyakov blocks)
   int nb_meas;
   double norm[3];   // 1/(V nSS), 1/(V nST), 1/V_s
 };
@@ -72,17 +72,13 @@ __global__ void __launch_bounds__(256, 8)
   a.chain = sch.chain;
   a.pass_dev = ph.pass_dev;
   a.hit = ph.hit;
+  a.bump_ptr = ph.bump_ptr;
+  a.bump_by = ph.bump_by;
   const int local = (int)blockIdx.x - (PAIR ? sch.first_pair : sch.first_site);
-  pdl_wait_prior_grid();
-  if (!MET && ph.bump_ptr != nullptr && blockIdx.x == 0 && threadIdx.x == 0) *ph.bump_ptr += ph.bump_by;
-  if (PAIR) {
-    const int i = 2 * (local * blockDim.x + threadIdx.x);
-    if (i < a.g.Vh) update_pair_body<D, MU, MET, false>(a, i);
-  } else {
-    const int i = local * blockDim.x + threadIdx.x;
-    if (i < a.g.Vh) update_single_body<D, MU, MET, false>(a, i);
-  }
-  pdl_release_dependents();
+  if (PAIR)
+    update_pair_body<D, MU, MET, false>(a, 2 * (local * blockDim.x + threadIdx.x));
+  else
+    update_single_body<D, MU, MET, false>(a, local * blockDim.x + threadIdx.x);
 }
 
 template <int D>
@@ -110,14 +106,13 @@ __global__ void __launch_bounds__(kRedThreads)
     k_batch_measure(const BatchChain *__restrict__ chains, const int *__restrict__ block_chain, double *partials) {
   __shared__ BatchChain sch;
   __shared__ double smem[kRedWarps * 6];
+  __shared__ float2 lp[kRedThreads];
   stage_chain(chains, __ldg(block_chain + blockIdx.x), sch);
   float vs[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  measure_block_values<D>(sch.links, sch.g, (int)blockIdx.x - sch.first_meas, sch.nb_plaq, vs);
-  double v[6];
-#pragma unroll
-  for (int k = 0; k < 6; ++k) v[k] = (double)vs[k];
-  block_sum<6>(v, smem);
-  if (threadIdx.x < 6) partials[(size_t)blockIdx.x * 6 + threadIdx.x] = v[0];
+  const int local = (int)blockIdx.x - sch.first_meas;
+  measure_block_values<D>(sch.links, sch.g, local, sch.meas, vs, lp);
+  const double tot = measure_block_total(vs, local < sch.meas.nb_plaq, smem);
+  if (threadIdx.x < 6) partials[(size_t)blockIdx.x * 6 + threadIdx.x] = tot;
 }
 
 // One CTA per chain: sum the chain's measurement blocks in block order.
@@ -126,10 +121,9 @@ __global__ void __launch_bounds__(kRedThreads)
   __shared__ BatchChain sch;
   __shared__ double smem[kRedWarps * 6];
   stage_chain(chains, blockIdx.x, sch);
-  double w[6] = {0, 0, 0, 0, 0, 0};
-  for (int b = threadIdx.x; b < sch.nb_meas; b += blockDim.x)
+  double w[6];
 #pragma unroll
-    for (int k = 0; k < 6; ++k) w[k] += partials[(size_t)(sch.first_meas + b) * 6 + k];
+  for (int k = 0; k < 6; ++k) w[k] = strided_partial_sum(partials + (size_t)sch.first_meas * 6, sch.nb_meas, 6, k);
   block_sum<6>(w, smem);
   if (threadIdx.x < 6) out[(size_t)blockIdx.x * 6 + threadIdx.x] = w[0] * sch.norm[threadIdx.x / 2];
 }
@@ -232,8 +226,8 @@ extern "C" int u1_batch_create(u1_ctx *ctx, int nchains, const u1_geom *geoms, u
     ch.first_pair = (int)tab_pair.size();
     ch.first_site = (int)tab_site.size();
     ch.first_meas = (int)tab_meas.size();
-    ch.nb_plaq = measure_plaq_blocks(g);
-    ch.nb_meas = ch.nb_plaq + measure_poly_blocks(g);
+    ch.meas = measure_layout(g);
+    ch.nb_meas = ch.meas.nb_plaq + ch.meas.nb_poly;
     tab_pair.insert(tab_pair.end(), np, c);
     tab_site.insert(tab_site.end(), ns, c);
     tab_meas.insert(tab_meas.end(), ch.nb_meas, c);

@@ -118,9 +118,7 @@ static __global__ void __launch_bounds__(kRedThreads)
   if (!am_last) return;
   __threadfence();
   for (int k = 0; k < 2 * R; ++k) {
-    double w[1] = {0.0};
-    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
-      w[0] += __ldcg(partials + (size_t)b * 2 * R + k);
+    double w[1] = {strided_partial_sum(partials, gridDim.x, 2 * R, k)};
     block_sum<1>(w, smem);
     if (threadIdx.x == 0) out[k] = w[0] * norm;
   }

@@ -36,8 +36,8 @@ using namespace u1b;
 
 namespace {
 
-// Room for the measurement's plaquette blocks (V/2 / 256 <= 4096) plus its
-// Polyakov blocks (V_s / 256 <= V/2 / 256).
+// Room for the measurement's plaquette blocks (at most V/2 / 256 <= 4096)
+// plus its Polyakov blocks (V_s * chunks / 256 <= V/2 / 256, chunks <= Nt/2).
 constexpr int kNoAllocMaxPlaqBlocks = 4096;
 constexpr int kNoAllocMaxBlocks = 2 * kNoAllocMaxPlaqBlocks;
 constexpr int kNoAllocMaxDevices = 64;
@@ -71,8 +71,12 @@ int noalloc_scratch(double **out) {
 
 template <int D>
 int launch_noalloc(const float2 *links, const GeomK &g, double *scratch, double *out, cudaStream_t s) {
-  const int nbp = measure_plaq_blocks(g);
-  const int nb = nbp + measure_poly_blocks(g);
+  const MeasK m = measure_layout(g);
+  const int nb = m.nb_plaq + m.nb_poly;
+  if (nb > kNoAllocMaxBlocks) {
+    u1i::set_error("u1_measure_noalloc: measurement needs more blocks than the fixed scratch array holds");
+    return U1_ERR_INVALID;
+  }
   unsigned int *counter = reinterpret_cast<unsigned int *>(scratch + (size_t)kNoAllocMaxBlocks * 6);
   U1_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned int), s));
   int nSS = 0, nST = 0;
@@ -81,7 +85,7 @@ int launch_noalloc(const float2 *links, const GeomK &g, double *scratch, double 
   const double normSS = 1.0 / ((double)g.V * nSS);
   const double normST = 1.0 / ((double)g.V * nST);
   const double normL = 1.0 / (double)g.Vs;
-  k_measure<D><<<nb, kRedThreads, 0, s>>>(links, g, nbp, scratch, counter, out, normSS, normST, normL);
+  k_measure<D><<<nb, kRedThreads, 0, s>>>(links, g, m, scratch, counter, out, normSS, normST, normL);
   U1_LAUNCH_CHECK("k_measure (noalloc)");
   return U1_OK;
 }

@@ -166,12 +166,27 @@ __device__ __forceinline__ float2 update_one(const UpdArgs &a, int i, float2 S, 
   return overrelax_link(S, U);
 }
 
-// Body of the one-site-per-thread update of EO site i of phase (a.p, MU);
-// shared by the single-lattice and batched kernels.
+// Body of the one-site-per-thread update of EO site i of phase (a.p, MU)
+// (i >= V/2: only the kernel entry); shared by the single-lattice and
+// batched kernels.
+// Entry of every phase kernel: the site decode (pure arithmetic) runs
+// before it, overlapping the previous grid's tail under programmatic
+// dependent launch.  Waits for the previous grid; an overrelaxation kernel
+// that carries the sweep's pass-counter bump then applies it (block 0).
+// The bodies signal dependents after their store; threads that leave
+// early (out of range, frozen links) count as done when they exit.
+template <bool MET>
+__device__ __forceinline__ void phase_entry(const UpdArgs &a) {
+  pdl_wait_prior_grid();
+  if (!MET && a.bump_ptr != nullptr && blockIdx.x == 0 && threadIdx.x == 0) *a.bump_ptr += a.bump_by;
+}
+
 template <int D, int MU, bool MET, bool REPLAY>
 __device__ __forceinline__ void update_single_body(const UpdArgs &a, int i) {
   int x[4], k;
   eo_decode_fast<D>(a.g, i, a.p, x, k);
+  phase_entry<MET>(a);
+  if (i >= a.g.Vh) return;
   // Multilevel freeze rule, reference src/multilevel.cu:41: update unless the
   // site lies on a frozen time slice (x_t multiple of ml, ml = 2 or 4) and
   // the link is spatial (the reference tests the literal direction index 3).
@@ -181,6 +196,7 @@ __device__ __forceinline__ void update_single_body(const UpdArgs &a, int i) {
   float2 *own = a.lat + MU * a.g.V + a.p * a.g.Vh + i;
   const float2 S = staple_steps<D, MU>(a.lat, a.g, a.c, i, a.p, fwd, bwd);
   *own = update_one<D, MU, MET, REPLAY>(a, i, S, *own);
+  pdl_release_dependents();
 }
 
 // ---------------------------------------------------------------------------
@@ -210,13 +226,16 @@ __device__ __forceinline__ void staple_term2(const Pair2 &a, const Pair2 &b, con
 }
 
 // Body of the two-sites-per-thread update for EO sites i, i+1 (i even) of
-// the phase (a.p, MU); shared by the single-lattice and batched kernels.
+// the phase (a.p, MU) (i >= V/2: only the kernel entry); shared by the
+// single-lattice and batched kernels.
 // Every variant forms the staple and the update with the same operations in
 // the same order, so all of them give bit-identical links.
 template <int D, int MU, bool MET, bool REPLAY>
 __device__ __forceinline__ void update_pair_body(const UpdArgs &a, int i) {
   int x[4], k;
   eo_decode_fast<D>(a.g, i, a.p, x, k);
+  phase_entry<MET>(a);
+  if (i >= a.g.Vh) return;
   if (MU != 3 && a.ml > 0 && (x[D - 1] & (a.ml - 1)) == 0) return;  // freeze rule, src/multilevel.cu:41
   int fwd[4], bwd[4];
   eo_steps<D>(a.g, x, k, fwd, bwd);  // steps of site i; site i+1 shares those along x1..x3
@@ -268,37 +287,26 @@ __device__ __forceinline__ void update_pair_body(const UpdArgs &a, int i) {
   const float2 N0 = update_one<D, MU, MET, REPLAY>(a, i, S0, make_float2(U.x, U.y));
   const float2 N1 = update_one<D, MU, MET, REPLAY>(a, i + 1, S1, make_float2(U.z, U.w));
   *own = make_float4(N0.x, N0.y, N1.x, N1.y);
+  pdl_release_dependents();
 }
 
 // Two sites per thread, register budget capped at 32 so 8 CTAs of 256
 // threads fit an SM (a 32^4 phase is then a single wave).
 template <int D, int MU, bool MET, bool REPLAY>
 __global__ void __launch_bounds__(256, 8) k_update_pair(const UpdArgs a) {
-  const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
-  pdl_wait_prior_grid();
-  if (!MET && a.bump_ptr != nullptr && blockIdx.x == 0 && threadIdx.x == 0) *a.bump_ptr += a.bump_by;
-  if (i < a.g.Vh) update_pair_body<D, MU, MET, REPLAY>(a, i);
-  pdl_release_dependents();
+  update_pair_body<D, MU, MET, REPLAY>(a, 2 * (blockIdx.x * blockDim.x + threadIdx.x));
 }
 
 // The same with no register cap (fewer CTAs per SM, no spills).
 template <int D, int MU, bool MET, bool REPLAY>
 __global__ void __launch_bounds__(256) k_update_pair_free(const UpdArgs a) {
-  const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
-  pdl_wait_prior_grid();
-  if (!MET && a.bump_ptr != nullptr && blockIdx.x == 0 && threadIdx.x == 0) *a.bump_ptr += a.bump_by;
-  if (i < a.g.Vh) update_pair_body<D, MU, MET, REPLAY>(a, i);
-  pdl_release_dependents();
+  update_pair_body<D, MU, MET, REPLAY>(a, 2 * (blockIdx.x * blockDim.x + threadIdx.x));
 }
 
 // One site per thread (any geometry, N0/2 odd included).
 template <int D, int MU, bool MET, bool REPLAY>
 __global__ void __launch_bounds__(256) k_update(const UpdArgs a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  pdl_wait_prior_grid();
-  if (!MET && a.bump_ptr != nullptr && blockIdx.x == 0 && threadIdx.x == 0) *a.bump_ptr += a.bump_by;
-  if (i < a.g.Vh) update_single_body<D, MU, MET, REPLAY>(a, i);
-  pdl_release_dependents();
+  update_single_body<D, MU, MET, REPLAY>(a, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // Hot start (reference src/update.cu:30-48): every link gets
