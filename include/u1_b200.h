@@ -230,6 +230,57 @@ int u1_batch_export_angles(u1_batch *b, int chain, double *angles_host);
 /* Metropolis passes done so far (the rng pass counter of the batch). */
 int u1_batch_get_pass(const u1_batch *b, uint64_t *pass);
 
+/* ------------------------------------------------------------ Wilson action
+ * No counterpart in the reference (which never evaluates the action or its
+ * gradient; its per-plaquette angle is the one summed in src/plaquette.cu:
+ * 93-118, its staple weights include/staple.h:75-102).  For `batch`
+ * configurations theta_dev[b][mu*V + parity*V/2 + eo] (the reference's angle
+ * layout; dtype 0 = float, 1 = double; device memory):
+ *   S_b = beta sum_x sum_{mu<nu} w_{mu nu} (1 - cos theta_P(x)),
+ *   w = 1/aniso (spatial-spatial) or aniso (with the time direction),
+ * out_dev[2b] = S_b and out_dev[2b+1] = the topological charge
+ * Q_b = (1/2pi) sum_x wrap(theta_P(x)) in 2D (0 otherwise), FP64 sums in a
+ * fixed order.  workspace: u1_action_workspace_bytes of device memory.
+ * Nothing is allocated; all work is queued on `stream` (cudaStream_t). */
+int u1_action_workspace_bytes(const u1_geom *geom, int batch, size_t *bytes);
+int u1_wilson_action(const u1_geom *geom, const void *theta_dev, int dtype, int batch, void *workspace,
+                     double *out_dev, void *stream);
+/* Adjoint: grad_dev[b][link] = scale_dev[b] * dS_b/dtheta(link)
+ * = scale * beta sum_{nu != mu} w [sin theta_{mu nu}(x) - sin theta_{mu nu}(x - nu)]
+ * (scale_dev may be NULL for 1), same dtype and layout as theta. */
+int u1_wilson_action_grad(const u1_geom *geom, const void *theta_dev, int dtype, int batch,
+                          const double *scale_dev, void *grad_dev, void *stream);
+
+/* ------------------------------------------------------------------ formats
+ * Replaces ConvLattice_EO_NO (reference src/convertOrder.cu:32-63): FP64
+ * angle arrays (device memory, V*dims doubles) between the even/odd order
+ * theta[eo + parity*V/2 + mu*V] and the natural order theta[lex + mu*V],
+ * lex = x0 + N0*(x1 + N1*(x2 + N2*x3)).  eo_to_no != 0: EO -> NO.  in and
+ * out must not alias.  Queued on `stream`. */
+int u1_convert_order(const u1_geom *geom, const double *in_dev, double *out_dev, int eo_to_no, void *stream);
+/* Replaces PlaquetteFields(lat, field, spacetime, evenoddOrder=true)
+ * (reference src/plaquette_comps.cu:34-107, :220-235; 4D only): the six
+ * components (mu,nu) = (0,3),(1,3),(2,3),(1,2),(2,0),(0,1) of 1 - e^{i theta_P}
+ * as complex FP64 (re, im) pairs.  spacetime != 0: field_dev[2*(lex + d*V)],
+ * one value per site; else field_dev[2*(lex_s + d*V_s)], the time average at
+ * each spatial site (lex_s = x0 + N0*(x1 + N1*x2)).  means = the six
+ * component means (re, im) over the field.  Synchronous. */
+int u1_plaquette_fields(u1_lattice *lat, int spacetime, double *field_dev, double means[12]);
+/* Configuration checkpoints (no counterpart in the reference, which has no
+ * configuration I/O).  Version-1 file: a 128-byte header (magic "U1B200CK",
+ * geometry, beta, aniso, rng seed, pass and chain, flags, CRC-32s), the FP64
+ * angles in the reference's EO layout, and with exact != 0 the float2 links
+ * as well, so that u1_checkpoint_load resumes the chain bit for bit (without
+ * them the links are rebuilt from the angles).  rng may be NULL (saved as
+ * zeros / left unchanged).  Load checks the geometry, the CRCs, sets beta
+ * and aniso from the file and the rng's seed, pass and chain. */
+int u1_checkpoint_save(u1_lattice *lat, const u1_rng *rng, const char *path, int exact);
+int u1_checkpoint_load(u1_lattice *lat, u1_rng *rng, const char *path);
+/* Header of a checkpoint (no device work): geometry in this ABI's
+ * (Nx, Ny, Nz, Nt) convention, rng state and flags (bit 0: exact links). */
+int u1_checkpoint_info(const char *path, u1_geom *geom, uint64_t *seed, uint64_t *pass, uint32_t *chain,
+                       uint32_t *flags);
+
 /* Number of kernels this library has launched in the calling process. */
 int u1_kernel_launch_count(uint64_t *out);
 

@@ -83,6 +83,15 @@ SIGNATURES = {
     "u1_batch_import_angles": [_vp, _i, _vp],
     "u1_batch_export_angles": [_vp, _i, _vp],
     "u1_batch_get_pass": [_vp, C.POINTER(C.c_uint64)],
+    "u1_action_workspace_bytes": [C.POINTER(u1_geom), _i, C.POINTER(C.c_size_t)],
+    "u1_wilson_action": [C.POINTER(u1_geom), _vp, _i, _i, _vp, _vp, _vp],
+    "u1_wilson_action_grad": [C.POINTER(u1_geom), _vp, _i, _i, _vp, _vp, _vp],
+    "u1_convert_order": [C.POINTER(u1_geom), _vp, _vp, _i, _vp],
+    "u1_plaquette_fields": [_vp, _i, _vp, _dp],
+    "u1_checkpoint_save": [_vp, _vp, C.c_char_p, _i],
+    "u1_checkpoint_load": [_vp, _vp, C.c_char_p],
+    "u1_checkpoint_info": [C.c_char_p, C.POINTER(u1_geom), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                           C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
     "u1_kernel_launch_count": [C.POINTER(C.c_uint64)],
     "u1_last_error": [],
     "u1_version": [],

@@ -249,6 +249,35 @@ class Lattice:
         a = np.frombuffer(out, dtype=np.float64).copy()
         return a[0::2] + 1j * a[1::2]
 
+    # -- formats -----------------------------------------------------------
+    def plaquette_fields(self, spacetime: bool = True):
+        """(field, means): field is a complex128 CUDA tensor of shape
+        (6, V) (spacetime) or (6, V_s) (time averages), components
+        (mu,nu) = (0,3),(1,3),(2,3),(1,2),(2,0),(0,1) of 1 - e^{i theta_P},
+        natural site order; means holds the six component means."""
+        import torch
+        n = self.V if spacetime else self.Vs
+        field = torch.empty(12 * n, dtype=torch.float64, device=f"cuda:{self.ctx.device}")
+        means = (C.c_double * 12)()
+        check(lib.u1_plaquette_fields(self._h, int(bool(spacetime)), C.c_void_p(field.data_ptr()), means),
+              "u1_plaquette_fields")
+        m = np.frombuffer(means, dtype=np.float64).copy()
+        return torch.view_as_complex(field.view(6, n, 2)), m[0::2] + 1j * m[1::2]
+
+    def save(self, path, rng: Rng | None = None, exact: bool = True) -> None:
+        """Checkpoint: FP64 angles in the reference layout, the rng state and
+        (exact) the float2 links for a bit-identical resume."""
+        check(lib.u1_checkpoint_save(self._h, rng.handle if rng else None, str(path).encode(), int(bool(exact))),
+              "u1_checkpoint_save")
+
+    def load(self, path, rng: Rng | None = None) -> None:
+        check(lib.u1_checkpoint_load(self._h, rng.handle if rng else None, str(path).encode()),
+              "u1_checkpoint_load")
+        g = u1_geom()
+        check(lib.u1_checkpoint_info(str(path).encode(), C.byref(g), None, None, None, None),
+              "u1_checkpoint_info")
+        self.beta, self.aniso = float(g.beta), float(g.aniso)
+
     def close(self) -> None:
         if self._h:
             lib.u1_lattice_destroy(self._h)
@@ -259,6 +288,34 @@ class Lattice:
             self.close()
         except Exception:
             pass
+
+
+def checkpoint_info(path) -> dict:
+    """Header of a checkpoint through the library (no device work)."""
+    g = u1_geom()
+    seed, pass_, chain, flags = C.c_uint64(), C.c_uint64(), C.c_uint32(), C.c_uint32()
+    check(lib.u1_checkpoint_info(str(path).encode(), C.byref(g), C.byref(seed), C.byref(pass_), C.byref(chain),
+                                 C.byref(flags)), "u1_checkpoint_info")
+    return {"dims": g.dims, "N": tuple(g.N), "beta": g.beta, "aniso": g.aniso, "seed": seed.value,
+            "pass": pass_.value, "chain": chain.value, "flags": flags.value}
+
+
+def convert_order(theta, dims: int, N: Sequence[int], eo_to_no: bool = True):
+    """FP64 angles (CUDA tensor, V*dims) between the even/odd order and the
+    natural order theta[lex + mu V], lex = x0 + N0 (x1 + N1 (x2 + N2 x3));
+    returns a new tensor (queued on torch's current stream)."""
+    import torch
+    N = list(N) + [0] * (4 - len(N))
+    g = u1_geom(dims=int(dims), N=(C.c_int * 4)(*[int(n) for n in N[:4]]), beta=1.0, aniso=1.0)
+    if not (theta.is_cuda and theta.dtype == torch.float64):
+        raise ValueError("convert_order: theta must be a float64 CUDA tensor")
+    src = theta.contiguous()
+    out = torch.empty_like(src)
+    with torch.cuda.device(src.device):
+        stream = torch.cuda.current_stream(src.device).cuda_stream
+        check(lib.u1_convert_order(C.byref(g), C.c_void_p(src.data_ptr()), C.c_void_p(out.data_ptr()),
+                                   int(bool(eo_to_no)), C.c_void_p(stream)), "u1_convert_order")
+    return out
 
 
 class Batch:
