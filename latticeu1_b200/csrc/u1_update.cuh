@@ -182,7 +182,7 @@ __device__ __forceinline__ void phase_entry(const UpdArgs &a) {
 }
 
 template <int D, int MU, bool MET, bool REPLAY>
-__device__ __forceinline__ void update_single_body(const UpdArgs &a, int i) {
+__device__ __forceinline__ void update_single_body(const UpdArgs a, int i) {
   int x[4], k;
   eo_decode_fast<D>(a.g, i, a.p, x, k);
   phase_entry<MET>(a);
@@ -231,7 +231,7 @@ __device__ __forceinline__ void staple_term2(const Pair2 &a, const Pair2 &b, con
 // Every variant forms the staple and the update with the same operations in
 // the same order, so all of them give bit-identical links.
 template <int D, int MU, bool MET, bool REPLAY>
-__device__ __forceinline__ void update_pair_body(const UpdArgs &a, int i) {
+__device__ __forceinline__ void update_pair_body(const UpdArgs a, int i) {
   int x[4], k;
   eo_decode_fast<D>(a.g, i, a.p, x, k);
   phase_entry<MET>(a);
