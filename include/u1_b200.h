@@ -281,6 +281,27 @@ int u1_checkpoint_load(u1_lattice *lat, u1_rng *rng, const char *path);
 int u1_checkpoint_info(const char *path, u1_geom *geom, uint64_t *seed, uint64_t *pass, uint32_t *chain,
                        uint32_t *flags);
 
+/* --------------------------------------------------------- flow transform
+ * No counterpart in the reference.  Elementwise circular coupling transform
+ * of the 2D gauge-equivariant flow (mixture of K <= 8 non-compact
+ * projections on plaquette angles, after Kanwar et al., arXiv:2003.06413).
+ * n elements, FP32 device buffers; params[e*(2K+1) + .] = (a_0..a_{K-1},
+ * logit_0..logit_{K-1}, shift), alpha_k = exp(a_k) (a clamped to [-8, 8]),
+ * w = softmax(logit).  With xc = remainder(x, 2 pi) and
+ * H(xc) = sum_k w_k 2 atan2(alpha_k sin(xc/2), cos(xc/2)):
+ *   forward:  dy = H(xc) + shift - xc,  logd = log H'(xc)
+ *   inverse:  z = remainder(y - shift, 2 pi), xsol solves H(xsol) = z,
+ *             dx = xsol - z - shift,  logd = log H'(xsol)
+ * The backward entry points take the upstream gradients (either may be NULL
+ * for zero) and write the input and parameter gradients.  Queued on `stream`. */
+int u1_ncp_forward(const float *x, const float *params, int64_t n, int K, float *dy, float *logd, void *stream);
+int u1_ncp_backward(const float *x, const float *params, const float *gdy, const float *glogd, int64_t n, int K,
+                    float *gx, float *gparams, void *stream);
+int u1_ncp_inverse(const float *y, const float *params, int64_t n, int K, float *dx, float *xsol, float *logd,
+                   void *stream);
+int u1_ncp_inverse_backward(const float *xsol, const float *params, const float *gdx, const float *glogd, int64_t n,
+                            int K, float *gy, float *gparams, void *stream);
+
 /* Number of kernels this library has launched in the calling process. */
 int u1_kernel_launch_count(uint64_t *out);
 

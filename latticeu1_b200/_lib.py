@@ -92,6 +92,10 @@ SIGNATURES = {
     "u1_checkpoint_load": [_vp, _vp, C.c_char_p],
     "u1_checkpoint_info": [C.c_char_p, C.POINTER(u1_geom), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                            C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
+    "u1_ncp_forward": [_vp, _vp, C.c_int64, _i, _vp, _vp, _vp],
+    "u1_ncp_backward": [_vp, _vp, _vp, _vp, C.c_int64, _i, _vp, _vp, _vp],
+    "u1_ncp_inverse": [_vp, _vp, C.c_int64, _i, _vp, _vp, _vp, _vp],
+    "u1_ncp_inverse_backward": [_vp, _vp, _vp, _vp, C.c_int64, _i, _vp, _vp, _vp],
     "u1_kernel_launch_count": [C.POINTER(C.c_uint64)],
     "u1_last_error": [],
     "u1_version": [],

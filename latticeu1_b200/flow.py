@@ -1,0 +1,338 @@
+"""Gauge-equivariant normalizing flow for 2D U(1) and an independence
+Metropolis-Hastings sampler built on it.
+
+Method after Kanwar et al., "Equivariant flow-based sampling for lattice
+gauge theory", arXiv:2003.06413 (restated, not copied): masked coupling
+layers transform plaquette angles with an invertible circular map whose
+parameters come from a convolutional net over the plaquettes the layer leaves
+unchanged; the updated link absorbs the change of its "active" plaquette, so
+the map is gauge-equivariant and its Jacobian is the product of the circular
+map's derivatives.  The reference has no flow; its 2D Wilson action and
+Metropolis + overrelaxation chain (src/update.cu, include/staple.h) are the
+target distribution and the baseline sampler.
+
+Layout inside the flow: theta[b, mu, x1, x0] (the reference's natural order
+with x0 fastest, include/index.h:51-56), mu = 0 along x0, mu = 1 along x1
+(the time direction of the 2D lattice).  The action is evaluated by the
+library's kernel (latticeu1_b200.action) after a permutation to the
+even/odd layout.
+
+Library kernels on this path: the circular coupling transform and its
+inverse with analytic backward passes (u1_ncp_*), the Wilson action and its
+adjoint (u1_wilson_action*).  The 3x3 convolutions run through cuDNN in
+bfloat16 with FP32 accumulation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+import torch
+from torch import nn
+
+from ._lib import check, lib
+from .action import WilsonAction
+
+__all__ = ["Flow2D", "eo_permutation", "plaquettes_no", "independence_mh", "tau_int", "sample_mc"]
+
+TWO_PI = 2.0 * math.pi
+
+
+def _stream(t: torch.Tensor) -> C.c_void_p:
+    return C.c_void_p(torch.cuda.current_stream(t.device).cuda_stream)
+
+
+def _p(t: torch.Tensor | None) -> C.c_void_p:
+    return C.c_void_p(t.data_ptr() if t is not None else 0)
+
+
+class _NCP(torch.autograd.Function):
+    """(x, params) -> (dy, logd), elementwise; x: (n,), params: (n, 2K+1)."""
+
+    @staticmethod
+    def forward(ctx, x, params, K: int):
+        x = x.contiguous().float()
+        params = params.contiguous().float()
+        n = x.numel()
+        dy = torch.empty_like(x)
+        logd = torch.empty_like(x)
+        with torch.cuda.device(x.device):
+            check(lib.u1_ncp_forward(_p(x), _p(params), n, K, _p(dy), _p(logd), _stream(x)), "u1_ncp_forward")
+        ctx.save_for_backward(x, params)
+        ctx.K = K
+        return dy, logd
+
+    @staticmethod
+    def backward(ctx, gdy, glogd):
+        x, params = ctx.saved_tensors
+        gx = torch.empty_like(x)
+        gp = torch.empty_like(params)
+        gdy = gdy.contiguous().float() if gdy is not None else None
+        glogd = glogd.contiguous().float() if glogd is not None else None
+        with torch.cuda.device(x.device):
+            check(lib.u1_ncp_backward(_p(x), _p(params), _p(gdy), _p(glogd), x.numel(), ctx.K, _p(gx), _p(gp),
+                                      _stream(x)), "u1_ncp_backward")
+        return gx, gp, None
+
+
+class _NCPInverse(torch.autograd.Function):
+    """(y, params) -> (dx, logd) of the inverse map (bisection solve)."""
+
+    @staticmethod
+    def forward(ctx, y, params, K: int):
+        y = y.contiguous().float()
+        params = params.contiguous().float()
+        n = y.numel()
+        dx = torch.empty_like(y)
+        xs = torch.empty_like(y)
+        logd = torch.empty_like(y)
+        with torch.cuda.device(y.device):
+            check(lib.u1_ncp_inverse(_p(y), _p(params), n, K, _p(dx), _p(xs), _p(logd), _stream(y)),
+                  "u1_ncp_inverse")
+        ctx.save_for_backward(xs, params)
+        ctx.K = K
+        return dx, logd
+
+    @staticmethod
+    def backward(ctx, gdx, glogd):
+        xs, params = ctx.saved_tensors
+        gy = torch.empty_like(xs)
+        gp = torch.empty_like(params)
+        gdx = gdx.contiguous().float() if gdx is not None else None
+        glogd = glogd.contiguous().float() if glogd is not None else None
+        with torch.cuda.device(xs.device):
+            check(lib.u1_ncp_inverse_backward(_p(xs), _p(params), _p(gdx), _p(glogd), xs.numel(), ctx.K, _p(gy),
+                                              _p(gp), _stream(xs)), "u1_ncp_inverse_backward")
+        return gy, gp, None
+
+
+def ncp_forward(x, params, K):
+    return _NCP.apply(x, params, K)
+
+
+def ncp_inverse(y, params, K):
+    return _NCPInverse.apply(y, params, K)
+
+
+def plaquettes_no(th: torch.Tensor) -> torch.Tensor:
+    """P(x) = th_0(x) + th_1(x + e0) - th_0(x + e1) - th_1(x) for th[b, mu, x1, x0]."""
+    t0, t1 = th[:, 0], th[:, 1]
+    return t0 + torch.roll(t1, -1, dims=-1) - torch.roll(t0, -1, dims=-2) - t1
+
+
+def eo_permutation(L0: int, L1: int) -> np.ndarray:
+    """perm with theta_eo = theta_no.reshape(B, -1)[:, perm]: the reference's
+    EO link index e = eo + parity V/2 + mu V (include/index.h:114-153) taken
+    from the natural-order index mu V + lex, lex = x0 + L0 x1."""
+    V = L0 * L1
+    lex = np.arange(V)
+    x0, x1 = lex % L0, lex // L0
+    par = (x0 + x1) & 1
+    eo_pos = (lex >> 1) + par * (V // 2)
+    perm = np.empty(2 * V, dtype=np.int64)
+    for mu in range(2):
+        perm[mu * V + eo_pos] = mu * V + lex
+    return perm
+
+
+class Coupling(nn.Module):
+    """One masked coupling layer: links of direction mu at sites with
+    x_nu = off (mod 4), nu = 1 - mu, are updated through the plaquette in
+    which they enter with a + sign; the context is the plaquettes that hold
+    no updated link."""
+
+    def __init__(self, L: int, mu: int, off: int, K: int = 6, hidden: int = 32):
+        super().__init__()
+        self.L, self.mu, self.off, self.K = L, mu, off, K
+        self.net = nn.Sequential(
+            nn.Conv2d(2, hidden, 3, padding=1, padding_mode="circular"),
+            nn.LeakyReLU(),
+            nn.Conv2d(hidden, 2 * K + 1, 3, padding=1, padding_mode="circular"),
+        )
+        nn.init.zeros_(self.net[2].weight)  # start at the identity map (alpha = 1, uniform weights, no shift)
+        nn.init.zeros_(self.net[2].bias)
+        r = np.arange(L)
+        # coordinate along nu (the axis the stripes are offset on), in tensor axes [x1, x0]
+        if mu == 0:
+            link = (r % 4 == off)[:, None] & np.ones(L, bool)[None, :]           # x1 = off
+            active = link                                                       # P(x)
+            frozen = np.isin((r - off) % 4, (1, 2))[:, None] & np.ones(L, bool)[None, :]  # x1 = off+1, off+2
+        else:
+            link = np.ones(L, bool)[:, None] & (r % 4 == off)[None, :]           # x0 = off
+            active = np.ones(L, bool)[:, None] & (r % 4 == (off - 1) % 4)[None, :]  # P(x - e0)
+            frozen = np.ones(L, bool)[:, None] & np.isin((r - off) % 4, (1, 2))[None, :]  # x0 = off+1, off+2
+        # the active plaquette of link (x1, x0) is at (x1, x0) (mu = 0) or (x1, x0 - 1) (mu = 1)
+        li = np.argwhere(link)
+        ai = li.copy()
+        if mu == 1:
+            ai[:, 1] = (ai[:, 1] - 1) % L
+        assert active[ai[:, 0], ai[:, 1]].all()
+        self.register_buffer("link_idx", torch.as_tensor(li[:, 0] * L + li[:, 1]))
+        self.register_buffer("act_idx", torch.as_tensor(ai[:, 0] * L + ai[:, 1]))
+        self.register_buffer("frozen", torch.as_tensor(frozen, dtype=torch.float32)[None, None])
+
+    def _params(self, P: torch.Tensor) -> torch.Tensor:
+        ctx = torch.stack([torch.cos(P), torch.sin(P)], 1) * self.frozen
+        with torch.autocast("cuda", dtype=torch.bfloat16):
+            prm = self.net(ctx)
+        B = P.shape[0]
+        prm = prm.float().reshape(B, 2 * self.K + 1, -1)[:, :, self.act_idx]  # (B, 2K+1, n)
+        return prm.permute(0, 2, 1).reshape(-1, 2 * self.K + 1)
+
+    def _apply_delta(self, th: torch.Tensor, delta: torch.Tensor) -> torch.Tensor:
+        B = th.shape[0]
+        flat = th.reshape(B, 2, -1)
+        upd = flat[:, self.mu].index_add(1, self.link_idx, delta.reshape(B, -1))
+        parts = [upd, flat[:, 1]] if self.mu == 0 else [flat[:, 0], upd]
+        return torch.stack(parts, 1).reshape_as(th)
+
+    def forward(self, th: torch.Tensor):
+        B = th.shape[0]
+        P = plaquettes_no(th)
+        prm = self._params(P)
+        Pa = P.reshape(B, -1)[:, self.act_idx].reshape(-1)
+        dy, logd = ncp_forward(Pa, prm, self.K)
+        return self._apply_delta(th, dy), logd.reshape(B, -1).sum(1)
+
+    def inverse(self, th: torch.Tensor):
+        B = th.shape[0]
+        P = plaquettes_no(th)
+        prm = self._params(P)  # the context plaquettes are unchanged by the layer
+        Pa = P.reshape(B, -1)[:, self.act_idx].reshape(-1)
+        dx, logd = ncp_inverse(Pa, prm, self.K)
+        return self._apply_delta(th, dx), logd.reshape(B, -1).sum(1)
+
+
+class Flow2D(nn.Module):
+    """n_layers coupling layers (mu = l % 2, stripe offset (l // 2) % 4) on
+    an L x L lattice; prior: uniform (Haar) link angles."""
+
+    def __init__(self, L: int, beta: float, n_layers: int = 8, K: int = 6, hidden: int = 32):
+        super().__init__()
+        if L % 4:
+            raise ValueError("L must be a multiple of 4")
+        self.L, self.beta = L, float(beta)
+        self.layers = nn.ModuleList([Coupling(L, l % 2, (l // 2) % 4, K, hidden) for l in range(n_layers)])
+        self.action = WilsonAction(2, (L, 0, 0, L), beta)
+        self.register_buffer("perm", torch.as_tensor(eo_permutation(L, L)))
+        self.log_prior = -2 * L * L * math.log(TWO_PI)
+
+    def to_eo(self, th: torch.Tensor) -> torch.Tensor:
+        return th.reshape(th.shape[0], -1)[:, self.perm]
+
+    def from_eo(self, th_eo: torch.Tensor) -> torch.Tensor:
+        out = torch.empty_like(th_eo)
+        out[:, self.perm] = th_eo
+        return out.reshape(-1, 2, self.L, self.L)
+
+    def sample(self, B: int, generator: torch.Generator | None = None):
+        """(theta, log q(theta)) for B flow samples."""
+        dev = self.perm.device
+        th = torch.rand((B, 2, self.L, self.L), device=dev, generator=generator) * TWO_PI
+        logq = torch.full((B,), self.log_prior, device=dev)
+        for layer in self.layers:
+            th, ld = layer(th)
+            logq = logq - ld
+        return torch.remainder(th, TWO_PI), logq
+
+    def log_prob(self, th: torch.Tensor) -> torch.Tensor:
+        """log q(theta) through the inverse flow."""
+        logq = torch.full((th.shape[0],), self.log_prior, device=th.device)
+        for layer in reversed(self.layers):
+            th, ld = layer.inverse(th)
+            logq = logq - ld
+        return logq
+
+    def S(self, th: torch.Tensor) -> torch.Tensor:
+        return self.action(self.to_eo(th))
+
+    def charge(self, th: torch.Tensor) -> torch.Tensor:
+        return self.action.charge(self.to_eo(th.detach()).double())
+
+    def reverse_kl_step(self, opt, B: int) -> dict:
+        th, logq = self.sample(B)
+        S = self.S(th)
+        loss = (logq + S).mean()
+        opt.zero_grad(set_to_none=True)
+        loss.backward()
+        opt.step()
+        with torch.no_grad():
+            lw = -(S + logq).double()
+            ess = (torch.exp(2 * torch.logsumexp(lw, 0) - torch.logsumexp(2 * lw, 0)) / B).item()
+        return {"loss": loss.item(), "ess": ess}
+
+    def forward_kl_step(self, opt, data: torch.Tensor) -> float:
+        loss = -self.log_prob(data).mean()
+        opt.zero_grad(set_to_none=True)
+        loss.backward()
+        opt.step()
+        return loss.item()
+
+
+def independence_mh(logw: np.ndarray, u: np.ndarray) -> tuple[np.ndarray, float]:
+    """Independence Metropolis-Hastings over proposals with log weights
+    logw = -S - log q, in order: index of the state after each step, and
+    the acceptance rate.  u: uniforms in (0, 1), one per proposal."""
+    n = len(logw)
+    idx = np.empty(n, dtype=np.int64)
+    cur = 0
+    acc = 0
+    for i in range(n):
+        if i > 0 and math.log(u[i]) < logw[i] - logw[cur]:
+            cur = i
+            acc += 1
+        idx[i] = cur
+    return idx, acc / max(1, n - 1)
+
+
+def tau_int(x: np.ndarray, S: float = 1.5) -> tuple[float, float, int]:
+    """Integrated autocorrelation time with Wolff's automatic window
+    (U. Wolff, Comput. Phys. Commun. 156 (2004) 143; the reference's
+    calculateCorTime, src/actime.cpp:19-145): (tau_int, its error, W)."""
+    x = np.asarray(x, dtype=np.float64)
+    N = len(x)
+    d = x - x.mean()
+    f = np.fft.rfft(d, 2 * N)
+    G = np.fft.irfft(f * np.conj(f))[:N] / (N - np.arange(N))
+    if G[0] == 0.0:
+        return 0.5, 0.0, 0
+    W = N // 2
+    acc = 0.0
+    for t in range(1, N // 2):
+        acc += G[t] / G[0]
+        tau = S / math.log((acc + 1.0) / acc) if acc > 0 else 1e-16
+        g = math.exp(-t / tau) - tau / math.sqrt(t * N)
+        if g < 0:
+            W = t
+            break
+    C0 = G[0] + 2 * G[1:W + 1].sum()
+    Gc = G + C0 / N
+    tint = 0.5 + Gc[1:W + 1].sum() / Gc[0]
+    return float(tint), float(tint * 2 * math.sqrt((W - tint + 0.5) / N)), int(W)
+
+
+def sample_mc(L: int, beta: float, n_chains: int, n_per_chain: int, therm: int = 200, every: int = 5,
+              seed: int = 1234, ctx=None) -> np.ndarray:
+    """Configurations from the library's Metropolis + 4 OR chains (batched),
+    natural order theta[b, mu, x1, x0]."""
+    from .lattice import Batch, Context
+    ctx = ctx or Context(0)
+    b = Batch(ctx, [(2, (L, 0, 0, L), beta)] * n_chains, seed=seed)
+    b.hot_start()
+    for _ in range(therm):
+        b.update(1, 4)
+    perm = eo_permutation(L, L)
+    out = np.empty((n_chains * n_per_chain, 2, L, L), dtype=np.float32)
+    k = 0
+    for _ in range(n_per_chain):
+        for _ in range(every):
+            b.update(1, 4)
+        for c in range(n_chains):
+            eo = b.export_angles(c)
+            no = np.empty_like(eo)
+            no[perm] = eo
+            out[k] = no.reshape(2, L, L)
+            k += 1
+    b.close()
+    return out
