@@ -227,6 +227,10 @@ int u1_batch_results_device(u1_batch *b, double **dev_ptr);
 /* Per-chain FP64 angles in the reference's EO layout (as u1_lattice_*_angles). */
 int u1_batch_import_angles(u1_batch *b, int chain, const double *angles_host);
 int u1_batch_export_angles(u1_batch *b, int chain, double *angles_host);
+/* Every chain's FP64 angles into device memory angles_dev (total-links
+ * doubles, chain after chain in creation order, each in the reference's EO
+ * layout).  Asynchronous on the batch's stream. */
+int u1_batch_export_all(u1_batch *b, double *angles_dev);
 /* Metropolis passes done so far (the rng pass counter of the batch). */
 int u1_batch_get_pass(const u1_batch *b, uint64_t *pass);
 

@@ -83,6 +83,7 @@ SIGNATURES = {
     "u1_batch_import_angles": [_vp, _i, _vp],
     "u1_batch_export_angles": [_vp, _i, _vp],
     "u1_batch_get_pass": [_vp, C.POINTER(C.c_uint64)],
+    "u1_batch_export_all": [_vp, _vp],
     "u1_action_workspace_bytes": [C.POINTER(u1_geom), _i, C.POINTER(C.c_size_t)],
     "u1_wilson_action": [C.POINTER(u1_geom), _vp, _i, _i, _vp, _vp, _vp],
     "u1_wilson_action_grad": [C.POINTER(u1_geom), _vp, _i, _i, _vp, _vp, _vp],

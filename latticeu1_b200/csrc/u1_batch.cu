@@ -483,6 +483,16 @@ static int chain_io(u1_batch *b, int chain, double *host, bool import) {
   return U1_OK;
 }
 
+extern "C" int u1_batch_export_all(u1_batch *b, double *angles_dev) {
+  if (!b || !angles_dev) return bfail(U1_ERR_INVALID, "u1_batch_export_all: null argument");
+  U1_CUDA_TRY(cudaSetDevice(b->ctx->device));
+  // chains are stored back to back, so one elementwise pass converts them all
+  k_export_angles<<<nblocks((long long)b->total_links, 256), 256, 0, b->stream>>>(b->links, angles_dev,
+                                                                                  b->total_links);
+  U1_LAUNCH_CHECK("k_export_angles (batch)");
+  return U1_OK;
+}
+
 extern "C" int u1_batch_export_angles(u1_batch *b, int chain, double *angles_host) {
   return chain_io(b, chain, angles_host, false);
 }

@@ -34,7 +34,8 @@ from torch import nn
 from ._lib import check, lib
 from .action import WilsonAction
 
-__all__ = ["Flow2D", "eo_permutation", "plaquettes_no", "independence_mh", "tau_int", "sample_mc"]
+__all__ = ["Flow2D", "eo_permutation", "plaquettes_no", "independence_mh", "tau_int", "sample_mc",
+           "plain_chain_q", "run_experiment"]
 
 TWO_PI = 2.0 * math.pi
 
@@ -174,7 +175,7 @@ class Coupling(nn.Module):
 
     def _params(self, P: torch.Tensor) -> torch.Tensor:
         ctx = torch.stack([torch.cos(P), torch.sin(P)], 1) * self.frozen
-        with torch.autocast("cuda", dtype=torch.bfloat16):
+        with torch.autocast("cuda", dtype=torch.bfloat16, cache_enabled=False):
             prm = self.net(ctx)
         B = P.shape[0]
         prm = prm.float().reshape(B, 2 * self.K + 1, -1)[:, :, self.act_idx]  # (B, 2K+1, n)
@@ -262,6 +263,39 @@ class Flow2D(nn.Module):
             ess = (torch.exp(2 * torch.logsumexp(lw, 0) - torch.logsumexp(2 * lw, 0)) / B).item()
         return {"loss": loss.item(), "ess": ess}
 
+    def graphed_reverse_kl(self, opt, B: int):
+        """The reverse-KL step (sampling, flow, action, backward, optimizer)
+        captured once as a CUDA graph; returns a function that replays it and
+        the static (loss, S, logq) tensors it refreshes.  opt must be built
+        with capturable=True (e.g. Adam(..., capturable=True))."""
+        def body():
+            th, logq = self.sample(B)
+            S = self.S(th)
+            loss = (logq + S).mean()
+            loss.backward()
+            opt.step()
+            return loss.detach(), S.detach(), logq.detach()
+
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            for _ in range(3):  # warm-up outside the graph (allocations, autograd state)
+                opt.zero_grad(set_to_none=False)
+                body()
+        torch.cuda.current_stream().wait_stream(side)
+        graph = torch.cuda.CUDAGraph()
+        opt.zero_grad(set_to_none=False)
+        with torch.cuda.graph(graph):
+            opt.zero_grad(set_to_none=False)
+            static = body()
+
+        def step():
+            graph.replay()
+            return static
+
+        step.graph = graph
+        return step, static
+
     def forward_kl_step(self, opt, data: torch.Tensor) -> float:
         loss = -self.log_prob(data).mean()
         opt.zero_grad(set_to_none=True)
@@ -313,26 +347,155 @@ def tau_int(x: np.ndarray, S: float = 1.5) -> tuple[float, float, int]:
 
 
 def sample_mc(L: int, beta: float, n_chains: int, n_per_chain: int, therm: int = 200, every: int = 5,
-              seed: int = 1234, ctx=None) -> np.ndarray:
-    """Configurations from the library's Metropolis + 4 OR chains (batched),
-    natural order theta[b, mu, x1, x0]."""
+              seed: int = 1234, ctx=None) -> torch.Tensor:
+    """Configurations from the library's Metropolis + 4 OR chains (one batch
+    of n_chains), as a float32 CUDA tensor theta[b, mu, x1, x0]."""
     from .lattice import Batch, Context
     ctx = ctx or Context(0)
     b = Batch(ctx, [(2, (L, 0, 0, L), beta)] * n_chains, seed=seed)
+    stream = torch.cuda.current_stream()
+    b.set_stream(stream.cuda_stream)
     b.hot_start()
     for _ in range(therm):
         b.update(1, 4)
-    perm = eo_permutation(L, L)
-    out = np.empty((n_chains * n_per_chain, 2, L, L), dtype=np.float32)
-    k = 0
-    for _ in range(n_per_chain):
+    perm = torch.as_tensor(eo_permutation(L, L), device="cuda")
+    out = torch.empty((n_per_chain, n_chains, 2 * L * L), dtype=torch.float32, device="cuda")
+    for k in range(n_per_chain):
         for _ in range(every):
             b.update(1, 4)
-        for c in range(n_chains):
-            eo = b.export_angles(c)
-            no = np.empty_like(eo)
-            no[perm] = eo
-            out[k] = no.reshape(2, L, L)
-            k += 1
+        eo = b.export_all().reshape(n_chains, 2 * L * L)
+        out[k][:, perm] = eo.float()
+    torch.cuda.synchronize()
     b.close()
-    return out
+    return out.reshape(-1, 2, L, L)
+
+
+def plain_chain_q(L: int, beta: float, n_chains: int, n_sweeps: int, therm: int = 500, seed: int = 99,
+                  ctx=None) -> tuple[np.ndarray, np.ndarray, float]:
+    """Topological charge and mean cos(theta_P) after every sweep (1 Met + 4 OR)
+    of n_chains independent chains: arrays (n_sweeps, n_chains), and the
+    device seconds per sweep of one chain (batched)."""
+    from .lattice import Batch, Context
+    ctx = ctx or Context(0)
+    b = Batch(ctx, [(2, (L, 0, 0, L), beta)] * n_chains, seed=seed)
+    stream = torch.cuda.current_stream()
+    b.set_stream(stream.cuda_stream)
+    b.hot_start()
+    for _ in range(therm):
+        b.update(1, 4)
+    S = WilsonAction(2, (L, 0, 0, L), beta)
+    q = torch.empty((n_sweeps, n_chains), dtype=torch.float64, device="cuda")
+    pl = torch.empty_like(q)
+    for k in range(n_sweeps):
+        b.update(1, 4)
+        th = b.export_all().reshape(n_chains, 2 * L * L)
+        with torch.no_grad():
+            q[k] = S.charge(th)
+            pl[k] = 1.0 - S(th) / (beta * L * L)
+    # device time of the sweeps alone
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(64):
+        b.update(1, 4)
+    e1.record(stream)
+    e1.synchronize()
+    t_sweep = e0.elapsed_time(e1) * 1e-3 / 64
+    b.close()
+    return q.cpu().numpy(), pl.cpu().numpy(), t_sweep / n_chains
+
+
+def run_experiment(L: int = 16, beta: float = 2.0, n_layers: int = 8, K: int = 6, hidden: int = 32,
+                   batch: int = 1024, n_warm: int = 10000, warm_epochs: int = 10, rkl_steps: int = 1000,
+                   lr: float = 1e-3, n_props: int = 65536, plain_chains: int = 256, plain_sweeps: int = 2048,
+                   seed: int = 0) -> dict:
+    """Config: 2D U(1) L x L at beta; flow of n_layers coupling layers
+    (2 conv 3x3 layers of `hidden` channels each) warm-started by forward KL
+    on n_warm Metropolis + OR configurations and trained by reverse KL; an
+    independence MH chain of n_props flow proposals is compared with plain
+    Metropolis + OR chains: acceptance, <cos theta_P> against the exact
+    I1(beta)/I0(beta) and tau_int of the topological charge."""
+    import time
+
+    from scipy.special import ive
+    torch.manual_seed(seed)
+    res = {"L": L, "beta": beta, "layers": n_layers, "K": K, "hidden": hidden, "batch": batch}
+    flow = Flow2D(L, beta, n_layers, K, hidden).cuda()
+    opt = torch.optim.Adam(flow.parameters(), lr=lr)
+    # warm start: forward KL on Markov-chain configurations
+    t0 = time.perf_counter()
+    per_chain = max(1, n_warm // 1000)
+    data = sample_mc(L, beta, n_warm // per_chain, per_chain, therm=300, every=10, seed=seed + 1)
+    res["warm_data_s"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    fkl = []
+    for ep in range(warm_epochs):
+        idx = torch.randperm(data.shape[0], device="cuda")
+        for i in range(0, data.shape[0] - batch + 1, batch):
+            fkl.append(flow.forward_kl_step(opt, data[idx[i:i + batch]]))
+    torch.cuda.synchronize()
+    res["warm_s"] = time.perf_counter() - t0
+    res["forward_kl_first_last"] = [fkl[0], fkl[-1]] if fkl else None
+    # reverse KL, one CUDA graph per step (optimizer state moved to a capturable Adam)
+    opt2 = torch.optim.Adam(flow.parameters(), lr=lr, capturable=True)
+    opt2.load_state_dict(opt.state_dict())
+    for grp in opt2.param_groups:
+        grp["capturable"] = True
+    for st in opt2.state.values():
+        if "step" in st and not st["step"].is_cuda:
+            st["step"] = st["step"].cuda()
+    step, (loss_t, S_t, logq_t) = flow.graphed_reverse_kl(opt2, batch)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    losses, ess = [], []
+    for it in range(rkl_steps):
+        step()
+        if it % 100 == 0 or it == rkl_steps - 1:
+            lw = -(S_t + logq_t).double()
+            ess.append((torch.exp(2 * torch.logsumexp(lw, 0) - torch.logsumexp(2 * lw, 0)) / batch).item())
+            losses.append(loss_t.item())
+    torch.cuda.synchronize()
+    res["rkl_s"] = time.perf_counter() - t0
+    res["rkl_step_ms"] = 1e3 * res["rkl_s"] / max(1, rkl_steps)
+    res["reverse_kl_loss_first_last"] = [losses[0], losses[-1]] if losses else None
+    res["ess_last"] = float(np.mean(ess[-3:])) if ess else None
+    res["min_loss_exact"] = -(2 * L * L * math.log(TWO_PI) + L * L * math.log(float(ive(0, beta))))
+    # proposals
+    lw, qs, pls = [], [], []
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    with torch.no_grad():
+        for _ in range(n_props // batch):
+            th, logq = flow.sample(batch)
+            S = flow.S(th)
+            lw.append((-S - logq).double())
+            qs.append(flow.charge(th))
+            pls.append(1.0 - S.double() / (beta * L * L))
+    ev1.record()
+    ev1.synchronize()
+    res["proposal_s_per_sample"] = ev0.elapsed_time(ev1) * 1e-3 / (n_props // batch * batch)
+    lw = torch.cat(lw).cpu().numpy()
+    qs = torch.cat(qs).cpu().numpy()
+    pls = torch.cat(pls).cpu().numpy()
+    u = np.random.default_rng(seed + 7).uniform(size=len(lw))
+    idx, acc = independence_mh(lw, u)
+    q_chain, p_chain = qs[idx], pls[idx]
+    res["mh_acceptance"] = acc
+    t_q, dt_q, _ = tau_int(np.round(q_chain))
+    res["flow_tau_int_Q"] = [t_q, dt_q]
+    t_p, _, _ = tau_int(p_chain)
+    exact = float(ive(1, beta) / ive(0, beta))
+    res["exact_cosP"] = exact
+    res["flow_cosP"] = [float(p_chain.mean()), float(p_chain.std() * math.sqrt(2 * t_p / len(p_chain)))]
+    res["flow_Q2"] = float(np.mean(np.round(q_chain) ** 2))
+    # plain Metropolis + OR chains
+    qp, pp, s_sweep = plain_chain_q(L, beta, plain_chains, plain_sweeps, seed=seed + 11)
+    taus = [tau_int(np.round(qp[:, c]))[0] for c in range(plain_chains)]
+    res["plain_tau_int_Q"] = [float(np.mean(taus)), float(np.std(taus) / math.sqrt(plain_chains))]
+    tp = float(np.mean([tau_int(pp[:, c])[0] for c in range(min(plain_chains, 32))]))
+    res["plain_cosP"] = [float(pp.mean()), float(pp.std() * math.sqrt(2 * tp / pp.size))]
+    res["plain_Q2"] = float(np.mean(np.round(qp) ** 2))
+    res["plain_s_per_sweep_per_chain"] = s_sweep
+    # cost of one independent Q sample (2 tau_int steps)
+    res["s_per_indep_Q_flow"] = 2 * t_q * res["proposal_s_per_sample"]
+    res["s_per_indep_Q_plain"] = 2 * res["plain_tau_int_Q"][0] * s_sweep
+    return res

@@ -403,6 +403,16 @@ class Batch:
         check(lib.u1_batch_import_angles(self._h, int(chain), arr.ctypes.data_as(C.c_void_p)),
               "u1_batch_import_angles")
 
+    def export_all(self, out=None):
+        """All chains' FP64 angles as one CUDA tensor (chain after chain, EO
+        layout each); queued on the batch's stream, which the caller orders
+        against its own (e.g. by attaching torch's stream with set_stream)."""
+        import torch
+        if out is None:
+            out = torch.empty(self.total_links, dtype=torch.float64, device=f"cuda:{self.ctx.device}")
+        check(lib.u1_batch_export_all(self._h, C.c_void_p(out.data_ptr())), "u1_batch_export_all")
+        return out
+
     def export_angles(self, chain: int) -> np.ndarray:
         arr = np.empty(self.nlinks(chain), dtype=np.float64)
         check(lib.u1_batch_export_angles(self._h, int(chain), arr.ctypes.data_as(C.c_void_p)),
