@@ -44,6 +44,10 @@ static int fail(int code, const std::string &msg) {
 
 int ensure_scratch(u1_lattice *lat, size_t partial_doubles, size_t out_doubles) {
   if (partial_doubles > lat->partials_cap) {
+    // cached sweep graphs hold the old scratch pointers
+    cudaStreamSynchronize(lat->stream);
+    for (auto &kv : lat->graphs) cudaGraphExecDestroy(kv.second);
+    lat->graphs.clear();
     if (lat->partials) cudaFree(lat->partials);
     lat->partials = nullptr;
     lat->partials_cap = 0;
@@ -517,37 +521,76 @@ static int effective_variant(const u1_lattice *lat) {
   return lat->variant == U1V_AUTO ? default_variant(lat->g) : lat->variant;
 }
 
-template <int D, bool MET>
-static int launch_fused_last(const UpdArgs &a, cudaStream_t s, u1_lattice *lat, double *out) {
-  const GeomK &g = a.g;
-  int nSS = 0, nST = 0;
-  for (int mu = 0; mu < D - 1; ++mu)
-    for (int nu = mu + 1; nu < D; ++nu) (nu == D - 1 ? nST : nSS)++;
-  const double normSS = 1.0 / ((double)g.V * nSS), normST = 1.0 / ((double)g.V * nST);
-  const double normL = 1.0 / (double)g.Vs;
+// Phase (1, MU) of the last pass with the measurement terms (u1_fused.cuh),
+// writing the per-block partials of slot MU-1 into `partials`.
+template <int D, int MU>
+static int launch_meas_phase_mu(const UpdArgs &a, cudaStream_t s, bool met, double *partials) {
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)fused_blocks(g));
-  cfg.blockDim = dim3(kFusedThreads);
+  cfg.gridDim = dim3((unsigned)meas_phase_blocks(a.g));
+  cfg.blockDim = dim3(256);
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cudaError_t e = cudaLaunchKernelEx(&cfg, k_update_last_measure<D, MET>, a, fused_chunks(g), lat->partials,
-                                     lat->counter, out, normSS, normST, normL);
+  double *slot = partials + (size_t)(MU - 1) * meas_phase_blocks(a.g) * 2;
+  cudaError_t e;
+  if ((a.g.hN0 & 1) == 0)
+    e = met ? cudaLaunchKernelEx(&cfg, k_update_pair_meas<D, MU, true>, a, slot)
+            : cudaLaunchKernelEx(&cfg, k_update_pair_meas<D, MU, false>, a, slot);
+  else
+    e = met ? cudaLaunchKernelEx(&cfg, k_update_meas<D, MU, true>, a, slot)
+            : cudaLaunchKernelEx(&cfg, k_update_meas<D, MU, false>, a, slot);
   u1i::g_launches.fetch_add(1, std::memory_order_relaxed);
-  if (e != cudaSuccess) return u1i::cuda_fail(e, "k_update_last_measure");
+  if (e != cudaSuccess) return u1i::cuda_fail(e, "k_update_pair_meas");
+  return U1_OK;
+}
+
+template <int D>
+static int launch_meas_phase(const UpdArgs &a, cudaStream_t s, bool met, double *partials) {
+  switch (a.mu) {
+    case 1: return launch_meas_phase_mu<D, 1>(a, s, met, partials);
+    case 2:
+      if constexpr (D > 2) return launch_meas_phase_mu<D, 2>(a, s, met, partials);
+      break;
+    case 3:
+      if constexpr (D > 3) return launch_meas_phase_mu<D, 3>(a, s, met, partials);
+      break;
+  }
+  return fail(U1_ERR_INVALID, "measuring phase: direction out of range");
+}
+
+// Scratch (doubles) of a measured sweep: D-1 phase slots + Polyakov blocks.
+static size_t meas_sweep_scratch(const GeomK &g) {
+  return (size_t)(g.dims - 1) * meas_phase_blocks(g) * 2 + (size_t)measure_layout(g).nb_poly * 2;
+}
+
+// The Polyakov loops and the final sum of a measured sweep, into dev_out.
+template <int D>
+static int launch_poly_finish(u1_lattice *lat, double *dev_out) {
+  const GeomK &g = lat->g;
+  MeasK m = measure_layout(g);
+  int nSS = 0, nST = 0;
+  for (int mu = 0; mu < D - 1; ++mu)
+    for (int nu = mu + 1; nu < D; ++nu) (nu == D - 1 ? nST : nSS)++;
+  const double normSS = 1.0 / ((double)g.V * nSS), normST = 1.0 / ((double)g.V * nST);
+  const double normL = 1.0 / (double)g.Vs;
+  const int nbp = meas_phase_blocks(g);
+  double *poly = lat->partials + (size_t)(D - 1) * nbp * 2;
+  k_poly_finish<D><<<m.nb_poly, kRedThreads, 0, lat->stream>>>(lat->links, g, m, lat->partials, nbp, poly,
+                                                               lat->counter, dev_out, normSS, normST, normL);
+  U1_LAUNCH_CHECK("k_poly_finish");
   return U1_OK;
 }
 
 // Issue one sweep (metrop Metropolis + ovrn overrelaxation passes) on links
 // `links` with freeze period ml.  The device pass counter advances by metrop.
-// fused_out != nullptr: the sweep's last phase is the fused update +
-// measurement kernel writing the 6 observables to fused_out (needs the
-// lattice scratch sized by ensure_scratch for fused_blocks).
+// meas_partials != nullptr: phases (1, mu >= 1) of the sweep's last pass run
+// as the measuring kernels, writing their partial plaquette sums there
+// (meas_sweep_scratch doubles; k_poly_finish completes the measurement).
 static int issue_sweep(u1_lattice *lat, float2 *links, u1_rng *rng, int metrop, int ovrn, int ml,
-                       double *fused_out = nullptr) {
+                       double *meas_partials = nullptr) {
   UpdArgs a{};
   a.lat = links;
   a.g = lat->g;
@@ -565,14 +608,11 @@ static int issue_sweep(u1_lattice *lat, float2 *links, u1_rng *rng, int metrop, 
   int phase = 0;
   auto launch = [&](bool met) -> int {
     ++phase;
-    if (fused_out && phase == total) {
-      if (met) return D == 2 ? launch_fused_last<2, true>(a, lat->stream, lat, fused_out)
-                     : D == 3 ? launch_fused_last<3, true>(a, lat->stream, lat, fused_out)
-                              : launch_fused_last<4, true>(a, lat->stream, lat, fused_out);
-      return D == 2 ? launch_fused_last<2, false>(a, lat->stream, lat, fused_out)
-           : D == 3 ? launch_fused_last<3, false>(a, lat->stream, lat, fused_out)
-                    : launch_fused_last<4, false>(a, lat->stream, lat, fused_out);
-    }
+    // the last pass is phases total-2D+1 .. total; its parity-1 half with mu >= 1 measures
+    if (meas_partials && phase > total - 2 * D && a.p == 1 && a.mu >= 1)
+      return D == 2 ? launch_meas_phase<2>(a, lat->stream, met, meas_partials)
+           : D == 3 ? launch_meas_phase<3>(a, lat->stream, met, meas_partials)
+                    : launch_meas_phase<4>(a, lat->stream, met, meas_partials);
     const int var = effective_variant(lat);
     return D == 2 ? launch_phase<2>(a, lat->stream, met, met && replay, var)
          : D == 3 ? launch_phase<3>(a, lat->stream, met, met && replay, var)
@@ -789,7 +829,7 @@ extern "C" int u1_lattice_get_variant(const u1_lattice *lat, int *variant) {
   return U1_OK;
 }
 
-static int update_impl(u1_lattice *lat, u1_rng *rng, int metrop, int ovrn, double *fused_out) {
+static int update_impl(u1_lattice *lat, u1_rng *rng, int metrop, int ovrn, double *meas_partials) {
   U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
   int rc = check_replay(lat, rng, metrop);
   if (rc) return rc;
@@ -799,13 +839,13 @@ static int update_impl(u1_lattice *lat, u1_rng *rng, int metrop, int ovrn, doubl
     if (rc) return rc;
   }
   if (lat->use_graphs && !replay) {
-    // graph key: passes, rng object, seed/chain and whether the last phase is fused
-    auto key = std::make_tuple(metrop * 2 + (fused_out ? 1 : 0), ovrn, rng->id,
+    // graph key: passes, rng object, seed/chain and whether the last pass measures
+    auto key = std::make_tuple(metrop * 2 + (meas_partials ? 1 : 0), ovrn, rng->id,
                                rng->seed ^ ((uint64_t)rng->chain << 48));
     auto it = lat->graphs.find(key);
     if (it == lat->graphs.end()) {
       cudaGraphExec_t ex = nullptr;
-      rc = capture_graph(lat, [&]() { return issue_sweep(lat, lat->links, rng, metrop, ovrn, 0, fused_out); },
+      rc = capture_graph(lat, [&]() { return issue_sweep(lat, lat->links, rng, metrop, ovrn, 0, meas_partials); },
                          &ex);
       if (rc) return rc;
       it = lat->graphs.emplace(key, ex).first;
@@ -813,7 +853,7 @@ static int update_impl(u1_lattice *lat, u1_rng *rng, int metrop, int ovrn, doubl
     U1_CUDA_TRY(cudaGraphLaunch(it->second, lat->stream));
     u1i::g_launches += (unsigned long long)(2 * lat->g.dims * (metrop + ovrn) + (ovrn == 0 ? 1 : 0));
   } else {
-    rc = issue_sweep(lat, lat->links, rng, metrop, ovrn, 0, fused_out);
+    rc = issue_sweep(lat, lat->links, rng, metrop, ovrn, 0, meas_partials);
     if (rc) return rc;
   }
   rng->pass += (uint64_t)metrop;
@@ -839,13 +879,15 @@ extern "C" int u1_update_measure(u1_lattice *lat, u1_rng *rng, int metrop, int o
     if (rc) return rc;
     return measure_dispatch(lat, dev_out);
   }
-  int rc = u1i::ensure_scratch(lat, (size_t)fused_blocks(lat->g) * 6, 8);
+  int rc = u1i::ensure_scratch(lat, meas_sweep_scratch(lat->g), 8);
   if (rc) return rc;
-  rc = update_impl(lat, rng, metrop, ovrn, lat->d_out);
+  rc = update_impl(lat, rng, metrop, ovrn, lat->partials);
   if (rc) return rc;
-  if (dev_out != lat->d_out)
-    U1_CUDA_TRY(cudaMemcpyAsync(dev_out, lat->d_out, 6 * sizeof(double), cudaMemcpyDeviceToDevice, lat->stream));
-  return U1_OK;
+  switch (lat->g.dims) {
+    case 2: return launch_poly_finish<2>(lat, dev_out);
+    case 3: return launch_poly_finish<3>(lat, dev_out);
+    default: return launch_poly_finish<4>(lat, dev_out);
+  }
 }
 
 extern "C" int u1_update_phase(u1_lattice *lat, u1_rng *rng, int metropolis, int parity, int mu, int hit) {

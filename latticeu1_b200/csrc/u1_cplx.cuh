@@ -17,6 +17,9 @@ __device__ __forceinline__ float2 cconjmul(float2 a, float2 b) {
   return make_float2(m.x, -m.y);
 }
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// Im(a * b)
+__device__ __forceinline__ float cim_mul(float2 a, float2 b) { return fmaf(a.x, b.y, a.y * b.x); }
 __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
 // wa*a + wb*b with an explicit fused multiply-add, so every kernel that
 // forms a staple rounds it identically (the library is built with

@@ -141,11 +141,13 @@ __host__ inline MeasK measure_layout(const GeomK &g) {
   m.pair = (g.hN0 & 1) == 0;
   const int plaq_threads = m.pair ? g.Vh / 2 : g.Vh;
   m.nb_plaq = (plaq_threads + kRedThreads - 1) / kRedThreads;
-  // largest of 8, 4, 2 dividing Nt with at least two links per chunk
+  // largest of 8, 4, 2 dividing Nt with at least eight links per chunk (a
+  // thread's loads are independent; fewer, fuller blocks cut the per-block
+  // reduction cost), else one chunk
   const int Nt = g.N[g.dims - 1];
   m.chunks = 1;
   for (int c = 8; c > 1; c >>= 1)
-    if (Nt % c == 0 && Nt / c >= 2) {
+    if (Nt % c == 0 && Nt / c >= 8) {
       m.chunks = c;
       break;
     }

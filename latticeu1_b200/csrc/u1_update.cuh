@@ -108,9 +108,13 @@ struct UpdArgs {
 
 // Staple of link (x, MU) from precomputed EO steps (eo_steps): all six
 // neighbour indices of each plaquette pair are i plus one or two steps.
-template <int D, int MU>
+// MEAS: also return, over nu < MU, mA = sum (upper + lower) and
+// mD = sum (upper - lower) (the plaquette terms of the measurement taken from
+// the last pass, see update_pair_body); the staple itself is unchanged.
+template <int D, int MU, bool MEAS = false>
 __device__ __forceinline__ float2 staple_steps(const float2 *__restrict__ lat, const GeomK &g, const CoupK &c,
-                                               int i, int p, const int fwd[4], const int bwd[4]) {
+                                               int i, int p, const int fwd[4], const int bwd[4],
+                                               float2 *mA = nullptr, float2 *mD = nullptr) {
   const int q = 1 - p;
   const float2 *Lq_mu = lat + MU * g.V + q * g.Vh;
   const int i_xm = i + fwd[MU];
@@ -128,11 +132,16 @@ __device__ __forceinline__ float2 staple_steps(const float2 *__restrict__ lat, c
     const float2 d = __ldg(Lp_nu + i_xm + bwd[nu]);
     const float2 e = __ldg(Lq_mu + i + bwd[nu]);
     const float2 f = __ldg(Lq_nu + i + bwd[nu]);
-    const float2 sum = cadd(cmulc(cmulc(a, b), cc), cmul(cconjmul(d, e), f));
+    const float2 up = cmulc(cmulc(a, b), cc), lo = cmul(cconjmul(d, e), f);
+    const float2 sum = cadd(up, lo);
     if (MU == D - 1 || nu == D - 1)
       st = cadd(st, sum);
     else
       ss = cadd(ss, sum);
+    if (MEAS && nu < MU) {
+      *mA = cadd(*mA, sum);
+      *mD = cadd(*mD, csub(up, lo));
+    }
   }
   return cweigh(ss, c.w_ss, st, c.w_st);
 }
@@ -181,8 +190,19 @@ __device__ __forceinline__ void phase_entry(const UpdArgs &a) {
   if (!MET && a.bump_ptr != nullptr && blockIdx.x == 0 && threadIdx.x == 0) *a.bump_ptr += a.bump_by;
 }
 
-template <int D, int MU, bool MET, bool REPLAY>
-__device__ __forceinline__ void update_single_body(const UpdArgs a, int i) {
+// Measurement from the last pass (MEAS): after the final update of the
+// links U_MU at parity-1 sites, every plaquette (nu, MU) with nu < MU holds
+// exactly one such link (its two U_MU links sit at sites of opposite parity)
+// and all its other links are final (directions < MU were updated earlier
+// in the pass, U_MU at parity 0 in phase (0, MU)).  With the new link U' the
+// staple terms give it directly: upper * U' = conj P_{nu MU}(x),
+// lower * U' = P_{nu MU}(x - nu).  So the phase adds, per site,
+//   sum (1 - Re P) = 2 MU - Re(mA U'),   -sum Im P = Im(mD U'),
+// mA = sum_{nu<MU} (upper + lower), mD = sum_{nu<MU} (upper - lower).
+// Phases (1, MU), MU = 1..D-1, of the last pass therefore count every
+// plaquette of the final configuration once, from values already loaded.
+template <int D, int MU, bool MET, bool REPLAY, bool MEAS = false>
+__device__ __forceinline__ void update_single_body(const UpdArgs a, int i, float2 *meas = nullptr) {
   int x[4], k;
   eo_decode_fast<D>(a.g, i, a.p, x, k);
   phase_entry<MET>(a);
@@ -190,13 +210,16 @@ __device__ __forceinline__ void update_single_body(const UpdArgs a, int i) {
   // Multilevel freeze rule, reference src/multilevel.cu:41: update unless the
   // site lies on a frozen time slice (x_t multiple of ml, ml = 2 or 4) and
   // the link is spatial (the reference tests the literal direction index 3).
-  if (MU != 3 && a.ml > 0 && (x[D - 1] & (a.ml - 1)) == 0) return;
+  if (!MEAS && MU != 3 && a.ml > 0 && (x[D - 1] & (a.ml - 1)) == 0) return;
   int fwd[4], bwd[4];
   eo_steps<D>(a.g, x, k, fwd, bwd);
   float2 *own = a.lat + MU * a.g.V + a.p * a.g.Vh + i;
-  const float2 S = staple_steps<D, MU>(a.lat, a.g, a.c, i, a.p, fwd, bwd);
-  *own = update_one<D, MU, MET, REPLAY>(a, i, S, *own);
+  float2 mA = make_float2(0.f, 0.f), mD = mA;
+  const float2 S = staple_steps<D, MU, MEAS>(a.lat, a.g, a.c, i, a.p, fwd, bwd, &mA, &mD);
+  const float2 N = update_one<D, MU, MET, REPLAY>(a, i, S, *own);
+  *own = N;
   pdl_release_dependents();
+  if (MEAS) *meas = make_float2(2.f * MU - cre_mul(mA, N), cim_mul(mD, N));
 }
 
 // ---------------------------------------------------------------------------
@@ -230,13 +253,13 @@ __device__ __forceinline__ void staple_term2(const Pair2 &a, const Pair2 &b, con
 // single-lattice and batched kernels.
 // Every variant forms the staple and the update with the same operations in
 // the same order, so all of them give bit-identical links.
-template <int D, int MU, bool MET, bool REPLAY>
-__device__ __forceinline__ void update_pair_body(const UpdArgs a, int i) {
+template <int D, int MU, bool MET, bool REPLAY, bool MEAS = false>
+__device__ __forceinline__ void update_pair_body(const UpdArgs a, int i, float2 *meas = nullptr) {
   int x[4], k;
   eo_decode_fast<D>(a.g, i, a.p, x, k);
   phase_entry<MET>(a);
   if (i >= a.g.Vh) return;
-  if (MU != 3 && a.ml > 0 && (x[D - 1] & (a.ml - 1)) == 0) return;  // freeze rule, src/multilevel.cu:41
+  if (!MEAS && MU != 3 && a.ml > 0 && (x[D - 1] & (a.ml - 1)) == 0) return;  // freeze rule, src/multilevel.cu:41
   int fwd[4], bwd[4];
   eo_steps<D>(a.g, x, k, fwd, bwd);  // steps of site i; site i+1 shares those along x1..x3
   // x0 steps of the two sites: x0 = 2k+odd and 2k+2+odd
@@ -249,6 +272,7 @@ __device__ __forceinline__ void update_pair_body(const UpdArgs a, int i) {
   const float2 *lat = a.lat;
   const float2 *Lq_mu = lat + MU * V + q * Vh;
   float2 ss0 = make_float2(0.f, 0.f), ss1 = ss0, st0 = ss0, st1 = ss0;
+  float2 mA0 = ss0, mA1 = ss0, mD0 = ss0, mD1 = ss0;  // measurement sums (MEAS), see update_single_body
 #pragma unroll
   for (int nu = 0; nu < D; ++nu) {
     if (nu == MU) continue;
@@ -275,10 +299,27 @@ __device__ __forceinline__ void update_pair_body(const UpdArgs a, int i) {
       E = ld_vec2(Lq_mu, i + bwd[nu]);
       F = ld_vec2(Lq_nu, i + bwd[nu]);
     }
-    if (MU == D - 1 || nu == D - 1)
+    if (MEAS && nu < MU) {
+      // the same operations as staple_term2, with the upper and lower terms kept
+      const float2 up0 = cmulc(cmulc(A.s0, B.s0), C.s0), lo0 = cmul(cconjmul(Dd.s0, E.s0), F.s0);
+      const float2 up1 = cmulc(cmulc(A.s1, B.s1), C.s1), lo1 = cmul(cconjmul(Dd.s1, E.s1), F.s1);
+      const float2 sum0 = cadd(up0, lo0), sum1 = cadd(up1, lo1);
+      if (MU == D - 1) {
+        st0 = cadd(st0, sum0);
+        st1 = cadd(st1, sum1);
+      } else {
+        ss0 = cadd(ss0, sum0);
+        ss1 = cadd(ss1, sum1);
+        mA0 = cadd(mA0, sum0);
+        mA1 = cadd(mA1, sum1);
+      }
+      mD0 = cadd(mD0, csub(up0, lo0));
+      mD1 = cadd(mD1, csub(up1, lo1));
+    } else if (MU == D - 1 || nu == D - 1) {
       staple_term2(A, B, C, Dd, E, F, st0, st1);
-    else
+    } else {
       staple_term2(A, B, C, Dd, E, F, ss0, ss1);
+    }
   }
   const float2 S0 = cweigh(ss0, a.c.w_ss, st0, a.c.w_st);
   const float2 S1 = cweigh(ss1, a.c.w_ss, st1, a.c.w_st);
@@ -288,6 +329,11 @@ __device__ __forceinline__ void update_pair_body(const UpdArgs a, int i) {
   const float2 N1 = update_one<D, MU, MET, REPLAY>(a, i + 1, S1, make_float2(U.z, U.w));
   *own = make_float4(N0.x, N0.y, N1.x, N1.y);
   pdl_release_dependents();
+  if (MEAS) {
+    // for MU = D-1 every nu < MU term is in st: mA = st
+    const float2 a0 = (MU == D - 1) ? st0 : mA0, a1 = (MU == D - 1) ? st1 : mA1;
+    *meas = make_float2(4.f * MU - cre_mul(a0, N0) - cre_mul(a1, N1), cim_mul(mD0, N0) + cim_mul(mD1, N1));
+  }
 }
 
 // Two sites per thread, register budget capped at 32 so 8 CTAs of 256
