@@ -84,8 +84,11 @@ int u1_lattice_set_coupling(u1_lattice *lat, double beta, double aniso);
 int u1_lattice_set_graphs(u1_lattice *lat, int enable);
 /* Update kernel variants, all giving bit-identical links: 1 = two sites per
  * thread (32-register cap, 8 CTAs/SM), 2 = two sites per thread (no cap),
- * 3 = one site per thread; 0 = auto (tuned at the first u1_update).  The
- * two-site variants need Nx/2 even. */
+ * 3 = one site per thread; 0 = auto (tuned at the first u1_update among 1-3).
+ * The two-site variants need Nx/2 even.  4 = the whole sweep as one
+ * persistent cooperative kernel with neighbour-local phase synchronisation
+ * (4D, (Nx/2)*Ny/2 a multiple of 32 in [64, 256], every (z, t) tile resident
+ * at once; opt-in, slower than 1 on B200 at 32^4). */
 int u1_lattice_set_variant(u1_lattice *lat, int variant);
 /* The variant in use: 0 while automatic and not yet tuned. */
 int u1_lattice_get_variant(const u1_lattice *lat, int *variant);

@@ -23,6 +23,7 @@
 
 #include "u1_internal.h"
 #include "u1_fused.cuh"
+#include "u1_wave.cuh"
 #include "u1_multilevel.cuh"
 
 using namespace u1b;
@@ -232,6 +233,7 @@ extern "C" int u1_lattice_destroy(u1_lattice *lat) {
   if (lat->pfield) cudaFree(lat->pfield);
   if (lat->stage) cudaFree(lat->stage);
   if (lat->backup) cudaFree(lat->backup);
+  if (lat->wave_state) cudaFree(lat->wave_state);
   if (lat->own_stream) cudaStreamDestroy(lat->own_stream);
   delete lat;
   return U1_OK;
@@ -316,10 +318,16 @@ extern "C" int u1_lattice_import_angles(u1_lattice *lat, const double *angles, i
   return U1_OK;
 }
 
+static int wave_check(u1_lattice *lat);
+
 extern "C" int u1_lattice_export_angles(const u1_lattice *clat, double *angles, int on_device) {
   if (!clat || !angles) return fail(U1_ERR_INVALID, "u1_lattice_export_angles: null argument");
   u1_lattice *lat = const_cast<u1_lattice *>(clat);  // the staging buffer is a cache
   U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
+  {
+    int rc = wave_check(lat);
+    if (rc) return rc;
+  }
   const size_t n = (size_t)lat->g.V * lat->g.dims;
   double *dst = angles;
   if (!on_device) {
@@ -514,8 +522,79 @@ static int launch_phase(const UpdArgs &a, cudaStream_t s, bool met, bool replay,
 
 // Variant used when the tuner has not chosen one.
 static int default_variant(const GeomK &g) { return (g.hN0 & 1) ? U1V_SINGLE : U1V_PAIR32; }
-static bool variant_valid(const GeomK &g, int v) {
+
+// The persistent sweep needs a fitting geometry, cooperative launch support
+// and every tile's block resident at once.
+static bool wave_usable(u1_lattice *lat) {
+  if (lat->wave_ok >= 0) return lat->wave_ok == 1;
+  lat->wave_ok = 0;
+  const int threads = wave_threads(lat->g);
+  if (!threads) return false;
+  int coop = 0, per_sm = 0;
+  if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, lat->ctx->device) != cudaSuccess || !coop)
+    return false;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_wave<4>, threads, 0) != cudaSuccess)
+    return false;
+  if ((long long)per_sm * lat->ctx->prop.multiProcessorCount < wave_tiles(lat->g)) return false;
+  const size_t n = (size_t)wave_tiles(lat->g) + 2;  // flags, ticket, error word
+  if (cudaMalloc(&lat->wave_state, n * sizeof(unsigned int)) != cudaSuccess) return false;
+  if (cudaMemset(lat->wave_state, 0, n * sizeof(unsigned int)) != cudaSuccess) return false;
+  lat->wave_ok = 1;
+  return true;
+}
+
+static bool variant_valid(u1_lattice *lat, int v) {
+  const GeomK &g = lat->g;
+  if (v == U1V_WAVE) return wave_usable(lat);
   return v == U1V_SINGLE || ((v == U1V_PAIR32 || v == U1V_PAIR) && (g.hN0 & 1) == 0);
+}
+
+// One sweep as a single cooperative launch of k_sweep_wave (see u1_wave.cuh).
+static int launch_wave(u1_lattice *lat, float2 *links, u1_rng *rng, int metrop, int ovrn, double *meas) {
+  WaveArgs w{};
+  w.a.lat = links;
+  w.a.g = lat->g;
+  w.a.c = lat->c;
+  w.a.key0 = (uint32_t)rng->seed;
+  w.a.key1 = (uint32_t)(rng->seed >> 32);
+  w.a.chain = rng->chain;
+  w.a.pass_dev = rng->pass_dev;
+  w.metrop = metrop;
+  w.ovrn = ovrn;
+  w.meas = meas;
+  const int tiles = wave_tiles(lat->g);
+  w.flags = lat->wave_state;
+  w.ticket = lat->wave_state + tiles;
+  w.err = lat->wave_state + tiles + 1;
+  w.pass_rw = rng->pass_dev;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)tiles);
+  cfg.blockDim = dim3((unsigned)wave_threads(lat->g));
+  cfg.stream = lat->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaError_t e = cudaLaunchKernelEx(&cfg, k_sweep_wave<4>, w);
+  u1i::g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (e != cudaSuccess) return u1i::cuda_fail(e, "k_sweep_wave");
+  return U1_OK;
+}
+
+// A wait of the persistent sweep that ran out leaves its phase in the error
+// word; synchronous entry points report it (and clear the state).
+static int wave_check(u1_lattice *lat) {
+  if (lat->wave_ok != 1) return U1_OK;
+  const int tiles = wave_tiles(lat->g);
+  unsigned int err = 0;
+  U1_CUDA_TRY(cudaMemcpyAsync(&err, lat->wave_state + tiles + 1, sizeof(err), cudaMemcpyDeviceToHost, lat->stream));
+  U1_CUDA_TRY(cudaStreamSynchronize(lat->stream));
+  if (!err) return U1_OK;
+  cudaMemsetAsync(lat->wave_state, 0, (tiles + 2) * sizeof(unsigned int), lat->stream);
+  cudaStreamSynchronize(lat->stream);
+  return fail(U1_ERR_CUDA, "persistent sweep: a neighbour wait ran out in phase " + std::to_string(err - 1) +
+                               "; the configuration is invalid");
 }
 static int effective_variant(const u1_lattice *lat) {
   return lat->variant == U1V_AUTO ? default_variant(lat->g) : lat->variant;
@@ -561,9 +640,17 @@ static int launch_meas_phase(const UpdArgs &a, cudaStream_t s, bool met, double 
   return fail(U1_ERR_INVALID, "measuring phase: direction out of range");
 }
 
-// Scratch (doubles) of a measured sweep: D-1 phase slots + Polyakov blocks.
+// Entries per phase slot of a measured sweep: one per block of the measuring
+// phase kernels, or one per tile of the persistent sweep.
+static int meas_slot_entries(const u1_lattice *lat, int variant) {
+  return variant == U1V_WAVE ? wave_tiles(lat->g) : meas_phase_blocks(lat->g);
+}
+
+// Scratch (doubles) of a measured sweep: D-1 phase slots + Polyakov blocks
+// (sized for either layout).
 static size_t meas_sweep_scratch(const GeomK &g) {
-  return (size_t)(g.dims - 1) * meas_phase_blocks(g) * 2 + (size_t)measure_layout(g).nb_poly * 2;
+  const size_t slot = (size_t)std::max(meas_phase_blocks(g), wave_tiles(g));
+  return (size_t)(g.dims - 1) * slot * 2 + (size_t)measure_layout(g).nb_poly * 2;
 }
 
 // The Polyakov loops and the final sum of a measured sweep, into dev_out.
@@ -576,7 +663,7 @@ static int launch_poly_finish(u1_lattice *lat, double *dev_out) {
     for (int nu = mu + 1; nu < D; ++nu) (nu == D - 1 ? nST : nSS)++;
   const double normSS = 1.0 / ((double)g.V * nSS), normST = 1.0 / ((double)g.V * nST);
   const double normL = 1.0 / (double)g.Vs;
-  const int nbp = meas_phase_blocks(g);
+  const int nbp = meas_slot_entries(lat, effective_variant(lat));
   double *poly = lat->partials + (size_t)(D - 1) * nbp * 2;
   k_poly_finish<D><<<m.nb_poly, kRedThreads, 0, lat->stream>>>(lat->links, g, m, lat->partials, nbp, poly,
                                                                lat->counter, dev_out, normSS, normST, normL);
@@ -603,6 +690,8 @@ static int issue_sweep(u1_lattice *lat, float2 *links, u1_rng *rng, int metrop, 
   a.replay_base = rng->replay_base;
   a.ml = ml;
   const bool replay = rng->replay_dev != nullptr;
+  if (ml == 0 && !replay && effective_variant(lat) == U1V_WAVE)
+    return launch_wave(lat, links, rng, metrop, ovrn, meas_partials);
   const int D = lat->g.dims;
   const int total = 2 * D * (metrop + ovrn);
   int phase = 0;
@@ -727,7 +816,7 @@ void tune_load_locked(TuneCache &c) {
     const size_t t2 = line.find('\t', t1 + 1);
     const std::string key = line.substr(0, t1);
     const int v = std::atoi(line.substr(t1 + 1, t2 == std::string::npos ? std::string::npos : t2 - t1 - 1).c_str());
-    if (v >= U1V_PAIR32 && v <= U1V_SINGLE) c.best[key] = v;
+    if (v >= U1V_PAIR32 && v <= U1V_WAVE) c.best[key] = v;
   }
 }
 void tune_save(const std::string &key, int v, double us) {
@@ -745,15 +834,15 @@ static int tune_update(u1_lattice *lat, u1_rng *rng, bool use_cache) {
     std::lock_guard<std::mutex> lock(c.mu);
     tune_load_locked(c);
     auto it = c.best.find(key);
-    if (it != c.best.end() && variant_valid(lat->g, it->second)) {
+    if (it != c.best.end() && variant_valid(lat, it->second)) {
       lat->variant = it->second;
       drop_graphs(lat);
       return U1_OK;
     }
   }
   std::vector<int> cand;
-  for (int v : {U1V_PAIR32, U1V_PAIR, U1V_SINGLE})
-    if (variant_valid(lat->g, v)) cand.push_back(v);
+  for (int v : {U1V_PAIR32, U1V_PAIR, U1V_SINGLE})  // the persistent sweep is opt-in (u1_wave.cuh)
+    if (variant_valid(lat, v)) cand.push_back(v);
   int best = cand[0];
   double best_us = -1.0;
   if (cand.size() > 1) {
@@ -816,7 +905,7 @@ extern "C" int u1_tune(u1_lattice *lat, u1_rng *rng, int *variant) {
 
 extern "C" int u1_lattice_set_variant(u1_lattice *lat, int variant) {
   if (!lat) return fail(U1_ERR_INVALID, "u1_lattice_set_variant: null lattice");
-  if (variant != U1V_AUTO && !variant_valid(lat->g, variant))
+  if (variant != U1V_AUTO && !variant_valid(lat, variant))
     return fail(U1_ERR_INVALID, "u1_lattice_set_variant: variant not valid for this geometry (pair variants need Nx/2 even)");
   lat->variant = variant;
   drop_graphs(lat);
@@ -838,7 +927,7 @@ static int update_impl(u1_lattice *lat, u1_rng *rng, int metrop, int ovrn, doubl
     rc = tune_update(lat, rng, true);
     if (rc) return rc;
   }
-  if (lat->use_graphs && !replay) {
+  if (lat->use_graphs && !replay && effective_variant(lat) != U1V_WAVE) {
     // graph key: passes, rng object, seed/chain and whether the last pass measures
     auto key = std::make_tuple(metrop * 2 + (meas_partials ? 1 : 0), ovrn, rng->id,
                                rng->seed ^ ((uint64_t)rng->chain << 48));
@@ -959,7 +1048,9 @@ extern "C" int u1_measure_async(u1_lattice *lat, double *dev_out) {
 extern "C" int u1_measure(u1_lattice *lat, double out[6]) {
   if (!lat || !out) return fail(U1_ERR_INVALID, "u1_measure: null argument");
   U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
-  int rc = u1i::ensure_scratch(lat, 0, 8);
+  int rc = wave_check(lat);
+  if (rc) return rc;
+  rc = u1i::ensure_scratch(lat, 0, 8);
   if (rc) return rc;
   rc = measure_dispatch(lat, nullptr);
   if (rc) return rc;

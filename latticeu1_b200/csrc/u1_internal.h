@@ -29,7 +29,7 @@ struct u1_rng {
 };
 
 // Update kernel variants (all bit-identical; the tuner picks the fastest).
-enum : int { U1V_AUTO = 0, U1V_PAIR32 = 1, U1V_PAIR = 2, U1V_SINGLE = 3 };
+enum : int { U1V_AUTO = 0, U1V_PAIR32 = 1, U1V_PAIR = 2, U1V_SINGLE = 3, U1V_WAVE = 4 };
 
 struct u1_lattice {
   u1_ctx *ctx = nullptr;
@@ -54,6 +54,9 @@ struct u1_lattice {
   bool use_graphs = true;
   int variant = U1V_AUTO;          // update kernel variant (U1V_AUTO: tune on first update)
   float2 *backup = nullptr;        // link backup used while tuning
+  // persistent sweep (U1V_WAVE): per-tile phase flags, then ticket and error word
+  unsigned int *wave_state = nullptr;
+  int wave_ok = -1;                // -1 unknown, 0 not usable, 1 usable
 };
 
 namespace u1i {

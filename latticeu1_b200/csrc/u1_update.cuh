@@ -233,12 +233,19 @@ struct Pair2 {
   float2 s0, s1;
 };
 
-__device__ __forceinline__ Pair2 ld_vec2(const float2 *__restrict__ base, int idx) {
-  const float4 t = __ldg(reinterpret_cast<const float4 *>(base + idx));
+// COH = false: read-only (non-coherent) loads, valid because a phase kernel
+// never reads what it writes.  COH = true: ordinary coherent (L1-cached) loads,
+// for the persistent sweep kernel that reads links other blocks wrote earlier
+// in the same launch (ordered by its acquire fences).
+template <bool COH = false>
+__device__ __forceinline__ Pair2 ld_vec2(const float2 *base, int idx) {
+  const float4 *p = reinterpret_cast<const float4 *>(base + idx);
+  const float4 t = COH ? __ldca(p) : __ldg(p);
   return Pair2{make_float2(t.x, t.y), make_float2(t.z, t.w)};
 }
-__device__ __forceinline__ Pair2 ld_two(const float2 *__restrict__ base, int i0, int i1) {
-  return Pair2{__ldg(base + i0), __ldg(base + i1)};
+template <bool COH = false>
+__device__ __forceinline__ Pair2 ld_two(const float2 *base, int i0, int i1) {
+  return COH ? Pair2{__ldca(base + i0), __ldca(base + i1)} : Pair2{__ldg(base + i0), __ldg(base + i1)};
 }
 
 // upper + lower staple contributions of one nu for both sites
@@ -253,7 +260,7 @@ __device__ __forceinline__ void staple_term2(const Pair2 &a, const Pair2 &b, con
 // single-lattice and batched kernels.
 // Every variant forms the staple and the update with the same operations in
 // the same order, so all of them give bit-identical links.
-template <int D, int MU, bool MET, bool REPLAY, bool MEAS = false>
+template <int D, int MU, bool MET, bool REPLAY, bool MEAS = false, bool COH = false>
 __device__ __forceinline__ void update_pair_body(const UpdArgs a, int i, float2 *meas = nullptr) {
   int x[4], k;
   eo_decode_fast<D>(a.g, i, a.p, x, k);
@@ -279,25 +286,25 @@ __device__ __forceinline__ void update_pair_body(const UpdArgs a, int i, float2 
     const float2 *Lp_nu = lat + nu * V + a.p * Vh;
     const float2 *Lq_nu = lat + nu * V + q * Vh;
     Pair2 A, B, C, Dd, E, F;
-    C = ld_vec2(Lp_nu, i);
+    C = ld_vec2<COH>(Lp_nu, i);
     if (MU == 0) {  // nu != 0: steps along nu shared, along x0 per site
-      A = ld_two(Lq_nu, i + f0a, i + 1 + f0b);
-      B = ld_vec2(Lq_mu, i + fwd[nu]);
-      Dd = ld_two(Lp_nu, i + f0a + bwd[nu], i + 1 + f0b + bwd[nu]);
-      E = ld_vec2(Lq_mu, i + bwd[nu]);
-      F = ld_vec2(Lq_nu, i + bwd[nu]);
+      A = ld_two<COH>(Lq_nu, i + f0a, i + 1 + f0b);
+      B = ld_vec2<COH>(Lq_mu, i + fwd[nu]);
+      Dd = ld_two<COH>(Lp_nu, i + f0a + bwd[nu], i + 1 + f0b + bwd[nu]);
+      E = ld_vec2<COH>(Lq_mu, i + bwd[nu]);
+      F = ld_vec2<COH>(Lq_nu, i + bwd[nu]);
     } else if (nu == 0) {  // MU != 0
-      A = ld_vec2(Lq_nu, i + fwd[MU]);
-      B = ld_two(Lq_mu, i + f0a, i + 1 + f0b);
-      Dd = ld_two(Lp_nu, i + fwd[MU] + b0a, i + 1 + fwd[MU] + b0b);
-      E = ld_two(Lq_mu, i + b0a, i + 1 + b0b);
-      F = ld_two(Lq_nu, i + b0a, i + 1 + b0b);
+      A = ld_vec2<COH>(Lq_nu, i + fwd[MU]);
+      B = ld_two<COH>(Lq_mu, i + f0a, i + 1 + f0b);
+      Dd = ld_two<COH>(Lp_nu, i + fwd[MU] + b0a, i + 1 + fwd[MU] + b0b);
+      E = ld_two<COH>(Lq_mu, i + b0a, i + 1 + b0b);
+      F = ld_two<COH>(Lq_nu, i + b0a, i + 1 + b0b);
     } else {  // MU != 0, nu != 0: every step even, all loads 128-bit
-      A = ld_vec2(Lq_nu, i + fwd[MU]);
-      B = ld_vec2(Lq_mu, i + fwd[nu]);
-      Dd = ld_vec2(Lp_nu, i + fwd[MU] + bwd[nu]);
-      E = ld_vec2(Lq_mu, i + bwd[nu]);
-      F = ld_vec2(Lq_nu, i + bwd[nu]);
+      A = ld_vec2<COH>(Lq_nu, i + fwd[MU]);
+      B = ld_vec2<COH>(Lq_mu, i + fwd[nu]);
+      Dd = ld_vec2<COH>(Lp_nu, i + fwd[MU] + bwd[nu]);
+      E = ld_vec2<COH>(Lq_mu, i + bwd[nu]);
+      F = ld_vec2<COH>(Lq_nu, i + bwd[nu]);
     }
     if (MEAS && nu < MU) {
       // the same operations as staple_term2, with the upper and lower terms kept

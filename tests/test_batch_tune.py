@@ -174,3 +174,54 @@ def test_batch_import_export_and_errors(ctx):
         Batch(ctx, [(4, (7, 8, 8, 8), 1.0)])
     with pytest.raises(ValueError):
         b.import_angles(0, th[:10])
+
+
+# geometries where the persistent sweep (variant 4) fits: N0/2 * N1 / 2 threads in [64, 256]
+WAVE_GEOMS = [(4, (16, 16, 8, 8), 1.0, 1.0), (4, (32, 16, 6, 4), 0.9, 1.4), (4, (32, 32, 32, 32), 1.0, 1.0)]
+
+
+@pytest.mark.parametrize("geom", WAVE_GEOMS, ids=lambda g: "x".join(map(str, g[1])))
+def test_wave_sweep_bit_identical(ctx, geom):
+    """The persistent sweep gives the phase kernels' links bit for bit, for
+    mixed, Metropolis-only and overrelaxation-only sweeps."""
+    dims, N, beta, aniso = geom
+    sweeps = ((1, 4), (2, 0), (0, 3), (1, 1))
+    ref, rr = _run(ctx, geom, 1, seed=31, sweeps=sweeps)
+    lat = Lattice(ctx, dims, N, beta, aniso)
+    try:
+        lat.set_variant(4)
+    except U1Error:
+        pytest.skip("persistent sweep not usable on this device")
+    rng = Rng(ctx, 31)
+    lat.hot_start(rng)
+    for m, o in sweeps:
+        lat.update(rng, m, o)
+    assert np.array_equal(lat.export_angles(), ref.export_angles())
+    assert rng.state == rr.state
+
+
+@pytest.mark.parametrize("geom", WAVE_GEOMS[:2], ids=lambda g: "x".join(map(str, g[1])))
+def test_wave_measured_sweep(ctx, geom):
+    import torch
+    dims, N, beta, aniso = geom
+    a = Lattice(ctx, dims, N, beta, aniso)
+    b = Lattice(ctx, dims, N, beta, aniso)
+    try:
+        a.set_variant(4)
+    except U1Error:
+        pytest.skip("persistent sweep not usable on this device")
+    b.set_variant(1)
+    ra, rb = Rng(ctx, 8), Rng(ctx, 8)
+    a.hot_start(ra)
+    b.hot_start(rb)
+    out = torch.zeros(6, dtype=torch.float64, device="cuda")
+    for m, o in ((1, 4), (2, 0)):
+        a.update_measure(ra, m, o, out.data_ptr())
+        b.update(rb, m, o)
+        torch.cuda.synchronize()
+        assert np.array_equal(a.export_angles(), b.export_angles())
+        want = b.measure()
+        got = out.cpu().numpy()
+        assert abs(complex(got[0], got[1]) - want["plaq_ss"]) < 2e-6
+        assert abs(complex(got[2], got[3]) - want["plaq_st"]) < 2e-6
+        assert abs(complex(got[4], got[5]) - want["poly"]) < 2e-6
