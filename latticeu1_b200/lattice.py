@@ -188,10 +188,20 @@ class Lattice:
         check(lib.u1_lattice_import_angles(self._h, arr.ctypes.data_as(C.c_void_p), 0), "u1_lattice_import_angles")
 
     def export_angles(self, out=None) -> np.ndarray:
+        """FP64 angles in the reference layout: into `out` (a CUDA float64
+        tensor, or a contiguous float64 host array, e.g. pinned memory) or a
+        new numpy array."""
         if out is not None and hasattr(out, "is_cuda") and out.is_cuda:
             check(lib.u1_lattice_export_angles(self._h, C.c_void_p(out.data_ptr()), 1), "u1_lattice_export_angles")
             return out
-        arr = np.empty(self.nlinks, dtype=np.float64)
+        if out is not None:
+            if hasattr(out, "numpy"):  # host torch tensor (possibly pinned)
+                out = out.numpy()
+            if out.dtype != np.float64 or not out.flags.c_contiguous or out.size != self.nlinks:
+                raise ValueError(f"out must be a contiguous float64 array of {self.nlinks} angles")
+            arr = out
+        else:
+            arr = np.empty(self.nlinks, dtype=np.float64)
         check(lib.u1_lattice_export_angles(self._h, arr.ctypes.data_as(C.c_void_p), 0), "u1_lattice_export_angles")
         return arr
 

@@ -378,3 +378,21 @@ def test_fused_measurement_sweep(ctx, dims, N, beta, aniso, metrop, ovrn):
         assert abs(complex(got[2], got[3]) - want["plaq_st"]) < 2e-6
         assert abs(complex(got[4], got[5]) - want["poly"]) < 2e-6
     assert ra.state == rb.state
+
+
+def test_export_into_caller_buffers(ctx):
+    """export_angles writes into a caller's host array / pinned tensor / CUDA tensor."""
+    import torch
+    lat = Lattice(ctx, 4, (8, 6, 4, 6), 1.0)
+    lat.hot_start(Rng(ctx, 3))
+    ref = lat.export_angles()
+    host = np.zeros(lat.nlinks)
+    assert lat.export_angles(host) is host and np.array_equal(host, ref)
+    pinned = torch.zeros(lat.nlinks, dtype=torch.float64, pin_memory=True)
+    lat.export_angles(pinned)
+    assert np.array_equal(pinned.numpy(), ref)
+    dev = torch.zeros(lat.nlinks, dtype=torch.float64, device="cuda")
+    lat.export_angles(dev)
+    assert np.array_equal(dev.cpu().numpy(), ref)
+    with pytest.raises(ValueError):
+        lat.export_angles(np.zeros(lat.nlinks, dtype=np.float32))
