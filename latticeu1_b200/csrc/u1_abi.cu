@@ -1157,27 +1157,65 @@ extern "C" int u1_multilevel(u1_lattice *lat, u1_rng *rng, int n4, int k4, int n
     cleanup();
     return rc;
   }
+  // The level-4 update (k4 sweeps, freeze period 4) and one level-2
+  // sub-update (k2 sweeps with freeze period 2, the multihit field, the T2
+  // accumulation) are each captured once as a CUDA graph and replayed; the
+  // Metropolis pass counter lives in device memory, so replays draw fresh
+  // numbers exactly as direct launches would.
+  auto level4 = [&]() -> int {
+    for (int j = 0; j < k4; ++j) {
+      int r = issue_sweep(lat, work, rng, metrop, ovrn, 4);
+      if (r) return r;
+    }
+    return U1_OK;
+  };
+  auto level2 = [&]() -> int {
+    for (int l = 0; l < k2; ++l) {
+      int r = issue_sweep(lat, work, rng, metrop, ovrn, 2);
+      if (r) return r;
+    }
+    k_ml_mhit_field<4><<<u1i::blocks_for(g.V, 256), 256, 0, lat->stream>>>(work, g, lat->c, mh);
+    U1_LAUNCH_CHECK("k_ml_mhit_field");
+    k_ml_T2<<<nb_ps, 256, 0, lat->stream>>>(mh, g, R, T2);
+    U1_LAUNCH_CHECK("k_ml_T2");
+    return U1_OK;
+  };
+  const unsigned long long per_sweep = 2ull * g.dims * (metrop + ovrn) + (ovrn == 0 ? 1 : 0);
+  const bool graphed = lat->use_graphs && !rng->replay_dev;
+  cudaGraphExec_t g4 = nullptr, g2 = nullptr;
   auto body = [&]() -> int {
     U1_CUDA_TRY(cudaMemcpyAsync(work, lat->links, (size_t)g.V * g.dims * sizeof(float2),
                                 cudaMemcpyDeviceToDevice, lat->stream));
     U1_CUDA_TRY(cudaMemsetAsync(T4, 0, size * nl4 * sizeof(double2), lat->stream));
-    for (int i = 0; i < n4; ++i) {
-      for (int j = 0; j < k4; ++j) {
-        int r = issue_sweep(lat, work, rng, metrop, ovrn, 4);
+    if (graphed) {
+      if (k4 > 0) {
+        int r = capture_graph(lat, level4, &g4);
         if (r) return r;
-        rng->pass += (uint64_t)metrop;
       }
+      int r = capture_graph(lat, level2, &g2);
+      if (r) return r;
+    }
+    for (int i = 0; i < n4; ++i) {
+      if (graphed) {
+        if (k4 > 0) {
+          U1_CUDA_TRY(cudaGraphLaunch(g4, lat->stream));
+          u1i::g_launches += per_sweep * (unsigned long long)k4;
+        }
+      } else {
+        int r = level4();
+        if (r) return r;
+      }
+      rng->pass += (uint64_t)metrop * (uint64_t)k4;
       U1_CUDA_TRY(cudaMemsetAsync(T2, 0, size * nl2 * sizeof(double2), lat->stream));
       for (int k = 0; k < n2; ++k) {
-        for (int l = 0; l < k2; ++l) {
-          int r = issue_sweep(lat, work, rng, metrop, ovrn, 2);
+        if (graphed) {
+          U1_CUDA_TRY(cudaGraphLaunch(g2, lat->stream));
+          u1i::g_launches += per_sweep * (unsigned long long)k2 + 2ull;
+        } else {
+          int r = level2();
           if (r) return r;
-          rng->pass += (uint64_t)metrop;
         }
-        k_ml_mhit_field<4><<<u1i::blocks_for(g.V, 256), 256, 0, lat->stream>>>(work, g, lat->c, mh);
-        U1_LAUNCH_CHECK("k_ml_mhit_field");
-        k_ml_T2<<<nb_ps, 256, 0, lat->stream>>>(mh, g, R, T2);
-        U1_LAUNCH_CHECK("k_ml_T2");
+        rng->pass += (uint64_t)metrop * (uint64_t)k2;
       }
       k_ml_T4<<<nb_ps, 256, 0, lat->stream>>>(T2, g, R, 1.0 / (double)n2, T4);
       U1_LAUNCH_CHECK("k_ml_T4");
@@ -1200,6 +1238,8 @@ extern "C" int u1_multilevel(u1_lattice *lat, u1_rng *rng, int n4, int k4, int n
   }
   rc = body();
   cleanup();
+  if (g4) cudaGraphExecDestroy(g4);
+  if (g2) cudaGraphExecDestroy(g2);
   if (rc) return rc;
   memcpy(out, lat->h_out, (size_t)2 * R * sizeof(double));
   return U1_OK;

@@ -396,3 +396,17 @@ def test_export_into_caller_buffers(ctx):
     assert np.array_equal(dev.cpu().numpy(), ref)
     with pytest.raises(ValueError):
         lat.export_angles(np.zeros(lat.nlinks, dtype=np.float32))
+
+
+def test_multilevel_graphs_equal_direct(ctx):
+    """Graph-replayed multilevel sub-updates give the direct launches' result bit for bit."""
+    res = []
+    for graphs in (True, False):
+        lat = Lattice(ctx, 4, (8, 8, 8, 8), 1.0)
+        lat.set_graphs(graphs)
+        rng = Rng(ctx, 12)
+        lat.hot_start(rng)
+        lat.update(rng, 1, 2)
+        res.append((lat.multilevel(rng, 2, 1, 3, 1, 1, 2), rng.state))
+    assert np.array_equal(res[0][0], res[1][0])
+    assert res[0][1] == res[1][1]
