@@ -309,6 +309,20 @@ int u1_ncp_inverse(const float *y, const float *params, int64_t n, int K, float 
 int u1_ncp_inverse_backward(const float *xsol, const float *params, const float *gdx, const float *glogd, int64_t n,
                             int K, float *gy, float *gparams, void *stream);
 
+/* One whole coupling layer of the 2D flow, forward only (no counterpart in
+ * the reference): batch configurations theta_in[b][mu][x1][x0] (L x L,
+ * float32, device) -> theta_out, logdet[b] = sum of log H' over the layer's
+ * active plaquettes.  Layer (mu, off): links of direction mu on stripes
+ * x_nu = off (mod 4) change through their + plaquette; the context net sees
+ * (cos P, sin P) of the frozen plaquettes ((x_nu - off) mod 4 in {1, 2}):
+ * conv3x3(2 -> hidden; W1, B1), LeakyReLU(slope), conv3x3(hidden -> 2K+1;
+ * W2, B2), circular padding, weights rounded to bfloat16, FP32 arithmetic.
+ * L a multiple of 4 up to 32, K <= 8, hidden a multiple of 4 up to 32.  Queued on
+ * `stream`. */
+int u1_flow_layer_forward(const float *theta_in, float *theta_out, float *logdet, int batch, int L, int mu, int off,
+                          int K, int hidden, const float *W1, const float *B1, const float *W2, const float *B2,
+                          float slope, void *stream);
+
 /* Number of kernels this library has launched in the calling process. */
 int u1_kernel_launch_count(uint64_t *out);
 

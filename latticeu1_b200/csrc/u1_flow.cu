@@ -13,6 +13,8 @@
 //   forward:  dy = h(xc) - xc (the change the caller adds to the updated link), logd = log h'(xc)
 //   inverse:  given y, z = remainder(y - shift, 2 pi); x solves sum_k w_k g(x) = z (bisection);
 //             dx = x - z - shift (the change that undoes the forward step), logd = log h'(x)
+#include <cuda_bf16.h>
+
 #include <string>
 
 #include "u1_internal.h"
@@ -176,6 +178,183 @@ __global__ void k_ncp_inverse_backward(const float *__restrict__ xsol, const flo
   gpo[2 * K] = -r;
 }
 
+// ---------------------------------------------------------------------------
+// One whole coupling layer, forward only (the proposal path of the sampler),
+// one block per configuration of an L x L lattice, theta[b][mu][x1][x0]:
+//   P(x) = th_0(x) + th_1(x+e0) - th_0(x+e1) - th_1(x);
+//   context = (cos P, sin P) on the frozen plaquettes, 0 elsewhere;
+//   hidden = LeakyReLU(conv3x3(context; W1, B1)), circular padding;
+//   params = conv3x3(hidden; W2, B2) at the active plaquettes;
+//   the mixture transform moves each active plaquette, its updated link
+//   absorbs the change, and logdet[b] = sum of log H' over the active ones.
+// Masks for (mu, off): stripes x_nu = off (mod 4), nu = 1 - mu; the active
+// plaquette of link th_mu(x) is P(x) (mu = 0) or P(x - e0) (mu = 1); frozen
+// plaquettes have (x_nu - off) mod 4 in {1, 2}.  Weights are rounded to
+// bfloat16 on load (the layer's stored precision); activations and sums are
+// FP32.  Convolutions are cross-correlations as torch.nn.Conv2d:
+//   out[c][y][x] = B[c] + sum_{ci,ky,kx} W[c][ci][ky][kx] in[ci][y+ky-1][x+kx-1].
+__device__ __forceinline__ float bf16_round(float v) { return __bfloat162float(__float2bfloat16(v)); }
+
+__device__ __forceinline__ void active_pos(int a, int L, int mu, int off, int &x1, int &x0) {
+  if (mu == 0) {
+    x1 = 4 * (a / L) + off;
+    x0 = a % L;
+  } else {
+    const int q = L / 4;
+    x1 = a / q;
+    x0 = 4 * (a % q) + ((off + 3) & 3);
+  }
+}
+
+// 3x3 circular neighbourhood of pixel (x1, x0): offsets (yy * L + xx), ky-major.
+__device__ __forceinline__ void nbr9(int x1, int x0, int L, int (&o)[9]) {
+#pragma unroll
+  for (int ky = 0; ky < 3; ++ky) {
+    int yy = x1 + ky - 1;
+    yy = yy < 0 ? yy + L : (yy >= L ? yy - L : yy);
+#pragma unroll
+    for (int kx = 0; kx < 3; ++kx) {
+      int xx = x0 + kx - 1;
+      xx = xx < 0 ? xx + L : (xx >= L ? xx - L : xx);
+      o[ky * 3 + kx] = yy * L + xx;
+    }
+  }
+}
+
+__device__ __forceinline__ void fma4(float4 &acc, const float4 w, float h) {
+  acc.x = fmaf(w.x, h, acc.x);
+  acc.y = fmaf(w.y, h, acc.y);
+  acc.z = fmaf(w.z, h, acc.z);
+  acc.w = fmaf(w.w, h, acc.w);
+}
+
+// Shared memory (floats, each part a multiple of 4): th[2 LL], P[LL], ctx[2 LL],
+// hid[H LL], w1t[18 H] ([ci*9 + k][c]), b1[H], w2t[9 H CP] ([ci*9 + k][o],
+// outputs padded to CP = round4(2K+1) with zeros), b2[CP], prm[LL/4 * CP].
+__global__ void __launch_bounds__(256)
+    k_flow_layer_forward(const float *__restrict__ th_in, float *__restrict__ th_out, float *__restrict__ logdet,
+                         int L, int mu, int off, int K, int H, const float *__restrict__ W1,
+                         const float *__restrict__ B1, const float *__restrict__ W2, const float *__restrict__ B2,
+                         float slope) {
+  extern __shared__ float4 sm4[];
+  float *sm = reinterpret_cast<float *>(sm4);
+  const int LL = L * L, C2 = 2 * K + 1, CP = (C2 + 3) & ~3, nact = LL / 4;
+  float *th = sm;
+  float *P = th + 2 * LL;
+  float *ctx = P + LL;
+  float *hid = ctx + 2 * LL;
+  float *w1t = hid + H * LL;
+  float *b1 = w1t + 18 * H;
+  float *w2t = b1 + H;
+  float *b2 = w2t + 9 * H * CP;
+  float *prm = b2 + CP;
+  __shared__ double red[32];
+  const int nt = blockDim.x, tid = threadIdx.x;
+  const float *src = th_in + (size_t)blockIdx.x * 2 * LL;
+  for (int t = tid; t < 2 * LL; t += nt) th[t] = src[t];
+  for (int t = tid; t < 18 * H; t += nt) {  // W1[c][ci][ky][kx] -> w1t[(ci*9 + k) * H + c]
+    const int c = t / 18, r = t - c * 18;
+    w1t[r * H + c] = bf16_round(W1[t]);
+  }
+  for (int t = tid; t < H; t += nt) b1[t] = bf16_round(B1[t]);
+  for (int t = tid; t < 9 * H * CP; t += nt) {  // W2[o][ci][ky][kx] -> w2t[(ci*9 + k) * CP + o]
+    const int r = t / CP, o = t - r * CP;
+    w2t[t] = o < C2 ? bf16_round(W2[(size_t)o * H * 9 + r]) : 0.f;
+  }
+  for (int t = tid; t < CP; t += nt) b2[t] = t < C2 ? bf16_round(B2[t]) : 0.f;
+  __syncthreads();
+  for (int p = tid; p < LL; p += nt) {
+    const int x0 = p % L, x1 = p / L;
+    const int x0p = x0 + 1 == L ? 0 : x0 + 1, x1p = x1 + 1 == L ? 0 : x1 + 1;
+    const float v = th[p] + th[LL + x1 * L + x0p] - th[x1p * L + x0] - th[LL + p];
+    P[p] = v;
+    const int xn = mu == 0 ? x1 : x0;
+    const int r = (xn - off) & 3;
+    const bool frozen = r == 1 || r == 2;
+    float sn, cs;
+    sincosf(v, &sn, &cs);
+    ctx[p] = frozen ? cs : 0.f;
+    ctx[LL + p] = frozen ? sn : 0.f;
+  }
+  __syncthreads();
+  // conv1 + LeakyReLU: one pixel per work item, all H channels, four at a time
+  const float4 *w1v = reinterpret_cast<const float4 *>(w1t);
+  for (int p = tid; p < LL; p += nt) {
+    int o9[9];
+    nbr9(p / L, p % L, L, o9);
+    float in[18];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      in[k] = ctx[o9[k]];
+      in[9 + k] = ctx[LL + o9[k]];
+    }
+    for (int c4 = 0; c4 < H; c4 += 4) {
+      float4 acc = make_float4(b1[c4], b1[c4 + 1], b1[c4 + 2], b1[c4 + 3]);
+#pragma unroll
+      for (int r = 0; r < 18; ++r) fma4(acc, w1v[(r * H + c4) >> 2], in[r]);
+      hid[(c4 + 0) * LL + p] = acc.x > 0.f ? acc.x : slope * acc.x;
+      hid[(c4 + 1) * LL + p] = acc.y > 0.f ? acc.y : slope * acc.y;
+      hid[(c4 + 2) * LL + p] = acc.z > 0.f ? acc.z : slope * acc.z;
+      hid[(c4 + 3) * LL + p] = acc.w > 0.f ? acc.w : slope * acc.w;
+    }
+  }
+  __syncthreads();
+  // conv2 at the active plaquettes: work item = (active pixel, group of four outputs)
+  const float4 *w2v = reinterpret_cast<const float4 *>(w2t);
+  const int ng = CP / 4;
+  for (int q = tid; q < nact * ng; q += nt) {
+    const int a = q / ng, og = q - a * ng;
+    int x1, x0;
+    active_pos(a, L, mu, off, x1, x0);
+    int o9[9];
+    nbr9(x1, x0, L, o9);
+    float4 acc = make_float4(b2[og * 4], b2[og * 4 + 1], b2[og * 4 + 2], b2[og * 4 + 3]);
+    for (int ci = 0; ci < H; ++ci) {
+      const float *hc = hid + ci * LL;
+#pragma unroll
+      for (int k = 0; k < 9; ++k) fma4(acc, w2v[((ci * 9 + k) * CP >> 2) + og], hc[o9[k]]);
+    }
+    float *dst = prm + a * CP + og * 4;
+    dst[0] = acc.x;
+    dst[1] = acc.y;
+    dst[2] = acc.z;
+    dst[3] = acc.w;
+  }
+  __syncthreads();
+  double ld = 0.0;
+  for (int a = tid; a < nact; a += nt) {
+    int x1, x0;
+    active_pos(a, L, mu, off, x1, x0);
+    const float *pp = prm + a * CP;
+    const float xc = remainderf(P[x1 * L + x0], kTwoPi);
+    Mix m;
+    float g[kMaxK], gp[kMaxK], s, c;
+    mix_eval(xc, pp, K, m, g, gp, s, c);
+    const float dy = m.H + pp[2 * K] - xc;
+    ld += (double)logf(m.Hp);
+    if (mu == 0)
+      th[x1 * L + x0] += dy;
+    else
+      th[LL + x1 * L + (x0 + 1 == L ? 0 : x0 + 1)] += dy;
+  }
+  // block sum of the log-derivatives (fixed order)
+  for (int o = 16; o > 0; o >>= 1) ld += __shfl_xor_sync(0xffffffffu, ld, o);
+  if ((tid & 31) == 0) red[tid >> 5] = ld;
+  __syncthreads();
+  float *dst = th_out + (size_t)blockIdx.x * 2 * LL;
+  for (int t = tid; t < 2 * LL; t += nt) dst[t] = th[t];
+  if (tid == 0) {
+    double tot = 0.0;
+    for (int w = 0; w < (nt + 31) / 32; ++w) tot += red[w];
+    logdet[blockIdx.x] = (float)tot;
+  }
+}
+
+size_t flow_layer_smem(int L, int K, int H) {
+  const size_t LL = (size_t)L * L, CP = (2 * K + 1 + 3) & ~3;
+  return sizeof(float) * (2 * LL + LL + 2 * LL + H * LL + 18 * H + H + 9 * H * CP + CP + (LL / 4) * CP);
+}
+
 int check_args(long long n, int K) {
   if (n < 0) return flfail(U1_ERR_INVALID, "ncp: negative element count");
   if (K < 1 || K > kMaxK) return flfail(U1_ERR_INVALID, "ncp: K must be in [1, 8]");
@@ -227,5 +406,27 @@ extern "C" int u1_ncp_inverse_backward(const float *xsol, const float *params, c
   if (!xsol || !params || !gy || !gparams) return flfail(U1_ERR_INVALID, "u1_ncp_inverse_backward: null pointer");
   k_ncp_inverse_backward<<<blocks(n), 256, 0, (cudaStream_t)stream>>>(xsol, params, gdx, glogd, n, K, gy, gparams);
   U1_LAUNCH_CHECK("k_ncp_inverse_backward");
+  return U1_OK;
+}
+
+extern "C" int u1_flow_layer_forward(const float *theta_in, float *theta_out, float *logdet, int batch, int L,
+                                     int mu, int off, int K, int hidden, const float *W1, const float *B1,
+                                     const float *W2, const float *B2, float slope, void *stream) {
+  if (!theta_in || !theta_out || !logdet || !W1 || !B1 || !W2 || !B2)
+    return flfail(U1_ERR_INVALID, "u1_flow_layer_forward: null pointer");
+  if (theta_in == theta_out) return flfail(U1_ERR_INVALID, "u1_flow_layer_forward: in and out must not alias");
+  if (batch < 1 || L < 4 || L > 32 || L % 4 || (mu != 0 && mu != 1) || off < 0 || off > 3 || K < 1 || K > kMaxK ||
+      hidden < 4 || hidden > 32 || hidden % 4)
+    return flfail(U1_ERR_INVALID,
+                  "u1_flow_layer_forward: bad shape (L a multiple of 4 up to 32, K <= 8, hidden a multiple of 4 up to 32)");
+  const size_t smem = flow_layer_smem(L, K, hidden);
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_flow_layer_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return u1i::cuda_fail(e, "u1_flow_layer_forward: shared memory");
+  }
+  k_flow_layer_forward<<<batch, 256, smem, (cudaStream_t)stream>>>(theta_in, theta_out, logdet, L, mu, off, K,
+                                                                    hidden, W1, B1, W2, B2, slope);
+  U1_LAUNCH_CHECK("k_flow_layer_forward");
   return U1_OK;
 }

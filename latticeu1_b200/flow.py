@@ -19,8 +19,10 @@ even/odd layout.
 
 Library kernels on this path: the circular coupling transform and its
 inverse with analytic backward passes (u1_ncp_*), the Wilson action and its
-adjoint (u1_wilson_action*).  The 3x3 convolutions run through cuDNN in
-bfloat16 with FP32 accumulation.
+adjoint (u1_wilson_action*), and for proposals one fused kernel per coupling
+layer (u1_flow_layer_forward: context net, transform, link update, log-det).
+In training the 3x3 convolutions run through cuDNN in bfloat16 with FP32
+accumulation.
 """
 from __future__ import annotations
 
@@ -235,6 +237,28 @@ class Flow2D(nn.Module):
         for layer in self.layers:
             th, ld = layer(th)
             logq = logq - ld
+        return torch.remainder(th, TWO_PI), logq
+
+    @torch.no_grad()
+    def sample_fused(self, B: int, generator: torch.Generator | None = None):
+        """As sample(), each coupling layer one library kernel
+        (u1_flow_layer_forward: context net with bf16-rounded weights and FP32
+        arithmetic, transform, link update, log-det), for proposals."""
+        dev = self.perm.device
+        th = torch.rand((B, 2, self.L, self.L), device=dev, generator=generator) * TWO_PI
+        buf = torch.empty_like(th)
+        ld = torch.empty(B, device=dev)
+        logq = torch.full((B,), self.log_prior, device=dev)
+        with torch.cuda.device(dev):
+            stream = torch.cuda.current_stream(dev).cuda_stream
+            for layer in self.layers:
+                c1, c2 = layer.net[0], layer.net[2]
+                check(lib.u1_flow_layer_forward(_p(th), _p(buf), _p(ld), B, self.L, layer.mu, layer.off, layer.K,
+                                                c1.out_channels, _p(c1.weight), _p(c1.bias), _p(c2.weight),
+                                                _p(c2.bias), C.c_float(layer.net[1].negative_slope),
+                                                C.c_void_p(stream)), "u1_flow_layer_forward")
+                logq -= ld
+                th, buf = buf, th
         return torch.remainder(th, TWO_PI), logq
 
     def log_prob(self, th: torch.Tensor) -> torch.Tensor:
@@ -465,7 +489,7 @@ def run_experiment(L: int = 16, beta: float = 2.0, n_layers: int = 8, K: int = 6
     ev0.record()
     with torch.no_grad():
         for _ in range(n_props // batch):
-            th, logq = flow.sample(batch)
+            th, logq = flow.sample_fused(batch)  # log q from the same kernels that make the sample
             S = flow.S(th)
             lw.append((-S - logq).double())
             qs.append(flow.charge(th))

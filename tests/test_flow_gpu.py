@@ -149,3 +149,66 @@ def test_flow_inverts_and_trains():
     for _ in range(120):
         last = flow.reverse_kl_step(opt, 256)
     assert last["loss"] < np.mean(first) - 1.0
+
+
+def _layer_ref_fp32(c, th):
+    """The coupling layer in plain torch FP32 with bf16-rounded weights (the
+    fused kernel's arithmetic): returns (theta', logdet)."""
+    import torch.nn.functional as Fn
+    from latticeu1_b200.flow import ncp_forward, plaquettes_no
+    r = lambda t: t.detach().to(torch.bfloat16).float()
+    torch.backends.cudnn.allow_tf32 = False  # plain FP32 convolutions for the reference
+    B = th.shape[0]
+    P = plaquettes_no(th)
+    ctx = torch.stack([torch.cos(P), torch.sin(P)], 1) * c.frozen
+    h = Fn.conv2d(Fn.pad(ctx, (1, 1, 1, 1), mode="circular"), r(c.net[0].weight), r(c.net[0].bias))
+    h = Fn.leaky_relu(h, c.net[1].negative_slope)
+    prm = Fn.conv2d(Fn.pad(h, (1, 1, 1, 1), mode="circular"), r(c.net[2].weight), r(c.net[2].bias))
+    prm = prm.reshape(B, 2 * c.K + 1, -1)[:, :, c.act_idx].permute(0, 2, 1).reshape(-1, 2 * c.K + 1)
+    Pa = P.reshape(B, -1)[:, c.act_idx].reshape(-1)
+    dy, logd = ncp_forward(Pa, prm, c.K)
+    return c._apply_delta(th, dy), logd.reshape(B, -1).sum(1)
+
+
+@pytest.mark.parametrize("L,layer", [(8, 0), (8, 1), (16, 2), (16, 5), (32, 7)])
+def test_fused_layer_forward_matches_torch(L, layer):
+    import ctypes as C
+    from latticeu1_b200._lib import check, lib
+    torch.manual_seed(layer)
+    c = Coupling(L, layer % 2, (layer // 2) % 4, K=6, hidden=32).cuda()
+    with torch.no_grad():
+        for m in c.net:
+            if isinstance(m, torch.nn.Conv2d):
+                m.weight.normal_(0, 0.2)
+                m.bias.normal_(0, 0.2)
+    B = 16
+    th = torch.rand(B, 2, L, L, device="cuda") * TWO_PI
+    want, want_ld = _layer_ref_fp32(c, th)
+    out = torch.empty_like(th)
+    ld = torch.empty(B, device="cuda")
+    p = lambda t: C.c_void_p(t.data_ptr())
+    check(lib.u1_flow_layer_forward(p(th), p(out), p(ld), B, L, c.mu, c.off, c.K, 32, p(c.net[0].weight),
+                                    p(c.net[0].bias), p(c.net[2].weight), p(c.net[2].bias),
+                                    C.c_float(c.net[1].negative_slope), None), "u1_flow_layer_forward")
+    torch.cuda.synchronize()
+    d = torch.remainder(out - want + math.pi, TWO_PI) - math.pi
+    assert d.abs().max().item() < 2e-4
+    assert (ld - want_ld).abs().max().item() < 2e-3
+
+
+def test_fused_sampler_consistent_with_inverse():
+    """Proposals from the fused layers carry log q consistent with the inverse flow."""
+    torch.manual_seed(1)
+    flow = Flow2D(8, beta=2.0, n_layers=8, K=4, hidden=16).cuda()
+    with torch.no_grad():
+        for layer in flow.layers:
+            layer.net[2].weight.normal_(0, 0.05)
+            layer.net[2].weight.copy_(layer.net[2].weight.to(torch.bfloat16).float())
+            layer.net[2].bias.copy_(layer.net[2].bias.to(torch.bfloat16).float())
+            layer.net[0].weight.copy_(layer.net[0].weight.to(torch.bfloat16).float())
+            layer.net[0].bias.copy_(layer.net[0].bias.to(torch.bfloat16).float())
+    th, logq = flow.sample_fused(64)
+    assert torch.isfinite(logq).all()
+    # the torch inverse runs its convolutions in bf16 (autocast), so agreement is to bf16 level
+    lq2 = flow.log_prob(th)
+    assert (lq2 - logq).abs().max().item() < 0.5
