@@ -46,19 +46,36 @@ def algorithmic_bytes_per_link_update(d: int) -> int:
     return 16 * d + 8
 
 
-def workload_config(L: int) -> dict:
-    return {
-        "workload": f"U(1) Wilson 4D {L}^4 beta={BETA} hot start; step = 1 Metropolis + 4 OR sweep "
-                    "+ fused plaquette(SS/ST)+Polyakov measurement",
-        "lattice": f"{L}^4", "beta": BETA, "metrop": METROP, "ovrn": OVRN,
+def metric_for(N) -> str:
+    return METRIC if tuple(N) == (32, 32, 32, 32) else METRIC.replace("32^4", geom_name(N))
+
+
+def geom_name(N) -> str:
+    return f"{N[0]}^4" if len(set(N)) == 1 else "x".join(str(n) for n in N)
+
+
+def workload_config(N, beta: float = BETA, aniso: float = 1.0) -> dict:
+    name = geom_name(N)
+    cfg = {
+        "workload": f"U(1) Wilson 4D {name} beta={beta}" + (f" aniso={aniso}" if aniso != 1.0 else "") +
+                    " hot start; step = 1 Metropolis + 4 OR sweep + plaquette(SS/ST)+Polyakov measurement "
+                    "taken from the sweep's last pass",
+        "lattice": name, "beta": beta, "metrop": METROP, "ovrn": OVRN,
         "links": "float2 (cos,sin) even/odd SoA, 8 B/link",
         "l2": "flushed between timed steps (512 MiB device write)",
         "rng": "Philox4x32-10 keyed by (seed, site, mu, pass)",
     }
+    if aniso != 1.0:
+        cfg["aniso"] = aniso
+    return cfg
 
 
-def link_updates_per_step(L: int) -> int:
-    return (L ** DIMS) * DIMS * (METROP + OVRN)
+def volume(N) -> int:
+    return int(N[0]) * int(N[1]) * int(N[2]) * int(N[3])
+
+
+def link_updates_per_step(N) -> int:
+    return volume(N) * DIMS * (METROP + OVRN)
 
 
 # ------------------------------------------------------------------ clocks
@@ -118,9 +135,9 @@ def measured_peak() -> tuple[float, str]:
     return 6650.0, "fallback"
 
 
-def ncu_traffic_per_launch(L: int):
+def ncu_traffic_per_launch(N):
     """DRAM bytes per k_update launch from the committed ncu summary, if any."""
-    p = ROOT / "profiles" / f"k_update_{L}x4_traffic.txt"
+    p = ROOT / "profiles" / f"k_update_{geom_name(N).replace('^4', 'x4')}_traffic.txt"
     if not p.exists():
         return None
     for line in p.read_text().splitlines():
@@ -130,16 +147,16 @@ def ncu_traffic_per_launch(L: int):
 
 
 # ------------------------------------------------------------------ CPU baselines
-def cpu_reference_rate(L: int, budget_s: float, min_sweeps: int = 1) -> dict:
+def cpu_reference_rate(N, beta: float, aniso: float, budget_s: float, min_sweeps: int = 1) -> dict:
     """The reference's own FP64 CPU metropolis + overrelaxation (oracle/_ref),
-    OpenMP over all host threads, on the 32^4 workload; bounded by budget_s.
+    OpenMP over all host threads, on the bench geometry; bounded by budget_s.
     Falls back to the oracle port (oracle/u1_oracle.cpp) if _ref is absent."""
     import numpy as np
     from oracle.oracle import Oracle, Ref
     threads = os.cpu_count() or 1
-    lat = np.random.default_rng(1).uniform(0, 2 * np.pi, (L ** 4) * 4)
+    lat = np.random.default_rng(1).uniform(0, 2 * np.pi, volume(N) * 4)
     if Ref.available():
-        ref = Ref(4, (L, L, L, L), BETA, 1.0, METROP, OVRN)
+        ref = Ref(4, tuple(N), beta, aniso, METROP, OVRN)
         ref.seed_cpu(threads, 1234)
         kind = "reference"
 
@@ -148,7 +165,7 @@ def cpu_reference_rate(L: int, budget_s: float, min_sweeps: int = 1) -> dict:
             for _ in range(OVRN):
                 ref.overrelax(lat)
     else:
-        o = Oracle(4, (L, L, L, L), BETA)
+        o = Oracle(4, tuple(N), beta, aniso)
         kind = "port"
         state = {"p": 0}
 
@@ -165,22 +182,22 @@ def cpu_reference_rate(L: int, budget_s: float, min_sweeps: int = 1) -> dict:
             break
         if el + el / n > 3 * budget_s:
             break
-    rate = n * link_updates_per_step(L) / el
+    rate = n * link_updates_per_step(N) / el
     return {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"{n} full sweeps (1 Metropolis + 4 OR) of the {L}^4 lattice, {el:.1f} s, FP64"}
+            "sample": f"{n} full sweeps (1 Metropolis + 4 OR) of the {geom_name(N)} lattice, {el:.1f} s, FP64"}
 
 
 def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    L = args.L
+    N, beta, aniso = geometry(args)
     import numpy as np
     from oracle.oracle import Oracle, Ref
     threads = os.cpu_count() or 1
-    lat = np.random.default_rng(1).uniform(0, 2 * np.pi, (L ** 4) * 4)
+    lat = np.random.default_rng(1).uniform(0, 2 * np.pi, volume(N) * 4)
     if Ref.available():
-        ref = Ref(4, (L, L, L, L), BETA, 1.0, METROP, OVRN)
+        ref = Ref(4, tuple(N), beta, aniso, METROP, OVRN)
         ref.seed_cpu(threads, 1234)
         kind = "reference"
 
@@ -191,7 +208,7 @@ def run_reference(args) -> None:
             ref.plaquette(lat)
             ref.polyakov(lat)
     else:
-        o = Oracle(4, (L, L, L, L), BETA)
+        o = Oracle(4, tuple(N), beta, aniso)
         kind = "port"
         st = {"p": 0}
 
@@ -205,15 +222,15 @@ def run_reference(args) -> None:
     for _ in range(args.steps):
         step()
     el = time.perf_counter() - t0
-    rate = args.steps * link_updates_per_step(L) / el
+    rate = args.steps * link_updates_per_step(N) / el
     line = {
-        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+        "impl": "reference", "metric": metric_for(N), "value": rate, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload_config(L),
+        "config": workload_config(N, beta, aniso),
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
-                         "sample": f"{args.steps} timed full sweeps of {L}^4 (1 Met + 4 OR) + CPU plaquette "
-                                   "and Polyakov, FP64, OpenMP"},
+                         "sample": f"{args.steps} timed full sweeps of {geom_name(N)} (1 Met + 4 OR) + CPU "
+                                   "plaquette and Polyakov, FP64, OpenMP"},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -237,16 +254,16 @@ def run_ours(args) -> None:
     torch.cuda.set_device(local)
     from latticeu1_b200 import Context, Lattice, Rng, launch_count
 
-    L = args.L
+    N, beta, aniso = geometry(args)
     ctx = Context(local)
-    lat = Lattice(ctx, DIMS, (L, L, L, L), BETA)
+    lat = Lattice(ctx, DIMS, N, beta, aniso)
     stream = torch.cuda.Stream()
     lat.set_stream(stream.cuda_stream)
     rng = Rng(ctx, 1234)
     rng.set_chain(replicas.chain_id(rank))  # independent replica per rank
     flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device="cuda")
     obs = torch.zeros((args.steps + args.warmup, 6), dtype=torch.float64, device="cuda")
-    lu = link_updates_per_step(L)
+    lu = link_updates_per_step(N)
 
     with torch.cuda.stream(stream):
         lat.hot_start(rng)
@@ -314,14 +331,14 @@ def run_ours(args) -> None:
         peak, peak_kind = measured_peak()
         upd_launches = 2 * DIMS * (METROP + OVRN)  # the last one also measures
         avg_launch_s = upd_ms * 1e-3 / (args.steps * upd_launches)
-        alg_bytes = algorithmic_bytes_per_link_update(DIMS) * (L ** DIMS) // 2
+        alg_bytes = algorithmic_bytes_per_link_update(DIMS) * volume(N) // 2
         achieved = alg_bytes / avg_launch_s / 1e9
-        traffic = ncu_traffic_per_launch(L)
+        traffic = ncu_traffic_per_launch(N)
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "metric": metric_for(N), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": workload_config(L),
+            "config": workload_config(N, beta, aniso),
             "roofline": {"bound": "hbm", "kernel": "k_update_pair (one (parity,mu) phase; step average)",
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
@@ -341,7 +358,7 @@ def run_ours(args) -> None:
                             "per_chain_plaq_ss_st": per_chain},
         }
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_reference_rate(L, args.cpu_budget)
+            line["cpu_baseline"] = cpu_reference_rate(N, beta, aniso, args.cpu_budget)
         print(json.dumps(line), flush=True)
     lat.close()
     rng.close()
@@ -502,13 +519,27 @@ def run_batched(args) -> None:
     b.close()
 
 
+def geometry(args):
+    """(N, beta, aniso) of the update workload: --geom Nx,Ny,Nz,Nt or --L for L^4."""
+    if args.geom:
+        N = tuple(int(v) for v in args.geom.split(","))
+        if len(N) != 4:
+            raise SystemExit("--geom needs four extents Nx,Ny,Nz,Nt")
+    else:
+        N = (args.L,) * 4
+    return N, args.beta, args.aniso
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--L", type=int, default=L_DEFAULT)
+    ap.add_argument("--L", type=int, default=L_DEFAULT, help="L^4 lattice (update workload)")
+    ap.add_argument("--geom", type=str, default=None, help="Nx,Ny,Nz,Nt instead of --L (update workload)")
+    ap.add_argument("--beta", type=float, default=BETA)
+    ap.add_argument("--aniso", type=float, default=1.0)
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU baseline sampling")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["update32", "multilevel", "batched"], default="update32")
