@@ -84,4 +84,19 @@ U1_HD uint32_t u1_rng_word1(int mu, uint32_t tag, uint32_t chain) {
   return (uint32_t)mu | (tag << 8) | (chain << 16);
 }
 
+// Metropolis draws of the link (EO site s = parity * V/2 + eo, direction mu)
+// in pass `pass`: the proposal u1 (theta' = 2 pi u1) and the accept number b.
+// Sites 2k and 2k+1 share one Philox4x32-10 block, counter
+// (k, word1(mu, METROPOLIS, chain), pass lo, pass hi), key = seed: the even
+// site takes words 0 and 1, the odd site words 2 and 3.
+U1_HD Philox4 u1_metropolis_block(uint32_t s, int mu, uint32_t chain, unsigned long long pass, uint32_t key0,
+                                  uint32_t key1) {
+  return philox4x32_10(s >> 1, u1_rng_word1(mu, U1_TAG_METROPOLIS, chain), (uint32_t)pass, (uint32_t)(pass >> 32),
+                       key0, key1);
+}
+U1_HD void u1_metropolis_draws(const Philox4 &r, uint32_t s, float &u1, float &b) {
+  u1 = u1_uniform_open((s & 1u) ? r.v[2] : r.v[0]);
+  b = u1_uniform_open((s & 1u) ? r.v[3] : r.v[1]);
+}
+
 }  // namespace u1b

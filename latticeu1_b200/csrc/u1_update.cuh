@@ -148,8 +148,11 @@ __device__ __forceinline__ float2 staple_steps(const float2 *__restrict__ lat, c
 
 // One link update (Metropolis with Philox or replayed numbers, or
 // overrelaxation) given its staple S and current value U.
+// blk: the site's Philox block when the caller already drew it (two-site
+// bodies draw once for both sites), else nullptr.
 template <int D, int MU, bool MET, bool REPLAY>
-__device__ __forceinline__ float2 update_one(const UpdArgs &a, int i, float2 S, float2 U) {
+__device__ __forceinline__ float2 update_one(const UpdArgs &a, int i, float2 S, float2 U,
+                                             const Philox4 *blk = nullptr) {
   if (MET) {
     const unsigned long long pass = *a.pass_dev + (unsigned long long)a.hit;
     float2 Un;
@@ -161,10 +164,10 @@ __device__ __forceinline__ float2 update_one(const UpdArgs &a, int i, float2 S, 
       Un = make_float2((float)cs, (float)sn);
       b = (float)a.replay[pr + 1];
     } else {
-      Philox4 r = philox4x32_10((uint32_t)(a.p * a.g.Vh + i), u1_rng_word1(MU, U1_TAG_METROPOLIS, a.chain),
-                                (uint32_t)pass, (uint32_t)(pass >> 32), a.key0, a.key1);
-      const float u1 = u1_uniform_open(r.v[0]);
-      b = u1_uniform_open(r.v[1]);
+      const uint32_t s = (uint32_t)(a.p * a.g.Vh + i);
+      const Philox4 r = blk ? *blk : u1_metropolis_block(s, MU, a.chain, pass, a.key0, a.key1);
+      float u1;
+      u1_metropolis_draws(r, s, u1, b);
       float sn, cs;
       sincospif(2.0f * u1, &sn, &cs);
       Un = make_float2(cs, sn);
@@ -332,8 +335,13 @@ __device__ __forceinline__ void update_pair_body(const UpdArgs a, int i, float2 
   const float2 S1 = cweigh(ss1, a.c.w_ss, st1, a.c.w_st);
   float4 *own = reinterpret_cast<float4 *>(a.lat + MU * V + a.p * Vh + i);
   const float4 U = *own;
-  const float2 N0 = update_one<D, MU, MET, REPLAY>(a, i, S0, make_float2(U.x, U.y));
-  const float2 N1 = update_one<D, MU, MET, REPLAY>(a, i + 1, S1, make_float2(U.z, U.w));
+  // sites i, i+1 (i even, V/2 even) share one Philox block
+  Philox4 blk;
+  if (MET && !REPLAY)
+    blk = u1_metropolis_block((uint32_t)(a.p * Vh + i), MU, a.chain, *a.pass_dev + (unsigned long long)a.hit,
+                              a.key0, a.key1);
+  const float2 N0 = update_one<D, MU, MET, REPLAY>(a, i, S0, make_float2(U.x, U.y), &blk);
+  const float2 N1 = update_one<D, MU, MET, REPLAY>(a, i + 1, S1, make_float2(U.z, U.w), &blk);
   *own = make_float4(N0.x, N0.y, N1.x, N1.y);
   pdl_release_dependents();
   if (MEAS) {
@@ -410,10 +418,9 @@ static __global__ void k_rng_debug(float *out, int Vh, int p, int mu, uint32_t k
                             uint32_t chain, unsigned long long pass) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= Vh) return;
-  Philox4 r = philox4x32_10((uint32_t)(p * Vh + i), u1_rng_word1(mu, U1_TAG_METROPOLIS, chain),
-                            (uint32_t)pass, (uint32_t)(pass >> 32), key0, key1);
-  out[2 * i] = u1_uniform_open(r.v[0]);
-  out[2 * i + 1] = u1_uniform_open(r.v[1]);
+  const uint32_t s = (uint32_t)(p * Vh + i);
+  const Philox4 r = u1_metropolis_block(s, mu, chain, pass, key0, key1);
+  u1_metropolis_draws(r, s, out[2 * i], out[2 * i + 1]);
 }
 
 }  // namespace u1b

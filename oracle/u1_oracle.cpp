@@ -161,14 +161,13 @@ long o_metropolis_pairs(const OGeom *g, double *lat, const double *pairs) {
 }
 
 // Philox draws of link (parity, mu, id) in Metropolis pass `pass`
-// (the counter layout of latticeu1_b200/csrc/u1_philox.h).
+// (the counter layout of latticeu1_b200/csrc/u1_philox.h: EO sites 2k and
+// 2k+1 share one block, words 0,1 and 2,3).
 void o_philox_uniforms(const OGeom *g, uint64_t seed, uint32_t chain, uint64_t pass, int p, int mu, int id,
                        float out[2]) {
-  u1b::Philox4 r = u1b::philox4x32_10((uint32_t)(p * g->Vh + id),
-                                      u1b::u1_rng_word1(mu, u1b::U1_TAG_METROPOLIS, chain), (uint32_t)pass,
-                                      (uint32_t)(pass >> 32), (uint32_t)seed, (uint32_t)(seed >> 32));
-  out[0] = u1b::u1_uniform_open(r.v[0]);
-  out[1] = u1b::u1_uniform_open(r.v[1]);
+  const uint32_t s = (uint32_t)(p * g->Vh + id);
+  const u1b::Philox4 r = u1b::u1_metropolis_block(s, mu, chain, pass, (uint32_t)seed, (uint32_t)(seed >> 32));
+  u1b::u1_metropolis_draws(r, s, out[0], out[1]);
 }
 
 void o_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1, uint32_t out[4]) {
