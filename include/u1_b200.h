@@ -323,6 +323,17 @@ int u1_flow_layer_forward(const float *theta_in, float *theta_out, float *logdet
                           int K, int hidden, const float *W1, const float *B1, const float *W2, const float *B2,
                           float slope, void *stream);
 
+/* Backward of u1_flow_layer_forward (L up to 16): from theta_in and the
+ * upstream gradients grad_theta_out (batch x 2 x L x L) and grad_logdet
+ * (batch; NULL for zero), writes grad_theta_in and the weight gradients
+ * wgrad = (dW1[c][ci][ky][kx], dB1[c], dW2[o][ci][ky][kx], dB2[o]) summed over
+ * the batch in a fixed order (with respect to the bf16-rounded weights the
+ * forward uses).  wgrad_partials: batch * len(wgrad) floats of scratch. */
+int u1_flow_layer_backward(const float *theta_in, const float *grad_theta_out, const float *grad_logdet,
+                           float *grad_theta_in, float *wgrad_partials, float *wgrad, int batch, int L, int mu,
+                           int off, int K, int hidden, const float *W1, const float *B1, const float *W2,
+                           const float *B2, float slope, void *stream);
+
 /* Number of kernels this library has launched in the calling process. */
 int u1_kernel_launch_count(uint64_t *out);
 

@@ -98,6 +98,8 @@ SIGNATURES = {
     "u1_ncp_inverse": [_vp, _vp, C.c_int64, _i, _vp, _vp, _vp, _vp],
     "u1_ncp_inverse_backward": [_vp, _vp, _vp, _vp, C.c_int64, _i, _vp, _vp, _vp],
     "u1_flow_layer_forward": [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, C.c_float, _vp],
+    "u1_flow_layer_backward": [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, C.c_float,
+                               _vp],
     "u1_kernel_launch_count": [C.POINTER(C.c_uint64)],
     "u1_last_error": [],
     "u1_version": [],

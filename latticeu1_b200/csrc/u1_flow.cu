@@ -350,6 +350,275 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Backward of k_flow_layer_forward for one configuration per block.  The
+// forward is recomputed in shared memory (plaquettes, context, conv1
+// pre-activations, parameters); then, given gth_out (dL/dtheta_out) and
+// gld (dL/dlogdet), the adjoint runs backwards through the transform, conv2,
+// the LeakyReLU, conv1, the context and the plaquette map:
+//   gth_in = gth_out + plaquette-adjoint(gP),
+//   gP = [active] d/dP of the transform + [frozen] (-sin P, cos P) . g_context.
+// Convolution adjoints are written as gathers (each output element sums over
+// the inputs that read it), so no atomics are needed.  Weight gradients (with
+// respect to the bf16-rounded weights the forward used, passed straight to
+// the FP32 master weights) go to per-block partials wpart[b][:] =
+// (gW1[c][ci][k], gB1[c], gW2[o][ci][k], gB2[o]), summed over blocks in a
+// fixed order by k_flow_wgrad_reduce.  L <= 16 (shared-memory size).
+__global__ void __launch_bounds__(256)
+    k_flow_layer_backward(const float *__restrict__ th_in, const float *__restrict__ gth_out,
+                          const float *__restrict__ gld, float *__restrict__ gth_in, float *__restrict__ wpart, int L,
+                          int mu, int off, int K, int H, const float *__restrict__ W1, const float *__restrict__ B1,
+                          const float *__restrict__ W2, const float *__restrict__ B2, float slope) {
+  extern __shared__ float4 sm4[];
+  float *sm = reinterpret_cast<float *>(sm4);
+  const int LL = L * L, C2 = 2 * K + 1, CP = (C2 + 3) & ~3, nact = LL / 4;
+  float *th = sm;                  // 2 LL
+  float *P = th + 2 * LL;          // LL
+  float *ctx = P + LL;             // 2 LL
+  float *pre = ctx + 2 * LL;       // H LL   conv1 pre-activations
+  float *gh = pre + H * LL;        // H LL   dL/dhidden, then dL/dpre
+  float *w1t = gh + H * LL;        // 18 H   [ci*9 + k][c]
+  float *b1 = w1t + 18 * H;        // H
+  float *w2t = b1 + H;             // 9 H CP [ci*9 + k][o]
+  float *b2 = w2t + 9 * H * CP;    // CP
+  float *prm = b2 + CP;            // nact CP
+  float *gprm = prm + nact * CP;   // nact CP
+  float *gctx = gprm + nact * CP;  // 2 LL
+  float *gP = gctx + 2 * LL;       // LL
+  int *amap = reinterpret_cast<int *>(gP + LL);  // LL: active index of a plaquette, or -1
+  int *nbt = amap + LL;                          // 9 LL: nbt[k * LL + p] = pixel at offset k of p
+  int *apos = nbt + 9 * LL;                      // nact: pixel of active plaquette a
+  const int nt = blockDim.x, tid = threadIdx.x, b = blockIdx.x;
+  const float *src = th_in + (size_t)b * 2 * LL;
+  const float *go = gth_out + (size_t)b * 2 * LL;
+  for (int t = tid; t < 2 * LL; t += nt) th[t] = src[t];
+  for (int t = tid; t < 18 * H; t += nt) {
+    const int c = t / 18, r = t - c * 18;
+    w1t[r * H + c] = bf16_round(W1[t]);
+  }
+  for (int t = tid; t < H; t += nt) b1[t] = bf16_round(B1[t]);
+  for (int t = tid; t < 9 * H * CP; t += nt) {
+    const int r = t / CP, o = t - r * CP;
+    w2t[t] = o < C2 ? bf16_round(W2[(size_t)o * H * 9 + r]) : 0.f;
+  }
+  for (int t = tid; t < CP; t += nt) b2[t] = t < C2 ? bf16_round(B2[t]) : 0.f;
+  for (int p = tid; p < LL; p += nt) {
+    amap[p] = -1;
+    int o9[9];
+    nbr9(p / L, p % L, L, o9);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) nbt[k * LL + p] = o9[k];
+  }
+  __syncthreads();
+  for (int a = tid; a < nact; a += nt) {
+    int x1, x0;
+    active_pos(a, L, mu, off, x1, x0);
+    amap[x1 * L + x0] = a;
+    apos[a] = x1 * L + x0;
+  }
+  // ---- forward recomputation
+  for (int p = tid; p < LL; p += nt) {
+    const int x0 = p % L, x1 = p / L;
+    const int x0p = x0 + 1 == L ? 0 : x0 + 1, x1p = x1 + 1 == L ? 0 : x1 + 1;
+    const float v = th[p] + th[LL + x1 * L + x0p] - th[x1p * L + x0] - th[LL + p];
+    P[p] = v;
+    const int xn = mu == 0 ? x1 : x0;
+    const int r = (xn - off) & 3;
+    const bool frozen = r == 1 || r == 2;
+    float sn, cs;
+    sincosf(v, &sn, &cs);
+    ctx[p] = frozen ? cs : 0.f;
+    ctx[LL + p] = frozen ? sn : 0.f;
+  }
+  __syncthreads();
+  const float4 *w1v = reinterpret_cast<const float4 *>(w1t);
+  for (int p = tid; p < LL; p += nt) {
+    float in[18];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const int q = nbt[k * LL + p];
+      in[k] = ctx[q];
+      in[9 + k] = ctx[LL + q];
+    }
+    for (int c4 = 0; c4 < H; c4 += 4) {
+      float4 acc = make_float4(b1[c4], b1[c4 + 1], b1[c4 + 2], b1[c4 + 3]);
+#pragma unroll
+      for (int r = 0; r < 18; ++r) fma4(acc, w1v[(r * H + c4) >> 2], in[r]);
+      pre[(c4 + 0) * LL + p] = acc.x;
+      pre[(c4 + 1) * LL + p] = acc.y;
+      pre[(c4 + 2) * LL + p] = acc.z;
+      pre[(c4 + 3) * LL + p] = acc.w;
+    }
+  }
+  __syncthreads();
+  const float4 *w2v = reinterpret_cast<const float4 *>(w2t);
+  const int ng = CP / 4;
+  for (int q = tid; q < nact * ng; q += nt) {
+    const int a = q / ng, og = q - a * ng;
+    const int pa = apos[a];
+    float4 acc = make_float4(b2[og * 4], b2[og * 4 + 1], b2[og * 4 + 2], b2[og * 4 + 3]);
+    for (int ci = 0; ci < H; ++ci) {
+      const float *pc = pre + ci * LL;
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        const float v = pc[nbt[k * LL + pa]];
+        fma4(acc, w2v[((ci * 9 + k) * CP >> 2) + og], v > 0.f ? v : slope * v);
+      }
+    }
+    float *dst = prm + a * CP + og * 4;
+    dst[0] = acc.x;
+    dst[1] = acc.y;
+    dst[2] = acc.z;
+    dst[3] = acc.w;
+  }
+  for (int p = tid; p < LL; p += nt) gP[p] = 0.f;
+  __syncthreads();
+  // ---- transform adjoint: gprm and the active plaquettes' gP
+  const float gl = gld ? gld[b] : 0.f;
+  for (int a = tid; a < nact; a += nt) {
+    const int pa = apos[a];
+    const int x1 = pa / L, x0 = pa - x1 * L;
+    const float *pp = prm + a * CP;
+    float *gpo = gprm + a * CP;
+    const float xc = remainderf(P[pa], kTwoPi);
+    Mix m;
+    float g[kMaxK], gp[kMaxK], s, c;
+    mix_eval(xc, pp, K, m, g, gp, s, c);
+    const int link = mu == 0 ? pa : LL + x1 * L + (x0 + 1 == L ? 0 : x0 + 1);
+    const float gdy = go[link];
+    float gxc;
+    mix_backward(m, g, gp, s, c, K, gdy, gl / m.Hp, gxc, gpo);
+    for (int k = 0; k < K; ++k)
+      if (fabsf(pp[k]) > 8.f) gpo[k] = 0.f;
+    gpo[2 * K] = gdy;
+    for (int o = C2; o < CP; ++o) gpo[o] = 0.f;
+    gP[pa] = gxc - gdy;  // dy = H + shift - xc
+  }
+  __syncthreads();
+  float *wp = wpart + (size_t)b * (H * 18 + H + C2 * H * 9 + C2);
+  float *gW1 = wp, *gB1 = wp + H * 18, *gW2 = gB1 + H, *gB2 = gW2 + C2 * H * 9;
+  const float4 *gpv = reinterpret_cast<const float4 *>(gprm);
+  // gW2[o][ci][k] = sum_a gprm[a][o] h[ci][nbr(a, k)]: one (ci, k) per work item, all outputs
+  for (int e = tid; e < H * 9; e += nt) {
+    const int ci = e / 9, k = e - ci * 9;
+    const float *pc = pre + ci * LL;
+    const int *nk = nbt + k * LL;
+    float4 acc[5];
+#pragma unroll
+    for (int j = 0; j < 5; ++j) acc[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int a = 0; a < nact; ++a) {
+      const float v0 = pc[nk[apos[a]]];
+      const float v = v0 > 0.f ? v0 : slope * v0;
+#pragma unroll
+      for (int j = 0; j < 5; ++j)
+        if (j < ng) fma4(acc[j], gpv[a * ng + j], v);
+    }
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      if (j >= ng) break;
+      const float av[4] = {acc[j].x, acc[j].y, acc[j].z, acc[j].w};
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int o = 4 * j + t;
+        if (o < C2) gW2[(size_t)o * H * 9 + e] = av[t];
+      }
+    }
+  }
+  for (int o = tid; o < C2; o += nt) {
+    float acc = 0.f;
+    for (int a = 0; a < nact; ++a) acc += gprm[a * CP + o];
+    gB2[o] = acc;
+  }
+  // gh[ci][p] = sum_k sum_o W2[o][ci][k] gprm[a][o] over active a at p - (k offset); then * LeakyReLU'(pre)
+  for (int q = tid; q < H * LL; q += nt) {
+    const int ci = q / LL, p = q - ci * LL;
+    float acc = 0.f;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const int a = amap[nbt[(8 - k) * LL + p]];  // the pixel whose offset-k neighbour is p
+      if (a >= 0) {
+        const float4 *wv = w2v + ((ci * 9 + k) * CP >> 2);
+        for (int og = 0; og < ng; ++og) {
+          const float4 w = wv[og], gg = gpv[a * ng + og];
+          acc = fmaf(w.x, gg.x, fmaf(w.y, gg.y, fmaf(w.z, gg.z, fmaf(w.w, gg.w, acc))));
+        }
+      }
+    }
+    gh[q] = pre[q] > 0.f ? acc : slope * acc;  // dL/dpre
+  }
+  __syncthreads();
+  // gW1[c][ci][k] = sum_p gpre[c][p] ctx[ci][nbr(p, k)]: one (ci, k, 4 channels) per work item
+  for (int e = tid; e < 18 * (H / 4); e += nt) {
+    const int r = e % 18, c4 = 4 * (e / 18), ci = r / 9, k = r - ci * 9;
+    const float *cx = ctx + ci * LL;
+    const int *nk = nbt + k * LL;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+    for (int p = 0; p < LL; ++p) {
+      const float v = cx[nk[p]];
+      a0 = fmaf(gh[(c4 + 0) * LL + p], v, a0);
+      a1 = fmaf(gh[(c4 + 1) * LL + p], v, a1);
+      a2 = fmaf(gh[(c4 + 2) * LL + p], v, a2);
+      a3 = fmaf(gh[(c4 + 3) * LL + p], v, a3);
+    }
+    gW1[(c4 + 0) * 18 + r] = a0;
+    gW1[(c4 + 1) * 18 + r] = a1;
+    gW1[(c4 + 2) * 18 + r] = a2;
+    gW1[(c4 + 3) * 18 + r] = a3;
+  }
+  for (int c = tid; c < H; c += nt) {
+    float acc = 0.f;
+    for (int p = 0; p < LL; ++p) acc += gh[c * LL + p];
+    gB1[c] = acc;
+  }
+  // gctx[ci][p] = sum_k sum_c W1[c][ci][k] gpre[c][p - (k offset)]
+  for (int q = tid; q < 2 * LL; q += nt) {
+    const int ci = q / LL, p = q - ci * LL;
+    float acc = 0.f;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const int pq = nbt[(8 - k) * LL + p];
+      const float *wr = w1t + (ci * 9 + k) * H;
+      for (int c = 0; c < H; ++c) acc = fmaf(wr[c], gh[c * LL + pq], acc);
+    }
+    gctx[q] = acc;
+  }
+  __syncthreads();
+  // context adjoint into gP (frozen plaquettes): ctx = (cos P, sin P)
+  for (int p = tid; p < LL; p += nt) {
+    const int xn = mu == 0 ? p / L : p % L;
+    const int r = (xn - off) & 3;
+    if (r == 1 || r == 2) {
+      float sn, cs;
+      sincosf(P[p], &sn, &cs);
+      gP[p] += -sn * gctx[p] + cs * gctx[LL + p];
+    }
+  }
+  __syncthreads();
+  // plaquette adjoint: P(x) = th0(x) + th1(x+e0) - th0(x+e1) - th1(x)
+  float *dst = gth_in + (size_t)b * 2 * LL;
+  for (int p = tid; p < LL; p += nt) {
+    const int x0 = p % L, x1 = p / L;
+    const int x0m = x0 == 0 ? L - 1 : x0 - 1, x1m = x1 == 0 ? L - 1 : x1 - 1;
+    dst[p] = go[p] + gP[p] - gP[x1m * L + x0];
+    dst[LL + p] = go[LL + p] + gP[x1 * L + x0m] - gP[p];
+  }
+}
+
+// out[j] = sum over blocks b (in order) of wpart[b][j].
+__global__ void k_flow_wgrad_reduce(const float *__restrict__ wpart, int nb, int nw, float *__restrict__ out) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nw) return;
+  float acc = 0.f;
+  for (int b = 0; b < nb; ++b) acc += wpart[(size_t)b * nw + j];
+  out[j] = acc;
+}
+
+size_t flow_layer_bwd_smem(int L, int K, int H) {
+  const size_t LL = (size_t)L * L, CP = (2 * K + 1 + 3) & ~3, nact = LL / 4;
+  return sizeof(float) * (2 * LL + LL + 2 * LL + 2 * H * LL + 18 * H + H + 9 * H * CP + CP + 2 * nact * CP +
+                          2 * LL + LL + LL + 9 * LL + nact);
+}
+
 size_t flow_layer_smem(int L, int K, int H) {
   const size_t LL = (size_t)L * L, CP = (2 * K + 1 + 3) & ~3;
   return sizeof(float) * (2 * LL + LL + 2 * LL + H * LL + 18 * H + H + 9 * H * CP + CP + (LL / 4) * CP);
@@ -428,5 +697,31 @@ extern "C" int u1_flow_layer_forward(const float *theta_in, float *theta_out, fl
   k_flow_layer_forward<<<batch, 256, smem, (cudaStream_t)stream>>>(theta_in, theta_out, logdet, L, mu, off, K,
                                                                     hidden, W1, B1, W2, B2, slope);
   U1_LAUNCH_CHECK("k_flow_layer_forward");
+  return U1_OK;
+}
+
+extern "C" int u1_flow_layer_backward(const float *theta_in, const float *grad_theta_out, const float *grad_logdet,
+                                      float *grad_theta_in, float *wgrad_partials, float *wgrad, int batch, int L,
+                                      int mu, int off, int K, int hidden, const float *W1, const float *B1,
+                                      const float *W2, const float *B2, float slope, void *stream) {
+  if (!theta_in || !grad_theta_out || !grad_theta_in || !wgrad_partials || !wgrad || !W1 || !B1 || !W2 || !B2)
+    return flfail(U1_ERR_INVALID, "u1_flow_layer_backward: null pointer");
+  if (batch < 1 || L < 4 || L > 16 || L % 4 || (mu != 0 && mu != 1) || off < 0 || off > 3 || K < 1 ||
+      K > kMaxK || hidden < 4 || hidden > 32 || hidden % 4)
+    return flfail(U1_ERR_INVALID,
+                  "u1_flow_layer_backward: bad shape (L a multiple of 4 up to 16, K <= 8, hidden a multiple of 4 up to 32)");
+  const size_t smem = flow_layer_bwd_smem(L, K, hidden);
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_flow_layer_backward, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return u1i::cuda_fail(e, "u1_flow_layer_backward: shared memory");
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  k_flow_layer_backward<<<batch, 256, smem, s>>>(theta_in, grad_theta_out, grad_logdet, grad_theta_in,
+                                                  wgrad_partials, L, mu, off, K, hidden, W1, B1, W2, B2, slope);
+  U1_LAUNCH_CHECK("k_flow_layer_backward");
+  const int nw = hidden * 18 + hidden + (2 * K + 1) * hidden * 9 + (2 * K + 1);
+  k_flow_wgrad_reduce<<<(nw + 255) / 256, 256, 0, s>>>(wgrad_partials, batch, nw, wgrad);
+  U1_LAUNCH_CHECK("k_flow_wgrad_reduce");
   return U1_OK;
 }

@@ -118,6 +118,51 @@ def ncp_inverse(y, params, K):
     return _NCPInverse.apply(y, params, K)
 
 
+class _FusedLayer(torch.autograd.Function):
+    """A whole coupling layer as the library's fused kernels:
+    (theta, W1, B1, W2, B2) -> (theta_out, logdet) with u1_flow_layer_forward,
+    gradients with u1_flow_layer_backward (L <= 16)."""
+
+    @staticmethod
+    def forward(ctx, th, W1, B1, W2, B2, meta):
+        L, mu, off, K, H, slope = meta
+        th = th.contiguous()
+        out = torch.empty_like(th)
+        ld = torch.empty(th.shape[0], device=th.device)
+        with torch.cuda.device(th.device):
+            check(lib.u1_flow_layer_forward(_p(th), _p(out), _p(ld), th.shape[0], L, mu, off, K, H, _p(W1), _p(B1),
+                                            _p(W2), _p(B2), C.c_float(slope), _stream(th)), "u1_flow_layer_forward")
+        ctx.save_for_backward(th, W1, B1, W2, B2)
+        ctx.meta = meta
+        return out, ld
+
+    @staticmethod
+    def backward(ctx, g_out, g_ld):
+        th, W1, B1, W2, B2 = ctx.saved_tensors
+        L, mu, off, K, H, slope = ctx.meta
+        B = th.shape[0]
+        C2 = 2 * K + 1
+        nw = H * 18 + H + C2 * H * 9 + C2
+        g_out = torch.zeros_like(th) if g_out is None else g_out.contiguous()
+        g_ld = None if g_ld is None else g_ld.contiguous().float()
+        gth = torch.empty_like(th)
+        part = torch.empty((B, nw), device=th.device)
+        wg = torch.empty(nw, device=th.device)
+        with torch.cuda.device(th.device):
+            check(lib.u1_flow_layer_backward(_p(th), _p(g_out), _p(g_ld), _p(gth), _p(part), _p(wg), B, L, mu, off,
+                                             K, H, _p(W1), _p(B1), _p(W2), _p(B2), C.c_float(slope), _stream(th)),
+                  "u1_flow_layer_backward")
+        o = 0
+        gW1 = wg[o:o + H * 18].view_as(W1)
+        o += H * 18
+        gB1 = wg[o:o + H]
+        o += H
+        gW2 = wg[o:o + C2 * H * 9].view_as(W2)
+        o += C2 * H * 9
+        gB2 = wg[o:o + C2]
+        return gth, gW1, gB1, gW2, gB2, None
+
+
 def plaquettes_no(th: torch.Tensor) -> torch.Tensor:
     """P(x) = th_0(x) + th_1(x + e0) - th_0(x + e1) - th_1(x) for th[b, mu, x1, x0]."""
     t0, t1 = th[:, 0], th[:, 1]
@@ -190,6 +235,13 @@ class Coupling(nn.Module):
         parts = [upd, flat[:, 1]] if self.mu == 0 else [flat[:, 0], upd]
         return torch.stack(parts, 1).reshape_as(th)
 
+    def forward_fused(self, th: torch.Tensor):
+        """The layer as the library's fused forward/backward kernels (L <= 16
+        for gradients): bf16-rounded weights, FP32 arithmetic."""
+        c1, c2 = self.net[0], self.net[2]
+        meta = (self.L, self.mu, self.off, self.K, c1.out_channels, self.net[1].negative_slope)
+        return _FusedLayer.apply(th, c1.weight, c1.bias, c2.weight, c2.bias, meta)
+
     def forward(self, th: torch.Tensor):
         B = th.shape[0]
         P = plaquettes_no(th)
@@ -229,13 +281,14 @@ class Flow2D(nn.Module):
         out[:, self.perm] = th_eo
         return out.reshape(-1, 2, self.L, self.L)
 
-    def sample(self, B: int, generator: torch.Generator | None = None):
-        """(theta, log q(theta)) for B flow samples."""
+    def sample(self, B: int, generator: torch.Generator | None = None, fused: bool = False):
+        """(theta, log q(theta)) for B flow samples; fused: each layer through
+        the library's fused kernels (differentiable, L <= 16)."""
         dev = self.perm.device
         th = torch.rand((B, 2, self.L, self.L), device=dev, generator=generator) * TWO_PI
         logq = torch.full((B,), self.log_prior, device=dev)
         for layer in self.layers:
-            th, ld = layer(th)
+            th, ld = layer.forward_fused(th) if fused else layer(th)
             logq = logq - ld
         return torch.remainder(th, TWO_PI), logq
 
@@ -287,13 +340,14 @@ class Flow2D(nn.Module):
             ess = (torch.exp(2 * torch.logsumexp(lw, 0) - torch.logsumexp(2 * lw, 0)) / B).item()
         return {"loss": loss.item(), "ess": ess}
 
-    def graphed_reverse_kl(self, opt, B: int):
+    def graphed_reverse_kl(self, opt, B: int, fused: bool = False):
         """The reverse-KL step (sampling, flow, action, backward, optimizer)
         captured once as a CUDA graph; returns a function that replays it and
         the static (loss, S, logq) tensors it refreshes.  opt must be built
-        with capturable=True (e.g. Adam(..., capturable=True))."""
+        with capturable=True (e.g. Adam(..., capturable=True)).  fused: the
+        layers run as the library's fused kernels."""
         def body():
-            th, logq = self.sample(B)
+            th, logq = self.sample(B, fused=fused)
             S = self.S(th)
             loss = (logq + S).mean()
             loss.backward()
@@ -431,7 +485,7 @@ def plain_chain_q(L: int, beta: float, n_chains: int, n_sweeps: int, therm: int 
 def run_experiment(L: int = 16, beta: float = 2.0, n_layers: int = 8, K: int = 6, hidden: int = 32,
                    batch: int = 1024, n_warm: int = 10000, warm_epochs: int = 10, rkl_steps: int = 1000,
                    lr: float = 1e-3, n_props: int = 65536, plain_chains: int = 256, plain_sweeps: int = 2048,
-                   seed: int = 0) -> dict:
+                   seed: int = 0, fused: bool | None = None) -> dict:
     """Config: 2D U(1) L x L at beta; flow of n_layers coupling layers
     (2 conv 3x3 layers of `hidden` channels each) warm-started by forward KL
     on n_warm Metropolis + OR configurations and trained by reverse KL; an
@@ -442,7 +496,10 @@ def run_experiment(L: int = 16, beta: float = 2.0, n_layers: int = 8, K: int = 6
 
     from scipy.special import ive
     torch.manual_seed(seed)
-    res = {"L": L, "beta": beta, "layers": n_layers, "K": K, "hidden": hidden, "batch": batch}
+    if fused is None:
+        fused = L <= 16  # the fused backward kernel covers L <= 16
+    res = {"L": L, "beta": beta, "layers": n_layers, "K": K, "hidden": hidden, "batch": batch,
+           "training_layers": "fused kernels" if fused else "torch/cuDNN"}
     flow = Flow2D(L, beta, n_layers, K, hidden).cuda()
     opt = torch.optim.Adam(flow.parameters(), lr=lr)
     # warm start: forward KL on Markov-chain configurations
@@ -467,7 +524,7 @@ def run_experiment(L: int = 16, beta: float = 2.0, n_layers: int = 8, K: int = 6
     for st in opt2.state.values():
         if "step" in st and not st["step"].is_cuda:
             st["step"] = st["step"].cuda()
-    step, (loss_t, S_t, logq_t) = flow.graphed_reverse_kl(opt2, batch)
+    step, (loss_t, S_t, logq_t) = flow.graphed_reverse_kl(opt2, batch, fused=fused)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     losses, ess = [], []

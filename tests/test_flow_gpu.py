@@ -153,10 +153,11 @@ def test_flow_inverts_and_trains():
 
 def _layer_ref_fp32(c, th):
     """The coupling layer in plain torch FP32 with bf16-rounded weights (the
-    fused kernel's arithmetic): returns (theta', logdet)."""
+    fused kernel's arithmetic; the rounding passes gradients straight
+    through): returns (theta', logdet)."""
     import torch.nn.functional as Fn
     from latticeu1_b200.flow import ncp_forward, plaquettes_no
-    r = lambda t: t.detach().to(torch.bfloat16).float()
+    r = lambda t: t + (t.detach().to(torch.bfloat16).float() - t.detach())
     torch.backends.cudnn.allow_tf32 = False  # plain FP32 convolutions for the reference
     B = th.shape[0]
     P = plaquettes_no(th)
@@ -212,3 +213,33 @@ def test_fused_sampler_consistent_with_inverse():
     # the torch inverse runs its convolutions in bf16 (autocast), so agreement is to bf16 level
     lq2 = flow.log_prob(th)
     assert (lq2 - logq).abs().max().item() < 0.5
+
+
+@pytest.mark.parametrize("L,layer", [(8, 0), (8, 3), (16, 4), (16, 7)])
+def test_fused_layer_backward_matches_autograd(L, layer):
+    """Gradients of the fused layer (theta and all weights) equal torch autograd
+    through the FP32 reference layer with the same bf16-rounded weights."""
+    torch.manual_seed(10 + layer)
+    c = Coupling(L, layer % 2, (layer // 2) % 4, K=6, hidden=32).cuda()
+    with torch.no_grad():
+        for m in c.net:
+            if isinstance(m, torch.nn.Conv2d):
+                m.weight.normal_(0, 0.2)
+                m.bias.normal_(0, 0.2)
+    B = 8
+    th0 = torch.rand(B, 2, L, L, device="cuda") * TWO_PI
+    R = torch.randn(B, 2, L, L, device="cuda")
+    r = torch.randn(B, device="cuda")
+
+    def run(fn):
+        c.zero_grad(set_to_none=True)
+        th = th0.clone().requires_grad_(True)
+        out, ld = fn(th)
+        ((out * R).sum() + (ld * r).sum()).backward()
+        return th.grad.clone(), [p.grad.clone() for p in c.parameters()]
+
+    g_f, w_f = run(c.forward_fused)
+    g_r, w_r = run(lambda t: _layer_ref_fp32(c, t))
+    assert torch.allclose(g_f, g_r, atol=2e-3, rtol=2e-3)
+    for a, b in zip(w_f, w_r):
+        assert torch.allclose(a, b, atol=5e-3 * max(1.0, b.abs().max().item()), rtol=2e-3)
