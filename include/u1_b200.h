@@ -146,10 +146,10 @@ int u1_update(u1_lattice *lat, u1_rng *rng, int metrop, int ovrn);
 
 /* u1_update followed by the plaquette + Polyakov measurement of the new
  * configuration (the reference driver's UpdateLattice then Plaquette and
- * Polyakov, u1.cpp:120-126), with the measurement fused into the sweep's
- * last phase: dev_out (device, 6 doubles) receives {SS re, SS im, ST re,
- * ST im, L re, L im} as u1_measure.  The links are bit-identical to
- * u1_update.  Asynchronous. */
+ * Polyakov, u1.cpp:120-126), with the plaquettes taken from the staples of
+ * the sweep's last pass and one Polyakov kernel after it: dev_out (device,
+ * 6 doubles) receives {SS re, SS im, ST re, ST im, L re, L im} as
+ * u1_measure.  The links are bit-identical to u1_update.  Asynchronous. */
 int u1_update_measure(u1_lattice *lat, u1_rng *rng, int metrop, int ovrn, double *dev_out);
 
 /* Test and debugging aid: run exactly one (parity, mu) phase of a

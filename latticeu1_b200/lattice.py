@@ -216,8 +216,9 @@ class Lattice:
         check(lib.u1_update(self._h, rng.handle, int(metrop), int(ovrn)), "u1_update")
 
     def update_measure(self, rng: Rng, metrop: int, ovrn: int, dev_ptr: int) -> None:
-        """Sweep with the plaquette + Polyakov measurement fused into its last
-        phase; 6 doubles land at device address dev_ptr (asynchronous)."""
+        """Sweep whose last pass also measures the plaquettes and the Polyakov
+        loop of the final configuration; 6 doubles land at device address
+        dev_ptr (asynchronous)."""
         check(lib.u1_update_measure(self._h, rng.handle, int(metrop), int(ovrn), C.c_void_p(dev_ptr)),
               "u1_update_measure")
 
