@@ -2,11 +2,14 @@
 """Throughput of the U(1) Monte Carlo hot path: link-updates/s at 32^4.
 
 Workload (one step): one sweep of 1 Metropolis + 4 overrelaxation passes over a
-32^4 lattice at beta = 1.0 (hot start), followed by the fused plaquette
-(spatial/temporal) + Polyakov-loop measurement, FP64 reductions.  One chain per
-GPU (independent chains, no data-path collective: weak scaling).
+32^4 lattice at beta = 1.0 (hot start) with the plaquette (spatial/temporal) +
+Polyakov-loop measurement of the new configuration (taken from the sweep's
+last pass), FP64 reductions.  One chain per GPU (independent chains, no
+data-path collective: weak scaling).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--geom Nx,Ny,Nz,Nt | --L L] [--beta B] [--aniso XI]
+                  [--workload update32|batched|multilevel]
 
 `value` is device time (CUDA events on the lattice's stream, L2 flushed
 between steps), `e2e` runs the same step through the C ABI with host buffers:
