@@ -8,7 +8,7 @@ tune cache) and exits on CUDA errors, so every task runs in a fresh child:
 
     python -m oracle.ref_gpu <task> <in.npz> <out.npz>
 
-tasks: measure | or_pass | poly2 | multilevel | timing
+tasks: measure | or_pass | poly2 | multilevel | multilevel_timing | timing
 """
 from __future__ import annotations
 
@@ -68,6 +68,16 @@ def _child(task: str, fin: str, fout: str) -> None:
         c = np.zeros(2 * R)
         a = [int(v) for v in d["args"]]  # n4, k4, n2, k2, metrop, ovrn
         lib.ref_gpu_multilevel(lat.ctypes.data_as(_dp), *a, 1234, c.ctypes.data_as(_dp))
+        out["c"] = c
+    elif task == "multilevel_timing":
+        import time
+        c = np.zeros(2 * R)
+        a = [int(v) for v in d["args"]]  # n4, k4, n2, k2, metrop, ovrn
+        # first call: the reference tunes its kernels on first use
+        lib.ref_gpu_multilevel(lat.ctypes.data_as(_dp), 1, a[1], 2, a[3], a[4], a[5], 1234, c.ctypes.data_as(_dp))
+        t0 = time.perf_counter()
+        lib.ref_gpu_multilevel(lat.ctypes.data_as(_dp), *a, 1234, c.ctypes.data_as(_dp))
+        out["s"] = np.array([time.perf_counter() - t0])
         out["c"] = c
     elif task == "timing":
         warm, n = int(d["warmup"]), int(d["sweeps"])

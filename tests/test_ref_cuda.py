@@ -114,3 +114,41 @@ def test_throughput_vs_reference_cuda(ctx, ref_gpu):
         with open(out, "w") as f:
             json.dump(result, f, indent=1)
     assert ours_ms < ref_ms, result
+
+
+def test_multilevel_throughput_vs_reference_cuda(ctx, ref_gpu):
+    """MultiLevel at 24^3 x 32, beta = 0.95 (n4 = 1, k4 = 1, n2 = 20, k2 = 1,
+    1 Metropolis + 4 OR per sub-update): the reference's CUDA build (after a
+    first call that tunes its kernels) against u1_multilevel, wall clock of
+    one call each on the same B200 and configuration."""
+    import torch
+
+    from latticeu1_b200 import Lattice, Rng
+    N = (24, 24, 24, 32)
+    lat = Lattice(ctx, 4, N, 0.95)
+    rng = Rng(ctx, 5)
+    lat.hot_start(rng)
+    for _ in range(20):
+        lat.update(rng, 1, 4)
+    th = lat.export_angles()
+    args = np.array([1, 1, 20, 1, 1, 4])
+    r = ref_gpu.run("multilevel_timing", _inputs(4, N, 0.95, 1.0, th, args=args))
+    ref_s = float(r["s"][0])
+    lat.multilevel(rng, 1, 1, 2, 1, 1, 4)  # warm-up (graph capture, allocations)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    lat.multilevel(rng, *[int(a) for a in args])
+    ours_s = time.perf_counter() - t0
+    assert ours_s < ref_s
+    result = {"workload": "24^3x32 beta=0.95 MultiLevel(n4=1,k4=1,n2=20,k2=1,metrop=1,ovrn=4)",
+              "reference_cuda_s": ref_s, "ours_s": ours_s, "speedup": ref_s / ours_s}
+    print(json.dumps(result))
+    out = os.environ.get("U1_REF_TIMING_OUT")
+    if out:
+        d = {}
+        if os.path.exists(out):
+            with open(out) as f:
+                d = json.load(f)
+        d["multilevel"] = result
+        with open(out, "w") as f:
+            json.dump(d, f, indent=1)
