@@ -99,3 +99,37 @@ def test_reference_driver_runs_unmodified(tmp_path):
     ml = np.loadtxt(tmp_path / f"Pot_mlevel_{name}_iter_1000_10_1_20_1_2_5.dat")
     assert ml.shape == (12, 3) and np.all(np.isfinite(ml))
     assert re.search(r"Time: [0-9.eE+-]+ s", res.stdout)
+
+
+@pytest.mark.gpu
+def test_timing_driver_reference_vs_dropin(tmp_path):
+    """tests/dropin/timing_driver.cpp (the reference driver's workload through
+    its namespace U1 API) built against the reference's own objects and
+    against the drop-in shim: both run, agree on the physics scale, and the
+    drop-in is faster.  Writes the timings to $U1_REF_TIMING_OUT when set."""
+    import json
+    import os
+    import subprocess
+    ref_exe = ROOT / "oracle" / "_ref" / "timing_reference"
+    our_exe = ROOT / "oracle" / "_ref" / "timing_dropin"
+    if not (ref_exe.exists() and our_exe.exists()):
+        pytest.skip("timing drivers not built (make -C oracle timing)")
+    out = {}
+    for name, exe in (("reference", ref_exe), ("dropin", our_exe)):
+        r = subprocess.run([str(exe)], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+        lines = {ln.split()[0]: ln.split()[1:] for ln in r.stdout.splitlines() if ln.strip()}
+        out[name] = {"time_s": float(lines["TIME"][0]), "plaq_ss": float(lines["SWEEP"][1]),
+                     "plaq_st": float(lines["SWEEP"][2])}
+    # independent chains at the same beta: equilibrium plaquettes agree to a few 1e-3
+    assert abs(out["reference"]["plaq_ss"] - out["dropin"]["plaq_ss"]) < 0.01
+    assert out["dropin"]["time_s"] < out["reference"]["time_s"]
+    path = os.environ.get("U1_REF_TIMING_OUT")
+    if path:
+        d = {}
+        if os.path.exists(path):
+            with open(path) as f:
+                d = json.load(f)
+        d["driver_24x24x24x12_1000_sweeps"] = out
+        with open(path, "w") as f:
+            json.dump(d, f, indent=1)
