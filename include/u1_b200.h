@@ -215,6 +215,12 @@ int u1_batch_destroy(u1_batch *b);
 int u1_batch_set_stream(u1_batch *b, void *stream);
 /* out = {nchains, dims, total links, two-sites-per-thread kernels in use}. */
 int u1_batch_info(const u1_batch *b, int64_t out[4]);
+/* Number of chain groups a sweep runs one after another (consecutive chains
+ * whose links fit comfortably in L2, so that each group's sweep after its
+ * first phase is served from L2).  The result is the same as one group.
+ * The group size is U1_BATCH_GROUP_MB MiB (default 64; 0: one group), read
+ * at u1_batch_create. */
+int u1_batch_groups(const u1_batch *b, int *groups);
 /* Hot start of every chain (as u1_hot_start); advances the pass counter by 1. */
 int u1_batch_hot_start(u1_batch *b);
 /* One sweep of every chain: metrop Metropolis then ovrn overrelaxation

@@ -75,6 +75,7 @@ SIGNATURES = {
     "u1_batch_destroy": [_vp],
     "u1_batch_set_stream": [_vp, _vp],
     "u1_batch_info": [_vp, C.POINTER(C.c_int64)],
+    "u1_batch_groups": [_vp, C.POINTER(_i)],
     "u1_batch_hot_start": [_vp],
     "u1_batch_update": [_vp, _i, _i, _i],
     "u1_batch_measure": [_vp, _dp],

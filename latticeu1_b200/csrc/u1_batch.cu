@@ -12,6 +12,10 @@
 // a CUDA graph and replayed.  Per-chain plaquette/Polyakov results come from
 // per-block partials summed in block order by one CTA per chain.
 #include <algorithm>
+#include <climits>
+#include <cstdint>
+#include <cstdlib>
+#include <array>
 #include <cstring>
 #include <map>
 #include <string>
@@ -40,6 +44,7 @@ struct BatchChain {
 struct BatchPhase {
   int p;
   int hit;
+  int block_base;  // first block of the chain group this launch covers
   uint32_t key0, key1;
   const unsigned long long *pass_dev;
   unsigned long long *bump_ptr;
@@ -59,7 +64,8 @@ template <int D, int MU, bool MET, bool PAIR>
 __global__ void __launch_bounds__(256, 8)
     k_batch_update(const BatchChain *__restrict__ chains, const int *__restrict__ block_chain, BatchPhase ph) {
   __shared__ BatchChain sch;
-  const int cidx = __ldg(block_chain + blockIdx.x);
+  const int blk = (int)blockIdx.x + ph.block_base;
+  const int cidx = __ldg(block_chain + blk);
   stage_chain(chains, cidx, sch);
   UpdArgs a{};
   a.lat = sch.links;
@@ -74,7 +80,7 @@ __global__ void __launch_bounds__(256, 8)
   a.hit = ph.hit;
   a.bump_ptr = ph.bump_ptr;
   a.bump_by = ph.bump_by;
-  const int local = (int)blockIdx.x - (PAIR ? sch.first_pair : sch.first_site);
+  const int local = blk - (PAIR ? sch.first_pair : sch.first_site);
   if (PAIR)
     update_pair_body<D, MU, MET, false>(a, 2 * (local * blockDim.x + threadIdx.x));
   else
@@ -146,6 +152,11 @@ struct u1_batch {
   int nb_pair = 0, nb_site = 0, nb_meas = 0;
   double *partials = nullptr, *d_out = nullptr, *h_out = nullptr;
   std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
+  // Chain groups swept one after another: consecutive chains whose links
+  // together fit comfortably in L2, so that after a group's first phase its
+  // links are served from L2.  Each: first pair block, pair blocks, first
+  // site block, site blocks.
+  std::vector<std::array<int, 4>> groups;
 };
 
 using u1i::cuda_fail;
@@ -236,6 +247,33 @@ extern "C" int u1_batch_create(u1_ctx *ctx, int nchains, const u1_geom *geoms, u
   b->nb_pair = (int)tab_pair.size();
   b->nb_site = (int)tab_site.size();
   b->nb_meas = (int)tab_meas.size();
+  {
+    // groups of at most U1_BATCH_GROUP_MB (default 64) MiB of links; a
+    // single chain may exceed it; 0 puts every chain in one group
+    size_t kGroupBytes = 64ull << 20;
+    if (const char *env = std::getenv("U1_BATCH_GROUP_MB")) {
+      const long long mb = std::atoll(env);
+      kGroupBytes = mb > 0 ? (size_t)mb << 20 : SIZE_MAX;
+    }
+    size_t bytes = 0;
+    int c0 = 0;
+    auto close_group = [&](int c1) {
+      const BatchChain &a = b->h_chains[c0];
+      const int pair_end = c1 < nchains ? b->h_chains[c1].first_pair : b->nb_pair;
+      const int site_end = c1 < nchains ? b->h_chains[c1].first_site : b->nb_site;
+      b->groups.push_back({a.first_pair, pair_end - a.first_pair, a.first_site, site_end - a.first_site});
+    };
+    for (int c = 0; c < nchains; ++c) {
+      const size_t cb = (size_t)b->h_chains[c].g.V * b->h_chains[c].g.dims * sizeof(float2);
+      if (c > c0 && bytes + cb > kGroupBytes) {
+        close_group(c);
+        c0 = c;
+        bytes = 0;
+      }
+      bytes += cb;
+    }
+    close_group(nchains);
+  }
   cudaError_t e = cudaStreamCreate(&b->own_stream);
   b->stream = ctx->stream ? ctx->stream : b->own_stream;
   if (e == cudaSuccess) e = cudaMalloc(&b->links, b->total_links * sizeof(float2));
@@ -294,6 +332,12 @@ extern "C" int u1_batch_info(const u1_batch *b, int64_t out[4]) {
   return U1_OK;
 }
 
+extern "C" int u1_batch_groups(const u1_batch *b, int *groups) {
+  if (!b || !groups) return bfail(U1_ERR_INVALID, "u1_batch_groups: null argument");
+  *groups = (int)b->groups.size();
+  return U1_OK;
+}
+
 extern "C" int u1_batch_hot_start(u1_batch *b) {
   if (!b) return bfail(U1_ERR_INVALID, "u1_batch_hot_start: null batch");
   U1_CUDA_TRY(cudaSetDevice(b->ctx->device));
@@ -311,9 +355,11 @@ extern "C" int u1_batch_hot_start(u1_batch *b) {
 }
 
 template <int D, int MU, bool MET, bool PAIR>
-static int batch_launch(u1_batch *b, const BatchPhase &ph) {
+static int batch_launch(u1_batch *b, BatchPhase ph, int group) {
+  const std::array<int, 4> &gr = b->groups[group];
+  ph.block_base = PAIR ? gr[0] : gr[2];
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)(PAIR ? b->nb_pair : b->nb_site));
+  cfg.gridDim = dim3((unsigned)(PAIR ? gr[1] : gr[3]));
   cfg.blockDim = dim3(256);
   cfg.stream = b->stream;
   cudaLaunchAttribute attr[1];
@@ -329,21 +375,22 @@ static int batch_launch(u1_batch *b, const BatchPhase &ph) {
 }
 
 template <int D, int MU>
-static int batch_launch_mu(u1_batch *b, const BatchPhase &ph, bool met) {
-  if (b->pair_ok) return met ? batch_launch<D, MU, true, true>(b, ph) : batch_launch<D, MU, false, true>(b, ph);
-  return met ? batch_launch<D, MU, true, false>(b, ph) : batch_launch<D, MU, false, false>(b, ph);
+static int batch_launch_mu(u1_batch *b, const BatchPhase &ph, bool met, int group) {
+  if (b->pair_ok)
+    return met ? batch_launch<D, MU, true, true>(b, ph, group) : batch_launch<D, MU, false, true>(b, ph, group);
+  return met ? batch_launch<D, MU, true, false>(b, ph, group) : batch_launch<D, MU, false, false>(b, ph, group);
 }
 
 template <int D>
-static int batch_phase(u1_batch *b, const BatchPhase &ph, int mu, bool met) {
+static int batch_phase(u1_batch *b, const BatchPhase &ph, int mu, bool met, int group) {
   switch (mu) {
-    case 0: return batch_launch_mu<D, 0>(b, ph, met);
-    case 1: return batch_launch_mu<D, 1>(b, ph, met);
+    case 0: return batch_launch_mu<D, 0>(b, ph, met, group);
+    case 1: return batch_launch_mu<D, 1>(b, ph, met, group);
     case 2:
-      if constexpr (D > 2) return batch_launch_mu<D, 2>(b, ph, met);
+      if constexpr (D > 2) return batch_launch_mu<D, 2>(b, ph, met, group);
       break;
     case 3:
-      if constexpr (D > 3) return batch_launch_mu<D, 3>(b, ph, met);
+      if constexpr (D > 3) return batch_launch_mu<D, 3>(b, ph, met, group);
       break;
   }
   return bfail(U1_ERR_INVALID, "batch phase: direction out of range");
@@ -372,29 +419,39 @@ static int batch_issue_sweep(u1_batch *b, int metrop, int ovrn, bool measure) {
   ph.key1 = (uint32_t)(b->seed >> 32);
   ph.pass_dev = b->pass_dev;
   const int D = b->dims;
-  auto run = [&](int mu, bool met) {
-    return D == 2 ? batch_phase<2>(b, ph, mu, met) : D == 3 ? batch_phase<3>(b, ph, mu, met) : batch_phase<4>(b, ph, mu, met);
-  };
-  for (int m = 0; m < metrop; ++m)
-    for (int p = 0; p < 2; ++p)
-      for (int mu = 0; mu < D; ++mu) {
-        ph.p = p;
-        ph.hit = m;
-        int rc = run(mu, true);
-        if (rc) return rc;
-      }
+  const int ngroups = (int)b->groups.size();
+  // Each chain group runs the whole sweep before the next starts.  Every
+  // group's Metropolis phases read the same pass counter; the first
+  // overrelaxation kernel of the last group (after all of them) bumps it.
   bool bumped = (metrop == 0);
-  for (int o = 0; o < ovrn; ++o)
-    for (int p = 0; p < 2; ++p)
-      for (int mu = 0; mu < D; ++mu) {
-        ph.p = p;
-        ph.hit = 0;
-        ph.bump_ptr = bumped ? nullptr : b->pass_dev;
-        ph.bump_by = (unsigned)metrop;
-        bumped = true;
-        int rc = run(mu, false);
-        if (rc) return rc;
-      }
+  for (int grp = 0; grp < ngroups; ++grp) {
+    auto run = [&](int mu, bool met) {
+      return D == 2 ? batch_phase<2>(b, ph, mu, met, grp)
+           : D == 3 ? batch_phase<3>(b, ph, mu, met, grp)
+                    : batch_phase<4>(b, ph, mu, met, grp);
+    };
+    for (int m = 0; m < metrop; ++m)
+      for (int p = 0; p < 2; ++p)
+        for (int mu = 0; mu < D; ++mu) {
+          ph.p = p;
+          ph.hit = m;
+          ph.bump_ptr = nullptr;
+          int rc = run(mu, true);
+          if (rc) return rc;
+        }
+    for (int o = 0; o < ovrn; ++o)
+      for (int p = 0; p < 2; ++p)
+        for (int mu = 0; mu < D; ++mu) {
+          ph.p = p;
+          ph.hit = 0;
+          const bool carry = !bumped && grp == ngroups - 1;
+          ph.bump_ptr = carry ? b->pass_dev : nullptr;
+          ph.bump_by = (unsigned)metrop;
+          if (carry) bumped = true;
+          int rc = run(mu, false);
+          if (rc) return rc;
+        }
+  }
   if (!bumped) {  // no overrelaxation kernel carried the pass-counter bump
     k_pass_add<<<1, 1, 0, b->stream>>>(b->pass_dev, (unsigned long long)metrop);
     U1_LAUNCH_CHECK("k_pass_add");
@@ -429,7 +486,7 @@ extern "C" int u1_batch_update(u1_batch *b, int metrop, int ovrn, int measure) {
     it = b->graphs.emplace(key, ex).first;
   }
   U1_CUDA_TRY(cudaGraphLaunch(it->second, b->stream));
-  u1i::g_launches += (unsigned long long)(2 * b->dims * (metrop + ovrn) + (measure ? 2 : 0) +
+  u1i::g_launches += (unsigned long long)(2 * b->dims * (metrop + ovrn) * b->groups.size() + (measure ? 2 : 0) +
                                           (ovrn == 0 && metrop > 0 ? 1 : 0));
   b->pass += (uint64_t)metrop;
   return U1_OK;

@@ -370,6 +370,13 @@ class Batch:
         dims, V = self.shapes[chain]
         return dims * V
 
+    @property
+    def groups(self) -> int:
+        """Chain groups a sweep runs one after another (L2-sized)."""
+        v = C.c_int()
+        check(lib.u1_batch_groups(self._h, C.byref(v)), "u1_batch_groups")
+        return int(v.value)
+
     def set_stream(self, stream_ptr: int | None) -> None:
         check(lib.u1_batch_set_stream(self._h, C.c_void_p(stream_ptr or 0)), "u1_batch_set_stream")
 

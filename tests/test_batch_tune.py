@@ -111,6 +111,7 @@ def test_auto_variant_tunes_on_first_update(ctx, monkeypatch, tmp_path):
 
 
 BATCH_SETS = {
+    "4d-groups": [(4, (24, 24, 24, 24), 0.9 + 0.05 * k) for k in range(8)],  # 85 MB of links: two groups
     "4d-mixed": [(4, (8, 8, 8, 8), 1.0), (4, (12, 8, 4, 8), 0.85, 1.2), (4, (8, 4, 4, 16), 1.15)],
     "4d-odd-row": [(4, (6, 6, 4, 4), 1.0), (4, (8, 8, 8, 8), 0.9)],
     "3d": [(3, (8, 8, 0, 8), 1.2), (3, (16, 12, 0, 8), 1.6, 0.9)],
@@ -123,6 +124,8 @@ def test_batch_matches_single_lattices(ctx, name):
     geoms = BATCH_SETS[name]
     seed, first = 2024, 17
     b = Batch(ctx, geoms, seed=seed, first_chain=first)
+    if name == "4d-groups":
+        assert b.groups == 2
     b.hot_start()
     plan = ((1, 4, False), (2, 0, False), (1, 2, True))
     for m, o, meas in plan:
