@@ -57,10 +57,11 @@ def geom_name(N) -> str:
     return f"{N[0]}^4" if len(set(N)) == 1 else "x".join(str(n) for n in N)
 
 
-def workload_config(N, beta: float = BETA, aniso: float = 1.0) -> dict:
+def workload_config(N, beta: float = BETA, aniso: float = 1.0, delta: float = 0.0, nhits: int = 1) -> dict:
     name = geom_name(N)
+    prop = "" if (delta == 0.0 and nhits == 1) else f" Metropolis delta={delta:.6g} nhits={nhits}"
     cfg = {
-        "workload": f"U(1) Wilson 4D {name} beta={beta}" + (f" aniso={aniso}" if aniso != 1.0 else "") +
+        "workload": f"U(1) Wilson 4D {name} beta={beta}" + (f" aniso={aniso}" if aniso != 1.0 else "") + prop +
                     " hot start; step = 1 Metropolis + 4 OR sweep + plaquette(SS/ST)+Polyakov measurement "
                     "taken from the sweep's last pass",
         "lattice": name, "beta": beta, "metrop": METROP, "ovrn": OVRN,
@@ -70,6 +71,8 @@ def workload_config(N, beta: float = BETA, aniso: float = 1.0) -> dict:
     }
     if aniso != 1.0:
         cfg["aniso"] = aniso
+    if prop:
+        cfg["metropolis"] = {"delta": delta, "nhits": nhits}
     return cfg
 
 
@@ -260,6 +263,7 @@ def run_ours(args) -> None:
     N, beta, aniso = geometry(args)
     ctx = Context(local)
     lat = Lattice(ctx, DIMS, N, beta, aniso)
+    lat.set_metropolis(args.delta, args.nhits)
     stream = torch.cuda.Stream()
     lat.set_stream(stream.cuda_stream)
     rng = Rng(ctx, 1234)
@@ -341,7 +345,7 @@ def run_ours(args) -> None:
             "metric": metric_for(N), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": workload_config(N, beta, aniso),
+            "config": workload_config(N, beta, aniso, args.delta, args.nhits),
             "roofline": {"bound": "hbm", "kernel": "k_update_pair (one (parity,mu) phase; step average)",
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
@@ -360,7 +364,8 @@ def run_ours(args) -> None:
                             "abs_L": float(np.abs(ob[:, 4] + 1j * ob[:, 5]).mean()),
                             "per_chain_plaq_ss_st": per_chain},
         }
-        if world == 1 and not args.no_cpu_baseline:
+        if world == 1 and not args.no_cpu_baseline and args.delta == 0.0 and args.nhits == 1:
+            # the reference's CPU update has only the whole-circle single-hit proposal
             line["cpu_baseline"] = cpu_reference_rate(N, beta, aniso, args.cpu_budget)
         print(json.dumps(line), flush=True)
     lat.close()
@@ -543,6 +548,9 @@ def main() -> None:
     ap.add_argument("--geom", type=str, default=None, help="Nx,Ny,Nz,Nt instead of --L (update workload)")
     ap.add_argument("--beta", type=float, default=BETA)
     ap.add_argument("--aniso", type=float, default=1.0)
+    ap.add_argument("--delta", type=float, default=0.0,
+                    help="Metropolis proposal half-width (0: the reference's whole-circle proposal)")
+    ap.add_argument("--nhits", type=int, default=1, help="Metropolis hits per link and pass")
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU baseline sampling")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["update32", "multilevel", "batched"], default="update32")

@@ -92,6 +92,19 @@ int u1_lattice_set_graphs(u1_lattice *lat, int enable);
 int u1_lattice_set_variant(u1_lattice *lat, int variant);
 /* The variant in use: 0 while automatic and not yet tuned. */
 int u1_lattice_get_variant(const u1_lattice *lat, int *variant);
+/* Metropolis proposal (no reference counterpart; the reference proposes
+ * theta' = 2 pi u on the whole circle, once per link and pass,
+ * src/update.cu:181-182, and that stays the default: delta = 0, nhits = 1).
+ * nhits (1..127) hits per link and Metropolis pass, the staple held fixed;
+ * hit h proposes theta' = theta + delta (2u - 1) for delta in (0, pi]
+ * (theta' = 2 pi u for delta = 0) and accepts when
+ * exp(beta Re(S (U' - U))) > b.  Hit h draws its (u, b) from the Philox
+ * counter of the pass with stream tag 0 for h = 0 and 0x80 | h for h >= 1.
+ * Applies to u1_update, u1_update_measure, u1_update_phase and the
+ * multilevel sub-updates of this lattice; the persistent variant 4 is then
+ * replaced by the default phase kernels. */
+int u1_lattice_set_metropolis(u1_lattice *lat, double delta, int nhits);
+int u1_lattice_get_metropolis(const u1_lattice *lat, double *delta, int *nhits);
 /* Replaces the reference's autotuner (tuneLaunch, src/tune.cpp:306-416):
  * times every valid variant on a few sweeps of this lattice from a
  * backed-up state (links and rng pass restored afterwards), keeps the

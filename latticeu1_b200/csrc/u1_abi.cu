@@ -482,42 +482,49 @@ static int launch_pdl(K kernel, int blocks, cudaStream_t s, const UpdArgs &a, co
   return U1_OK;
 }
 
-// The phase kernel of the chosen variant.
-template <int D, int MU>
-static int launch_phase_mu(const UpdArgs &a, cudaStream_t s, bool met, bool replay, int variant) {
+// The phase kernel of the chosen variant; src: the Metropolis proposal
+// source (SRC_PHILOX, SRC_REPLAY or SRC_WINDOW; ignored for overrelaxation).
+template <int D, int MU, int SRC>
+static int launch_variant(const UpdArgs &a, cudaStream_t s, bool met, int variant) {
   if (variant == U1V_PAIR32 || variant == U1V_PAIR) {
     const int blocks = u1i::blocks_for(a.g.Vh / 2, 256);
-    if (variant == U1V_PAIR32) {
-      if (met)
-        return replay ? launch_pdl(k_update_pair<D, MU, true, true>, blocks, s, a, "k_update_pair")
-                      : launch_pdl(k_update_pair<D, MU, true, false>, blocks, s, a, "k_update_pair");
-      return launch_pdl(k_update_pair<D, MU, false, false>, blocks, s, a, "k_update_pair");
-    }
-    if (met)
-      return replay ? launch_pdl(k_update_pair_free<D, MU, true, true>, blocks, s, a, "k_update_pair_free")
-                    : launch_pdl(k_update_pair_free<D, MU, true, false>, blocks, s, a, "k_update_pair_free");
-    return launch_pdl(k_update_pair_free<D, MU, false, false>, blocks, s, a, "k_update_pair_free");
+    if (variant == U1V_PAIR32)
+      return met ? launch_pdl(k_update_pair<D, MU, true, SRC>, blocks, s, a, "k_update_pair")
+                 : launch_pdl(k_update_pair<D, MU, false, SRC_PHILOX>, blocks, s, a, "k_update_pair");
+    return met ? launch_pdl(k_update_pair_free<D, MU, true, SRC>, blocks, s, a, "k_update_pair_free")
+               : launch_pdl(k_update_pair_free<D, MU, false, SRC_PHILOX>, blocks, s, a, "k_update_pair_free");
   }
   const int blocks = u1i::blocks_for(a.g.Vh, 256);
-  if (met)
-    return replay ? launch_pdl(k_update<D, MU, true, true>, blocks, s, a, "k_update")
-                  : launch_pdl(k_update<D, MU, true, false>, blocks, s, a, "k_update");
-  return launch_pdl(k_update<D, MU, false, false>, blocks, s, a, "k_update");
+  return met ? launch_pdl(k_update<D, MU, true, SRC>, blocks, s, a, "k_update")
+             : launch_pdl(k_update<D, MU, false, SRC_PHILOX>, blocks, s, a, "k_update");
+}
+
+template <int D, int MU>
+static int launch_phase_mu(const UpdArgs &a, cudaStream_t s, bool met, int src, int variant) {
+  if (!met || src == SRC_PHILOX) return launch_variant<D, MU, SRC_PHILOX>(a, s, met, variant);
+  if (src == SRC_REPLAY) return launch_variant<D, MU, SRC_REPLAY>(a, s, met, variant);
+  return launch_variant<D, MU, SRC_WINDOW>(a, s, met, variant);
 }
 
 template <int D>
-static int launch_phase(const UpdArgs &a, cudaStream_t s, bool met, bool replay, int variant) {
+static int launch_phase(const UpdArgs &a, cudaStream_t s, bool met, int src, int variant) {
   switch (a.mu) {
-    case 0: return launch_phase_mu<D, 0>(a, s, met, replay, variant);
-    case 1: return launch_phase_mu<D, 1>(a, s, met, replay, variant);
+    case 0: return launch_phase_mu<D, 0>(a, s, met, src, variant);
+    case 1: return launch_phase_mu<D, 1>(a, s, met, src, variant);
     case 2:
-      if constexpr (D > 2) return launch_phase_mu<D, 2>(a, s, met, replay, variant);
+      if constexpr (D > 2) return launch_phase_mu<D, 2>(a, s, met, src, variant);
       break;
     case 3:
-      if constexpr (D > 3) return launch_phase_mu<D, 3>(a, s, met, replay, variant);
+      if constexpr (D > 3) return launch_phase_mu<D, 3>(a, s, met, src, variant);
       break;
   }
   return fail(U1_ERR_INVALID, "k_update: direction out of range");
+}
+
+// The proposal settings of `lat` into the kernel arguments.
+static void set_proposal(UpdArgs &a, const u1_lattice *lat) {
+  a.win = lat->win;
+  a.nhits = lat->nhits;
 }
 
 // Variant used when the tuner has not chosen one.
@@ -600,10 +607,27 @@ static int effective_variant(const u1_lattice *lat) {
   return lat->variant == U1V_AUTO ? default_variant(lat->g) : lat->variant;
 }
 
+// Metropolis proposal source of a lattice with this rng: the replay stream
+// when one is set, else the windowed multi-hit kernels unless the lattice
+// keeps the reference's single whole-circle proposal.
+static int metropolis_src(const u1_lattice *lat, const u1_rng *rng) {
+  if (rng->replay_dev) return SRC_REPLAY;
+  return (lat->win != 0.f || lat->nhits != 1) ? SRC_WINDOW : SRC_PHILOX;
+}
+
+// The variant a sweep with proposal source `src` and freeze period ml runs:
+// the persistent sweep covers only plain whole-circle sweeps; otherwise a
+// lattice set to it runs the default phase kernels (bit-identical).
+static int sweep_variant(const u1_lattice *lat, int src, int ml) {
+  const int v = effective_variant(lat);
+  if (v == U1V_WAVE && (ml != 0 || src != SRC_PHILOX)) return default_variant(lat->g);
+  return v;
+}
+
 // Phase (1, MU) of the last pass with the measurement terms (u1_fused.cuh),
 // writing the per-block partials of slot MU-1 into `partials`.
 template <int D, int MU>
-static int launch_meas_phase_mu(const UpdArgs &a, cudaStream_t s, bool met, double *partials) {
+static int launch_meas_phase_mu(const UpdArgs &a, cudaStream_t s, bool met, bool win, double *partials) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)meas_phase_blocks(a.g));
   cfg.blockDim = dim3(256);
@@ -616,25 +640,27 @@ static int launch_meas_phase_mu(const UpdArgs &a, cudaStream_t s, bool met, doub
   double *slot = partials + (size_t)(MU - 1) * meas_phase_blocks(a.g) * 2;
   cudaError_t e;
   if ((a.g.hN0 & 1) == 0)
-    e = met ? cudaLaunchKernelEx(&cfg, k_update_pair_meas<D, MU, true>, a, slot)
-            : cudaLaunchKernelEx(&cfg, k_update_pair_meas<D, MU, false>, a, slot);
+    e = !met ? cudaLaunchKernelEx(&cfg, k_update_pair_meas<D, MU, false>, a, slot)
+        : win ? cudaLaunchKernelEx(&cfg, k_update_pair_meas<D, MU, true, SRC_WINDOW>, a, slot)
+              : cudaLaunchKernelEx(&cfg, k_update_pair_meas<D, MU, true>, a, slot);
   else
-    e = met ? cudaLaunchKernelEx(&cfg, k_update_meas<D, MU, true>, a, slot)
-            : cudaLaunchKernelEx(&cfg, k_update_meas<D, MU, false>, a, slot);
+    e = !met ? cudaLaunchKernelEx(&cfg, k_update_meas<D, MU, false>, a, slot)
+        : win ? cudaLaunchKernelEx(&cfg, k_update_meas<D, MU, true, SRC_WINDOW>, a, slot)
+              : cudaLaunchKernelEx(&cfg, k_update_meas<D, MU, true>, a, slot);
   u1i::g_launches.fetch_add(1, std::memory_order_relaxed);
   if (e != cudaSuccess) return u1i::cuda_fail(e, "k_update_pair_meas");
   return U1_OK;
 }
 
 template <int D>
-static int launch_meas_phase(const UpdArgs &a, cudaStream_t s, bool met, double *partials) {
+static int launch_meas_phase(const UpdArgs &a, cudaStream_t s, bool met, bool win, double *partials) {
   switch (a.mu) {
-    case 1: return launch_meas_phase_mu<D, 1>(a, s, met, partials);
+    case 1: return launch_meas_phase_mu<D, 1>(a, s, met, win, partials);
     case 2:
-      if constexpr (D > 2) return launch_meas_phase_mu<D, 2>(a, s, met, partials);
+      if constexpr (D > 2) return launch_meas_phase_mu<D, 2>(a, s, met, win, partials);
       break;
     case 3:
-      if constexpr (D > 3) return launch_meas_phase_mu<D, 3>(a, s, met, partials);
+      if constexpr (D > 3) return launch_meas_phase_mu<D, 3>(a, s, met, win, partials);
       break;
   }
   return fail(U1_ERR_INVALID, "measuring phase: direction out of range");
@@ -655,7 +681,7 @@ static size_t meas_sweep_scratch(const GeomK &g) {
 
 // The Polyakov loops and the final sum of a measured sweep, into dev_out.
 template <int D>
-static int launch_poly_finish(u1_lattice *lat, double *dev_out) {
+static int launch_poly_finish(u1_lattice *lat, int variant, double *dev_out) {
   const GeomK &g = lat->g;
   MeasK m = measure_layout(g);
   int nSS = 0, nST = 0;
@@ -663,7 +689,7 @@ static int launch_poly_finish(u1_lattice *lat, double *dev_out) {
     for (int nu = mu + 1; nu < D; ++nu) (nu == D - 1 ? nST : nSS)++;
   const double normSS = 1.0 / ((double)g.V * nSS), normST = 1.0 / ((double)g.V * nST);
   const double normL = 1.0 / (double)g.Vs;
-  const int nbp = meas_slot_entries(lat, effective_variant(lat));
+  const int nbp = meas_slot_entries(lat, variant);
   double *poly = lat->partials + (size_t)(D - 1) * nbp * 2;
   k_poly_finish<D><<<m.nb_poly, kRedThreads, 0, lat->stream>>>(lat->links, g, m, lat->partials, nbp, poly,
                                                                lat->counter, dev_out, normSS, normST, normL);
@@ -689,9 +715,10 @@ static int issue_sweep(u1_lattice *lat, float2 *links, u1_rng *rng, int metrop, 
   a.replay = rng->replay_dev;
   a.replay_base = rng->replay_base;
   a.ml = ml;
-  const bool replay = rng->replay_dev != nullptr;
-  if (ml == 0 && !replay && effective_variant(lat) == U1V_WAVE)
-    return launch_wave(lat, links, rng, metrop, ovrn, meas_partials);
+  set_proposal(a, lat);
+  const int src = metropolis_src(lat, rng);
+  const int var = sweep_variant(lat, src, ml);
+  if (var == U1V_WAVE) return launch_wave(lat, links, rng, metrop, ovrn, meas_partials);
   const int D = lat->g.dims;
   const int total = 2 * D * (metrop + ovrn);
   int phase = 0;
@@ -699,13 +726,12 @@ static int issue_sweep(u1_lattice *lat, float2 *links, u1_rng *rng, int metrop, 
     ++phase;
     // the last pass is phases total-2D+1 .. total; its parity-1 half with mu >= 1 measures
     if (meas_partials && phase > total - 2 * D && a.p == 1 && a.mu >= 1)
-      return D == 2 ? launch_meas_phase<2>(a, lat->stream, met, meas_partials)
-           : D == 3 ? launch_meas_phase<3>(a, lat->stream, met, meas_partials)
-                    : launch_meas_phase<4>(a, lat->stream, met, meas_partials);
-    const int var = effective_variant(lat);
-    return D == 2 ? launch_phase<2>(a, lat->stream, met, met && replay, var)
-         : D == 3 ? launch_phase<3>(a, lat->stream, met, met && replay, var)
-                  : launch_phase<4>(a, lat->stream, met, met && replay, var);
+      return D == 2 ? launch_meas_phase<2>(a, lat->stream, met, src == SRC_WINDOW, meas_partials)
+           : D == 3 ? launch_meas_phase<3>(a, lat->stream, met, src == SRC_WINDOW, meas_partials)
+                    : launch_meas_phase<4>(a, lat->stream, met, src == SRC_WINDOW, meas_partials);
+    return D == 2 ? launch_phase<2>(a, lat->stream, met, src, var)
+         : D == 3 ? launch_phase<3>(a, lat->stream, met, src, var)
+                  : launch_phase<4>(a, lat->stream, met, src, var);
   };
   for (int m = 0; m < metrop; ++m)
     for (int p = 0; p < 2; ++p)
@@ -918,6 +944,26 @@ extern "C" int u1_lattice_get_variant(const u1_lattice *lat, int *variant) {
   return U1_OK;
 }
 
+extern "C" int u1_lattice_set_metropolis(u1_lattice *lat, double delta, int nhits) {
+  if (!lat) return fail(U1_ERR_INVALID, "u1_lattice_set_metropolis: null lattice");
+  if (!(delta >= 0.0 && delta <= M_PI))
+    return fail(U1_ERR_INVALID, "u1_lattice_set_metropolis: delta must lie in [0, pi]");
+  if (nhits < 1 || nhits > U1_MAX_HITS)
+    return fail(U1_ERR_INVALID, "u1_lattice_set_metropolis: nhits must lie in [1, 127]");
+  lat->delta = delta;
+  lat->win = (float)(delta / M_PI);
+  lat->nhits = nhits;
+  drop_graphs(lat);
+  return U1_OK;
+}
+
+extern "C" int u1_lattice_get_metropolis(const u1_lattice *lat, double *delta, int *nhits) {
+  if (!lat || !delta || !nhits) return fail(U1_ERR_INVALID, "u1_lattice_get_metropolis: null argument");
+  *delta = lat->delta;
+  *nhits = lat->nhits;
+  return U1_OK;
+}
+
 static int update_impl(u1_lattice *lat, u1_rng *rng, int metrop, int ovrn, double *meas_partials) {
   U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
   int rc = check_replay(lat, rng, metrop);
@@ -927,7 +973,7 @@ static int update_impl(u1_lattice *lat, u1_rng *rng, int metrop, int ovrn, doubl
     rc = tune_update(lat, rng, true);
     if (rc) return rc;
   }
-  if (lat->use_graphs && !replay && effective_variant(lat) != U1V_WAVE) {
+  if (lat->use_graphs && !replay && sweep_variant(lat, metropolis_src(lat, rng), 0) != U1V_WAVE) {
     // graph key: passes, rng object, seed/chain and whether the last pass measures
     auto key = std::make_tuple(metrop * 2 + (meas_partials ? 1 : 0), ovrn, rng->id,
                                rng->seed ^ ((uint64_t)rng->chain << 48));
@@ -972,10 +1018,11 @@ extern "C" int u1_update_measure(u1_lattice *lat, u1_rng *rng, int metrop, int o
   if (rc) return rc;
   rc = update_impl(lat, rng, metrop, ovrn, lat->partials);
   if (rc) return rc;
+  const int var = sweep_variant(lat, metropolis_src(lat, rng), 0);
   switch (lat->g.dims) {
-    case 2: return launch_poly_finish<2>(lat, dev_out);
-    case 3: return launch_poly_finish<3>(lat, dev_out);
-    default: return launch_poly_finish<4>(lat, dev_out);
+    case 2: return launch_poly_finish<2>(lat, var, dev_out);
+    case 3: return launch_poly_finish<3>(lat, var, dev_out);
+    default: return launch_poly_finish<4>(lat, var, dev_out);
   }
 }
 
@@ -1003,11 +1050,13 @@ extern "C" int u1_update_phase(u1_lattice *lat, u1_rng *rng, int metropolis, int
   a.hit = hit;
   a.replay = rng->replay_dev;
   a.replay_base = rng->replay_base;
-  const int var = effective_variant(lat);
+  set_proposal(a, lat);
+  const int src = metropolis_src(lat, rng);
+  const int var = sweep_variant(lat, src, 0);
   switch (lat->g.dims) {
-    case 2: return launch_phase<2>(a, lat->stream, met, replay, var);
-    case 3: return launch_phase<3>(a, lat->stream, met, replay, var);
-    default: return launch_phase<4>(a, lat->stream, met, replay, var);
+    case 2: return launch_phase<2>(a, lat->stream, met, src, var);
+    case 3: return launch_phase<3>(a, lat->stream, met, src, var);
+    default: return launch_phase<4>(a, lat->stream, met, src, var);
   }
 }
 

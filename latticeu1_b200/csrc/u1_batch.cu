@@ -82,9 +82,9 @@ __global__ void __launch_bounds__(256, 8)
   a.bump_by = ph.bump_by;
   const int local = blk - (PAIR ? sch.first_pair : sch.first_site);
   if (PAIR)
-    update_pair_body<D, MU, MET, false>(a, 2 * (local * blockDim.x + threadIdx.x));
+    update_pair_body<D, MU, MET, SRC_PHILOX>(a, 2 * (local * blockDim.x + threadIdx.x));
   else
-    update_single_body<D, MU, MET, false>(a, local * blockDim.x + threadIdx.x);
+    update_single_body<D, MU, MET, SRC_PHILOX>(a, local * blockDim.x + threadIdx.x);
 }
 
 template <int D>

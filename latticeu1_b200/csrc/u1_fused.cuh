@@ -17,21 +17,21 @@
 
 namespace u1b {
 
-template <int D, int MU, bool MET>
+template <int D, int MU, bool MET, int SRC = SRC_PHILOX>
 static __global__ void __launch_bounds__(256, 8) k_update_pair_meas(const UpdArgs a, double *partials) {
   __shared__ double smem[kRedWarps * 2];
   float2 m = make_float2(0.f, 0.f);
-  update_pair_body<D, MU, MET, false, true>(a, 2 * (blockIdx.x * blockDim.x + threadIdx.x), &m);
+  update_pair_body<D, MU, MET, SRC, true>(a, 2 * (blockIdx.x * blockDim.x + threadIdx.x), &m);
   double v[2] = {(double)m.x, (double)m.y};
   block_sum<2>(v, smem);
   if (threadIdx.x < 2) partials[2 * blockIdx.x + threadIdx.x] = v[0];
 }
 
-template <int D, int MU, bool MET>
+template <int D, int MU, bool MET, int SRC = SRC_PHILOX>
 static __global__ void __launch_bounds__(256) k_update_meas(const UpdArgs a, double *partials) {
   __shared__ double smem[kRedWarps * 2];
   float2 m = make_float2(0.f, 0.f);
-  update_single_body<D, MU, MET, false, true>(a, blockIdx.x * blockDim.x + threadIdx.x, &m);
+  update_single_body<D, MU, MET, SRC, true>(a, blockIdx.x * blockDim.x + threadIdx.x, &m);
   double v[2] = {(double)m.x, (double)m.y};
   block_sum<2>(v, smem);
   if (threadIdx.x < 2) partials[2 * blockIdx.x + threadIdx.x] = v[0];

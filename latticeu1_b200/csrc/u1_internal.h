@@ -53,6 +53,11 @@ struct u1_lattice {
   std::map<std::tuple<int, int, uint64_t, uint64_t>, cudaGraphExec_t> graphs;
   bool use_graphs = true;
   int variant = U1V_AUTO;          // update kernel variant (U1V_AUTO: tune on first update)
+  // Metropolis proposal: half-width delta (0: the reference's whole-circle
+  // theta' = 2 pi u), win = delta/pi as used by the kernels, hits per link
+  double delta = 0.0;
+  float win = 0.f;
+  int nhits = 1;
   float2 *backup = nullptr;        // link backup used while tuning
   // persistent sweep (U1V_WAVE): per-tile phase flags, then ticket and error word
   unsigned int *wave_state = nullptr;

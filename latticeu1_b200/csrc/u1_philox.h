@@ -78,7 +78,9 @@ enum : uint32_t {
   U1_TAG_METROPOLIS = 0u,
   U1_TAG_HOTSTART = 1u,
   U1_TAG_FLOW = 2u,
+  U1_TAG_HIT = 0x80u,  // multi-hit Metropolis: hit h >= 1 uses tag U1_TAG_HIT | h
 };
+enum : int { U1_MAX_HITS = 127 };
 
 U1_HD uint32_t u1_rng_word1(int mu, uint32_t tag, uint32_t chain) {
   return (uint32_t)mu | (tag << 8) | (chain << 16);
@@ -93,6 +95,14 @@ U1_HD Philox4 u1_metropolis_block(uint32_t s, int mu, uint32_t chain, unsigned l
                                   uint32_t key1) {
   return philox4x32_10(s >> 1, u1_rng_word1(mu, U1_TAG_METROPOLIS, chain), (uint32_t)pass, (uint32_t)(pass >> 32),
                        key0, key1);
+}
+// The block of hit h (0 <= h <= U1_MAX_HITS - 1) of a multi-hit Metropolis
+// pass: hit 0 is u1_metropolis_block itself, hit h >= 1 replaces the tag by
+// U1_TAG_HIT | h.  Sites 2k and 2k+1 share each block as above.
+U1_HD Philox4 u1_metropolis_block_hit(uint32_t s, int mu, uint32_t chain, unsigned long long pass, int h,
+                                      uint32_t key0, uint32_t key1) {
+  const uint32_t tag = h ? (U1_TAG_HIT | (uint32_t)h) : U1_TAG_METROPOLIS;
+  return philox4x32_10(s >> 1, u1_rng_word1(mu, tag, chain), (uint32_t)pass, (uint32_t)(pass >> 32), key0, key1);
 }
 U1_HD void u1_metropolis_draws(const Philox4 &r, uint32_t s, float &u1, float &b) {
   u1 = u1_uniform_open((s & 1u) ? r.v[2] : r.v[0]);

@@ -104,6 +104,15 @@ struct UpdArgs {
   unsigned long long *bump_ptr;        // OR kernels: *bump_ptr += bump_by (block 0)
   unsigned int bump_by;
   int ml;                              // multilevel freeze period (0 = none)
+  float win;                           // SRC_WINDOW: proposal half-width / pi (0: whole circle)
+  int nhits;                           // SRC_WINDOW: Metropolis hits per link and pass
+};
+
+// Where a Metropolis kernel takes its proposals from.
+enum : int {
+  SRC_PHILOX = 0,  // theta' = 2 pi u on the whole circle, one hit (the reference's proposal)
+  SRC_REPLAY = 1,  // recorded (theta', b) pairs (test mode)
+  SRC_WINDOW = 2,  // multi-hit, theta' = theta + pi win (2u - 1) (whole circle when win = 0)
 };
 
 // Staple of link (x, MU) from precomputed EO steps (eo_steps): all six
@@ -150,14 +159,48 @@ __device__ __forceinline__ float2 staple_steps(const float2 *__restrict__ lat, c
 // overrelaxation) given its staple S and current value U.
 // blk: the site's Philox block when the caller already drew it (two-site
 // bodies draw once for both sites), else nullptr.
-template <int D, int MU, bool MET, bool REPLAY>
+// Multi-hit Metropolis of one link (no reference counterpart: the reference
+// makes one whole-circle proposal per pass).  The staple S is fixed while
+// hit h = 0 .. nhits-1 draws (u, b) from block u1_metropolis_block_hit(h),
+// proposes U' = U e^{i pi win (2u - 1)} (a window of half-width pi win
+// around the current angle; U' = e^{2 pi i u} when win = 0) and accepts it
+// when exp(beta Re(S (U' - U))) > b.  A windowed result is renormalised.
+// With win = 0 and one hit this is the SRC_PHILOX update bit for bit.
+template <int MU>
+__device__ __forceinline__ float2 metropolis_hits(const UpdArgs &a, uint32_t s, unsigned long long pass, float2 S,
+                                                  float2 U, const Philox4 *blk0) {
+  float2 cur = U;
+  for (int h = 0; h < a.nhits; ++h) {
+    const Philox4 r = (h == 0 && blk0) ? *blk0 : u1_metropolis_block_hit(s, MU, a.chain, pass, h, a.key0, a.key1);
+    float u1, b, sn, cs;
+    u1_metropolis_draws(r, s, u1, b);
+    float2 Un;
+    if (a.win == 0.f) {
+      sincospif(2.0f * u1, &sn, &cs);
+      Un = make_float2(cs, sn);
+    } else {
+      sincospif(a.win * (2.0f * u1 - 1.0f), &sn, &cs);
+      Un = cmul(cur, make_float2(cs, sn));
+    }
+    const float dS = a.c.beta * (cre_mul(S, Un) - cre_mul(S, cur));
+    if (expf(dS) > b) cur = Un;
+  }
+  if (a.win != 0.f) {
+    const float r = rsqrtf(fmaf(cur.x, cur.x, cur.y * cur.y));
+    cur = make_float2(cur.x * r, cur.y * r);
+  }
+  return cur;
+}
+
+template <int D, int MU, bool MET, int SRC>
 __device__ __forceinline__ float2 update_one(const UpdArgs &a, int i, float2 S, float2 U,
                                              const Philox4 *blk = nullptr) {
   if (MET) {
     const unsigned long long pass = *a.pass_dev + (unsigned long long)a.hit;
+    if (SRC == SRC_WINDOW) return metropolis_hits<MU>(a, (uint32_t)(a.p * a.g.Vh + i), pass, S, U, blk);
     float2 Un;
     float b;
-    if (REPLAY) {
+    if (SRC == SRC_REPLAY) {
       const size_t pr = ((((size_t)(pass - a.replay_base) * 2 + a.p) * D + MU) * a.g.Vh + i) * 2;
       double sn, cs;
       sincos(a.replay[pr], &sn, &cs);
@@ -204,7 +247,7 @@ __device__ __forceinline__ void phase_entry(const UpdArgs &a) {
 // mA = sum_{nu<MU} (upper + lower), mD = sum_{nu<MU} (upper - lower).
 // Phases (1, MU), MU = 1..D-1, of the last pass therefore count every
 // plaquette of the final configuration once, from values already loaded.
-template <int D, int MU, bool MET, bool REPLAY, bool MEAS = false>
+template <int D, int MU, bool MET, int SRC, bool MEAS = false>
 __device__ __forceinline__ void update_single_body(const UpdArgs a, int i, float2 *meas = nullptr) {
   int x[4], k;
   eo_decode_fast<D>(a.g, i, a.p, x, k);
@@ -219,7 +262,7 @@ __device__ __forceinline__ void update_single_body(const UpdArgs a, int i, float
   float2 *own = a.lat + MU * a.g.V + a.p * a.g.Vh + i;
   float2 mA = make_float2(0.f, 0.f), mD = mA;
   const float2 S = staple_steps<D, MU, MEAS>(a.lat, a.g, a.c, i, a.p, fwd, bwd, &mA, &mD);
-  const float2 N = update_one<D, MU, MET, REPLAY>(a, i, S, *own);
+  const float2 N = update_one<D, MU, MET, SRC>(a, i, S, *own);
   *own = N;
   pdl_release_dependents();
   if (MEAS) *meas = make_float2(2.f * MU - cre_mul(mA, N), cim_mul(mD, N));
@@ -263,7 +306,7 @@ __device__ __forceinline__ void staple_term2(const Pair2 &a, const Pair2 &b, con
 // single-lattice and batched kernels.
 // Every variant forms the staple and the update with the same operations in
 // the same order, so all of them give bit-identical links.
-template <int D, int MU, bool MET, bool REPLAY, bool MEAS = false, bool COH = false>
+template <int D, int MU, bool MET, int SRC, bool MEAS = false, bool COH = false>
 __device__ __forceinline__ void update_pair_body(const UpdArgs a, int i, float2 *meas = nullptr) {
   int x[4], k;
   eo_decode_fast<D>(a.g, i, a.p, x, k);
@@ -337,11 +380,11 @@ __device__ __forceinline__ void update_pair_body(const UpdArgs a, int i, float2 
   const float4 U = *own;
   // sites i, i+1 (i even, V/2 even) share one Philox block
   Philox4 blk;
-  if (MET && !REPLAY)
+  if (MET && SRC != SRC_REPLAY)
     blk = u1_metropolis_block((uint32_t)(a.p * Vh + i), MU, a.chain, *a.pass_dev + (unsigned long long)a.hit,
                               a.key0, a.key1);
-  const float2 N0 = update_one<D, MU, MET, REPLAY>(a, i, S0, make_float2(U.x, U.y), &blk);
-  const float2 N1 = update_one<D, MU, MET, REPLAY>(a, i + 1, S1, make_float2(U.z, U.w), &blk);
+  const float2 N0 = update_one<D, MU, MET, SRC>(a, i, S0, make_float2(U.x, U.y), &blk);
+  const float2 N1 = update_one<D, MU, MET, SRC>(a, i + 1, S1, make_float2(U.z, U.w), &blk);
   *own = make_float4(N0.x, N0.y, N1.x, N1.y);
   pdl_release_dependents();
   if (MEAS) {
@@ -353,21 +396,21 @@ __device__ __forceinline__ void update_pair_body(const UpdArgs a, int i, float2 
 
 // Two sites per thread, register budget capped at 32 so 8 CTAs of 256
 // threads fit an SM (a 32^4 phase is then a single wave).
-template <int D, int MU, bool MET, bool REPLAY>
+template <int D, int MU, bool MET, int SRC>
 __global__ void __launch_bounds__(256, 8) k_update_pair(const UpdArgs a) {
-  update_pair_body<D, MU, MET, REPLAY>(a, 2 * (blockIdx.x * blockDim.x + threadIdx.x));
+  update_pair_body<D, MU, MET, SRC>(a, 2 * (blockIdx.x * blockDim.x + threadIdx.x));
 }
 
 // The same with no register cap (fewer CTAs per SM, no spills).
-template <int D, int MU, bool MET, bool REPLAY>
+template <int D, int MU, bool MET, int SRC>
 __global__ void __launch_bounds__(256) k_update_pair_free(const UpdArgs a) {
-  update_pair_body<D, MU, MET, REPLAY>(a, 2 * (blockIdx.x * blockDim.x + threadIdx.x));
+  update_pair_body<D, MU, MET, SRC>(a, 2 * (blockIdx.x * blockDim.x + threadIdx.x));
 }
 
 // One site per thread (any geometry, N0/2 odd included).
-template <int D, int MU, bool MET, bool REPLAY>
+template <int D, int MU, bool MET, int SRC>
 __global__ void __launch_bounds__(256) k_update(const UpdArgs a) {
-  update_single_body<D, MU, MET, REPLAY>(a, blockIdx.x * blockDim.x + threadIdx.x);
+  update_single_body<D, MU, MET, SRC>(a, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // Hot start (reference src/update.cu:30-48): every link gets

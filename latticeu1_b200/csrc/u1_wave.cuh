@@ -57,12 +57,12 @@ __device__ __forceinline__ void wave_phase(const UpdArgs &a, int i, double *slot
   if (MEAS) {
     __shared__ double smem[kRedWarps * 2];
     float2 m = make_float2(0.f, 0.f);
-    update_pair_body<D, MU, MET, false, true, true>(a, i, &m);
+    update_pair_body<D, MU, MET, SRC_PHILOX, true, true>(a, i, &m);
     double v[2] = {(double)m.x, (double)m.y};
     block_sum<2>(v, smem);
     if (threadIdx.x < 2) slot[2 * blockIdx.x + threadIdx.x] = v[0];
   } else {
-    update_pair_body<D, MU, MET, false, false, true>(a, i);
+    update_pair_body<D, MU, MET, SRC_PHILOX, false, true>(a, i);
   }
 }
 

@@ -162,6 +162,19 @@ class Lattice:
     def set_variant(self, variant: int) -> None:
         check(lib.u1_lattice_set_variant(self._h, int(variant)), "u1_lattice_set_variant")
 
+    def set_metropolis(self, delta: float = 0.0, nhits: int = 1) -> None:
+        """Metropolis proposal: nhits hits per link and pass, each proposing
+        theta' = theta + delta (2u - 1), or theta' = 2 pi u for delta = 0
+        (the reference's proposal, the default with nhits = 1)."""
+        check(lib.u1_lattice_set_metropolis(self._h, float(delta), int(nhits)), "u1_lattice_set_metropolis")
+
+    @property
+    def metropolis(self) -> tuple:
+        """(delta, nhits) of the Metropolis proposal."""
+        d, n = C.c_double(), C.c_int()
+        check(lib.u1_lattice_get_metropolis(self._h, C.byref(d), C.byref(n)), "u1_lattice_get_metropolis")
+        return float(d.value), int(n.value)
+
     def tune(self, rng: "Rng") -> int:
         v = C.c_int()
         check(lib.u1_tune(self._h, rng.handle, C.byref(v)), "u1_tune")

@@ -66,6 +66,10 @@ class Oracle:
                                              C.POINTER(C.c_float)]),
                 "o_philox": (None, [C.c_uint32] * 6 + [C.POINTER(C.c_uint32)]),
                 "o_overrelax": (None, [g, _dp, C.c_int]),
+                "o_metropolis_hits": (C.c_long, [g, _dp, C.c_uint64, C.c_uint32, C.c_uint64, C.c_double, C.c_int,
+                                                 C.c_int]),
+                "o_phase_hits": (None, [g, _dp, C.c_int, C.c_int, C.c_uint64, C.c_uint32, C.c_uint64, C.c_double,
+                                        C.c_int, _dp, _dp]),
                 "o_phase": (None, [g, _dp, C.c_int, C.c_int, C.c_int, _dp, C.c_uint64, C.c_uint32, C.c_uint64,
                                    C.c_int, _dp, _dp]),
                 "o_hot_start_philox": (None, [g, _dp, C.c_uint64, C.c_uint32, C.c_uint64]),
@@ -138,6 +142,12 @@ class Oracle:
     def metropolis_philox(self, lat, seed, pass_, chain=0, ml=0) -> int:
         return int(self.lib().o_metropolis_philox(self._g(), _arr(lat), seed, chain, pass_, ml))
 
+    def metropolis_hits(self, lat, seed, pass_, delta, nhits, chain=0, ml=0) -> int:
+        """One multi-hit windowed Metropolis pass (theta' = theta + delta (2u-1),
+        theta' = 2 pi u for delta = 0); returns the number of links moved."""
+        return int(self.lib().o_metropolis_hits(self._g(), _arr(lat), seed, chain, pass_, float(delta), int(nhits),
+                                                ml))
+
     def philox_uniforms(self, seed, pass_, parity, mu, chain=0) -> np.ndarray:
         out = np.empty((self.Vh, 2), dtype=np.float32)
         f = (C.c_float * 2)()
@@ -153,11 +163,19 @@ class Oracle:
         return [int(v) for v in out]
 
     def phase(self, lat, met: bool, parity: int, mu: int, pairs=None, seed: int = 0, pass_: int = 0,
-              chain: int = 0, ml: int = 0):
+              chain: int = 0, ml: int = 0, delta: float = 0.0, nhits: int = 1):
         """One (parity, mu) phase in place; returns (|S| per site, Metropolis
-        relative margin 1 - b/exp(dS) per site)."""
+        relative margin 1 - b/exp(dS) per site; with several hits, that of
+        the hit closest to its decision).  delta, nhits: the windowed
+        multi-hit proposal (defaults: the reference's single whole-circle
+        proposal)."""
         smag = np.zeros(self.Vh)
         margin = np.zeros(self.Vh)
+        if met and pairs is None and (delta != 0.0 or nhits != 1):
+            assert ml == 0
+            self.lib().o_phase_hits(self._g(), _arr(lat), parity, mu, seed, chain, pass_, float(delta), int(nhits),
+                                    _arr(smag), _arr(margin))
+            return smag, margin
         pp = None
         if pairs is not None:
             pairs = np.ascontiguousarray(pairs, dtype=np.float64).reshape(-1)
@@ -182,10 +200,13 @@ class Oracle:
         self.lib().o_hot_start_philox(self._g(), _arr(lat), seed, chain, pass_)
         return lat
 
-    def update_philox(self, lat, seed, pass_, metrop, ovrn, chain=0) -> int:
+    def update_philox(self, lat, seed, pass_, metrop, ovrn, chain=0, delta=0.0, nhits=1) -> int:
         """metrop Philox Metropolis passes then ovrn OR passes; returns next pass."""
         for m in range(metrop):
-            self.metropolis_philox(lat, seed, pass_ + m, chain)
+            if delta != 0.0 or nhits != 1:
+                self.metropolis_hits(lat, seed, pass_ + m, delta, nhits, chain)
+            else:
+                self.metropolis_philox(lat, seed, pass_ + m, chain)
         for _ in range(ovrn):
             self.overrelax(lat)
         return pass_ + metrop

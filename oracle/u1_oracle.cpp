@@ -252,6 +252,73 @@ void o_phase(const OGeom *g, double *lat, int met, int p, int mu, const double *
   }
 }
 
+// Multi-hit Metropolis with a proposal window, the library's
+// u1_lattice_set_metropolis(delta, nhits) (no reference counterpart: the
+// reference makes one whole-circle proposal, src/update.cu:181-182).  The
+// staple S of the link is fixed; hit h draws (u, b) from the Philox block of
+// tag 0 (h = 0) or 0x80 | h (u1_metropolis_block_hit), proposes
+// theta' = theta + delta (2u - 1) (theta' = 2 pi u when delta = 0) and
+// accepts when exp(beta Re(S (e^{i theta'} - e^{i theta}))) > b, the test of
+// include/lattice_functions.h:68-80.  *margin gets the relative decision
+// margin 1 - b/exp(dS) of the hit closest to its decision boundary.
+static double hits_link(const OGeom *g, double theta, const double S[2], uint64_t seed, uint32_t chain,
+                        uint64_t pass, int p, int mu, int id, double delta, int nhits, double *margin) {
+  const uint32_t s = (uint32_t)(p * g->Vh + id);
+  double best = HUGE_VAL;
+  for (int h = 0; h < nhits; ++h) {
+    const u1b::Philox4 r =
+        u1b::u1_metropolis_block_hit(s, mu, chain, pass, h, (uint32_t)seed, (uint32_t)(seed >> 32));
+    float u[2];
+    u1b::u1_metropolis_draws(r, s, u[0], u[1]);
+    const double th_new = delta == 0.0 ? 2.0 * M_PI * (double)u[0]
+                                       : std::fmod(theta + delta * (2.0 * (double)u[0] - 1.0) + 2.0 * M_PI,
+                                                   2.0 * M_PI);
+    const double dS = g->beta * (S[0] * (std::cos(th_new) - std::cos(theta)) -
+                                 S[1] * (std::sin(th_new) - std::sin(theta)));
+    const double e = std::exp(dS);
+    const double m = 1.0 - (double)u[1] / e;
+    if (std::fabs(m) < std::fabs(best)) best = m;
+    if (e > (double)u[1]) theta = th_new;
+  }
+  if (margin) *margin = best;
+  return theta;
+}
+
+// One multi-hit windowed Metropolis pass (see hits_link), optional multilevel
+// freeze period ml.  Returns the number of links whose angle changed.
+long o_metropolis_hits(const OGeom *g, double *lat, uint64_t seed, uint32_t chain, uint64_t pass, double delta,
+                       int nhits, int ml) {
+  long moved = 0;
+  for (int p = 0; p < 2; ++p)
+    for (int mu = 0; mu < g->dims; ++mu) {
+#pragma omp parallel for reduction(+ : moved) schedule(static)
+      for (int id = 0; id < (int)g->Vh; ++id) {
+        if (frozen(g, id, p, mu, ml)) continue;
+        const long pos = id + p * g->Vh + mu * g->V;
+        double S[2];
+        o_staple(g, lat, id, p, mu, S);
+        const double th = hits_link(g, lat[pos], S, seed, chain, pass, p, mu, id, delta, nhits, nullptr);
+        moved += th != lat[pos];
+        lat[pos] = th;
+      }
+    }
+  return moved;
+}
+
+// One (parity, mu) phase of a multi-hit windowed Metropolis pass, recording
+// |S| and the decision margin of the closest hit per site (as o_phase).
+void o_phase_hits(const OGeom *g, double *lat, int p, int mu, uint64_t seed, uint32_t chain, uint64_t pass,
+                  double delta, int nhits, double *smag, double *margin) {
+#pragma omp parallel for schedule(static)
+  for (int id = 0; id < (int)g->Vh; ++id) {
+    const long pos = id + p * g->Vh + mu * g->V;
+    double S[2];
+    o_staple(g, lat, id, p, mu, S);
+    smag[id] = std::sqrt(S[0] * S[0] + S[1] * S[1]);
+    lat[pos] = hits_link(g, lat[pos], S, seed, chain, pass, p, mu, id, delta, nhits, &margin[id]);
+  }
+}
+
 // One overrelaxation pass (reference src/update.cu:84-98,
 // include/lattice_functions.h:83-89), optional freeze period ml.
 void o_overrelax(const OGeom *g, double *lat, int ml) {

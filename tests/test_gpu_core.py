@@ -38,7 +38,7 @@ def test_import_export_roundtrip(ctx):
     assert back.min() >= 0.0 and back.max() < 2 * np.pi + 1e-12
 
 
-def check_phase(lat, o, rng, met, p, mu, pairs=None, seed=0, pass_=0, hit=0):
+def check_phase(lat, o, rng, met, p, mu, pairs=None, seed=0, pass_=0, hit=0, delta=0.0, nhits=1):
     """Run one (parity, mu) phase on the GPU and in the FP64 oracle from the
     same configuration and compare link by link.
 
@@ -50,10 +50,12 @@ def check_phase(lat, o, rng, met, p, mu, pairs=None, seed=0, pass_=0, hit=0):
     * Metropolis: accepted/rejected links agree to 1e-6 rad, except accept
       flips whose FP64 decision margin |1 - b/exp(dS)| is within the FP32
       error of beta*dS.
+    delta, nhits: the windowed multi-hit proposal (the margin is that of the
+    hit closest to its decision).
     Returns (number of flips, |dtheta| of the non-flipped links)."""
     th = lat.export_angles()
     ref = th.copy()
-    smag, margin = o.phase(ref, met, p, mu, pairs=pairs, seed=seed, pass_=pass_)
+    smag, margin = o.phase(ref, met, p, mu, pairs=pairs, seed=seed, pass_=pass_, delta=delta, nhits=nhits)
     lat.update_phase(rng, met, p, mu, hit)
     got = lat.export_angles()
     lo = mu * lat.V + p * lat.Vh
