@@ -121,6 +121,18 @@ int u1_lattice_copy(u1_lattice *dst, const u1_lattice *src);
  * on_device != 0: the pointer is a device pointer on the lattice's device. */
 int u1_lattice_import_angles(u1_lattice *lat, const double *angles, int on_device);
 int u1_lattice_export_angles(const u1_lattice *lat, double *angles, int on_device);
+/* Asynchronous forms (no counterpart in the reference, whose Array<double>
+ * stays on the device): queued on the lattice's stream behind the work
+ * already there, they return at once.  A host buffer should be page-locked
+ * (cudaHostAlloc / cudaHostRegister) and left alone until the stream has
+ * passed the copy; a pageable one still works, but then the copy blocks the
+ * host.  Lattices on separate streams so overlap one lattice's host-to-device
+ * copy with another's device-to-host copy and sweeps.  A failed wait of the
+ * persistent variant 4 is reported by the next synchronous call. */
+int u1_lattice_import_angles_async(u1_lattice *lat, const double *angles, int on_device);
+int u1_lattice_export_angles_async(const u1_lattice *lat, double *angles, int on_device);
+/* Wait for everything queued on the lattice's stream. */
+int u1_lattice_synchronize(u1_lattice *lat);
 /* Cold start: every theta = 0. */
 int u1_cold_start(u1_lattice *lat);
 

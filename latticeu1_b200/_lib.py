@@ -54,6 +54,9 @@ SIGNATURES = {
     "u1_lattice_copy": [_vp, _vp],
     "u1_lattice_import_angles": [_vp, _vp, _i],
     "u1_lattice_export_angles": [_vp, _vp, _i],
+    "u1_lattice_import_angles_async": [_vp, _vp, _i],
+    "u1_lattice_export_angles_async": [_vp, _vp, _i],
+    "u1_lattice_synchronize": [_vp],
     "u1_cold_start": [_vp],
     "u1_rng_create": [_vp, C.c_uint64, C.POINTER(_vp)],
     "u1_rng_destroy": [_vp],

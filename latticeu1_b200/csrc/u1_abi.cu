@@ -301,8 +301,9 @@ static int ensure_stage(u1_lattice *lat) {
   return U1_OK;
 }
 
-extern "C" int u1_lattice_import_angles(u1_lattice *lat, const double *angles, int on_device) {
-  if (!lat || !angles) return fail(U1_ERR_INVALID, "u1_lattice_import_angles: null argument");
+// Import (angles -> float2 links) queued on the lattice's stream; `wait`:
+// return only once it has completed.
+static int import_angles(u1_lattice *lat, const double *angles, int on_device, bool wait) {
   U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
   const size_t n = (size_t)lat->g.V * lat->g.dims;
   const double *src = angles;
@@ -314,17 +315,28 @@ extern "C" int u1_lattice_import_angles(u1_lattice *lat, const double *angles, i
   }
   k_import_angles<<<u1i::blocks_for((long long)n, 256), 256, 0, lat->stream>>>(lat->links, src, n);
   U1_LAUNCH_CHECK("k_import_angles");
-  U1_CUDA_TRY(cudaStreamSynchronize(lat->stream));
+  if (wait) U1_CUDA_TRY(cudaStreamSynchronize(lat->stream));
   return U1_OK;
+}
+
+extern "C" int u1_lattice_import_angles(u1_lattice *lat, const double *angles, int on_device) {
+  if (!lat || !angles) return fail(U1_ERR_INVALID, "u1_lattice_import_angles: null argument");
+  return import_angles(lat, angles, on_device, true);
+}
+
+extern "C" int u1_lattice_import_angles_async(u1_lattice *lat, const double *angles, int on_device) {
+  if (!lat || !angles) return fail(U1_ERR_INVALID, "u1_lattice_import_angles_async: null argument");
+  return import_angles(lat, angles, on_device, false);
 }
 
 static int wave_check(u1_lattice *lat);
 
-extern "C" int u1_lattice_export_angles(const u1_lattice *clat, double *angles, int on_device) {
-  if (!clat || !angles) return fail(U1_ERR_INVALID, "u1_lattice_export_angles: null argument");
-  u1_lattice *lat = const_cast<u1_lattice *>(clat);  // the staging buffer is a cache
+// Export (float2 links -> angles) queued on the lattice's stream; `wait`:
+// check the persistent sweep's error word first and return only once the
+// export has completed.
+static int export_angles(u1_lattice *lat, double *angles, int on_device, bool wait) {
   U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
-  {
+  if (wait) {
     int rc = wave_check(lat);
     if (rc) return rc;
   }
@@ -339,8 +351,25 @@ extern "C" int u1_lattice_export_angles(const u1_lattice *clat, double *angles, 
   U1_LAUNCH_CHECK("k_export_angles");
   if (!on_device)
     U1_CUDA_TRY(cudaMemcpyAsync(angles, lat->stage, n * sizeof(double), cudaMemcpyDeviceToHost, lat->stream));
-  U1_CUDA_TRY(cudaStreamSynchronize(lat->stream));
+  if (wait) U1_CUDA_TRY(cudaStreamSynchronize(lat->stream));
   return U1_OK;
+}
+
+extern "C" int u1_lattice_export_angles(const u1_lattice *clat, double *angles, int on_device) {
+  if (!clat || !angles) return fail(U1_ERR_INVALID, "u1_lattice_export_angles: null argument");
+  return export_angles(const_cast<u1_lattice *>(clat), angles, on_device, true);  // the staging buffer is a cache
+}
+
+extern "C" int u1_lattice_export_angles_async(const u1_lattice *clat, double *angles, int on_device) {
+  if (!clat || !angles) return fail(U1_ERR_INVALID, "u1_lattice_export_angles_async: null argument");
+  return export_angles(const_cast<u1_lattice *>(clat), angles, on_device, false);
+}
+
+extern "C" int u1_lattice_synchronize(u1_lattice *lat) {
+  if (!lat) return fail(U1_ERR_INVALID, "u1_lattice_synchronize: null lattice");
+  U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
+  U1_CUDA_TRY(cudaStreamSynchronize(lat->stream));
+  return wave_check(lat);
 }
 
 // ---------------------------------------------------------------- rng

@@ -218,6 +218,35 @@ class Lattice:
         check(lib.u1_lattice_export_angles(self._h, arr.ctypes.data_as(C.c_void_p), 0), "u1_lattice_export_angles")
         return arr
 
+    def _async_buffer(self, buf, what: str):
+        """(pointer, on_device) of a caller buffer used by an asynchronous
+        copy: no conversion or temporary copy is allowed, since the copy
+        reads or writes it after the call returns."""
+        if hasattr(buf, "is_cuda"):
+            if buf.dtype.__str__() != "torch.float64" or not buf.is_contiguous() or buf.numel() != self.nlinks:
+                raise ValueError(f"{what}: need a contiguous float64 tensor of {self.nlinks} angles")
+            return C.c_void_p(buf.data_ptr()), int(bool(buf.is_cuda))
+        if not isinstance(buf, np.ndarray) or buf.dtype != np.float64 or not buf.flags.c_contiguous \
+                or buf.size != self.nlinks:
+            raise ValueError(f"{what}: need a contiguous float64 array of {self.nlinks} angles")
+        return buf.ctypes.data_as(C.c_void_p), 0
+
+    def import_angles_async(self, theta) -> None:
+        """Queue an import on the lattice's stream and return at once.  theta
+        (CUDA float64 tensor, or host float64 array / tensor, pinned for an
+        asynchronous copy) must stay alive and unchanged until synchronize()."""
+        ptr, dev = self._async_buffer(theta, "import_angles_async")
+        check(lib.u1_lattice_import_angles_async(self._h, ptr, dev), "u1_lattice_import_angles_async")
+
+    def export_angles_async(self, out) -> None:
+        """Queue an export into `out` (as for import_angles_async); the
+        angles are there after synchronize()."""
+        ptr, dev = self._async_buffer(out, "export_angles_async")
+        check(lib.u1_lattice_export_angles_async(self._h, ptr, dev), "u1_lattice_export_angles_async")
+
+    def synchronize(self) -> None:
+        check(lib.u1_lattice_synchronize(self._h), "u1_lattice_synchronize")
+
     # -- Monte Carlo -----------------------------------------------------
     def cold_start(self) -> None:
         check(lib.u1_cold_start(self._h), "u1_cold_start")

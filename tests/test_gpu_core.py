@@ -400,6 +400,45 @@ def test_export_into_caller_buffers(ctx):
         lat.export_angles(np.zeros(lat.nlinks, dtype=np.float32))
 
 
+def test_async_import_export_matches_sync(ctx):
+    """Two chains stepped through the asynchronous import/export on their own
+    streams (pinned host buffers, one chain's copies overlapping the other's)
+    end bit-identical to the same chains stepped through the synchronous calls."""
+    import torch
+    geom = (4, (8, 6, 6, 8), 1.0)
+    th0 = [np.random.default_rng(k).uniform(0, 2 * np.pi, Lattice(ctx, *geom).nlinks) for k in range(2)]
+    pinned = [torch.from_numpy(t.copy()).pin_memory() for t in th0]
+    plain = [t.copy() for t in th0]
+    la = [Lattice(ctx, *geom) for _ in range(2)]
+    lb = [Lattice(ctx, *geom) for _ in range(2)]
+    streams = [torch.cuda.Stream() for _ in range(2)]
+    for x, s in zip(la, streams):
+        x.set_stream(s.cuda_stream)
+    ra = [Rng(ctx, 40 + k) for k in range(2)]
+    rb = [Rng(ctx, 40 + k) for k in range(2)]
+    for k in range(6):
+        c = k % 2
+        la[c].import_angles_async(pinned[c])
+        la[c].update(ra[c], 1, 2)
+        la[c].export_angles_async(pinned[c])
+        lb[c].import_angles(plain[c])
+        lb[c].update(rb[c], 1, 2)
+        lb[c].export_angles(plain[c])
+    for x in la:
+        x.synchronize()
+    for c in range(2):
+        np.testing.assert_array_equal(pinned[c].numpy(), plain[c])
+        assert not np.array_equal(plain[c], th0[c])
+    dev = torch.zeros(la[0].nlinks, dtype=torch.float64, device="cuda")
+    la[0].export_angles_async(dev)
+    la[0].synchronize()
+    np.testing.assert_array_equal(dev.cpu().numpy(), plain[0])
+    with pytest.raises(ValueError):
+        la[0].import_angles_async(np.zeros(la[0].nlinks, dtype=np.float32))
+    with pytest.raises(ValueError):
+        la[0].export_angles_async(torch.zeros(3, dtype=torch.float64))
+
+
 def test_multilevel_graphs_equal_direct(ctx):
     """Graph-replayed multilevel sub-updates give the direct launches' result bit for bit."""
     res = []
