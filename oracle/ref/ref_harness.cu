@@ -171,6 +171,30 @@ double ref_gpu_update(const double *lat_in, double *lat_out, int metrop, int ovr
   return (double)ms;
 }
 
+// A Markov chain of the reference's own CUDA code: from lat_in, nsweeps of
+// UpdateLattice(metrop, ovrn) with Plaquette and Polyakov after each, as the
+// reference driver's loop does; out[6 * sweep + k] = (SS re, im, ST re, im,
+// L re, im).
+void ref_gpu_chain(const double *lat_in, int metrop, int ovrn, int nsweeps, int seed, double *out) {
+  Array<double> *lat = upload(lat_in);
+  CudaRNG *rng = new CudaRNG(seed, HalfVolume());
+  for (int i = 0; i < nsweeps; ++i) {
+    UpdateLattice(lat, rng, metrop, ovrn);
+    complexd p[2];
+    Plaquette(lat, p, false);
+    complexd l = Polyakov(lat, false);
+    double *o = out + 6 * (size_t)i;
+    o[0] = p[0].real();
+    o[1] = p[0].imag();
+    o[2] = p[1].real();
+    o[3] = p[1].imag();
+    o[4] = l.real();
+    o[5] = l.imag();
+  }
+  delete rng;
+  delete lat;
+}
+
 void ref_gpu_measure(const double *lat_in, double out[6]) {
   Array<double> *lat = upload(lat_in);
   complexd p[2];

@@ -8,7 +8,7 @@ tune cache) and exits on CUDA errors, so every task runs in a fresh child:
 
     python -m oracle.ref_gpu <task> <in.npz> <out.npz>
 
-tasks: measure | or_pass | poly2 | multilevel | multilevel_timing | timing
+tasks: measure | or_pass | poly2 | multilevel | multilevel_timing | timing | chain
 """
 from __future__ import annotations
 
@@ -79,6 +79,12 @@ def _child(task: str, fin: str, fout: str) -> None:
         lib.ref_gpu_multilevel(lat.ctypes.data_as(_dp), *a, 1234, c.ctypes.data_as(_dp))
         out["s"] = np.array([time.perf_counter() - t0])
         out["c"] = c
+    elif task == "chain":
+        n = int(d["sweeps"])
+        o = np.zeros(6 * n)
+        lib.ref_gpu_chain(lat.ctypes.data_as(_dp), int(d["metrop"]), int(d["ovrn"]), n, int(d.get("seed", 1234)),
+                          o.ctypes.data_as(_dp))
+        out["obs"] = o.reshape(n, 6)
     elif task == "timing":
         warm, n = int(d["warmup"]), int(d["sweeps"])
         ms = lib.ref_gpu_update(lat.ctypes.data_as(_dp), None, int(d["metrop"]), int(d["ovrn"]), warm, n, 1234)
