@@ -131,6 +131,41 @@ def test_multilevel_vs_reference_cuda(ctx, ref_gpu):
     np.testing.assert_allclose(got, want, rtol=1e-4, atol=1e-6 * np.abs(want).max())
 
 
+def test_multilevel_statistics_vs_reference_cuda(ctx, ref_gpu):
+    """MultiLevel with updates (n4 = 4, k4 = 1, n2 = 10, k2 = 1, 1 Metropolis
+    + 2 OR per sub-update) on 10 configurations of one thermalised chain
+    (8^3 x 8, beta = 1.1), once by this library and once by the reference's
+    own CUDA MultiLevel from the same configuration: the mean C(r) over the
+    configurations agree within 4 combined errors (spread over the
+    configurations), r = 1..3, and both agree with the single-level multihit
+    estimator (Poly2) of the same configurations within its larger error."""
+    from latticeu1_b200 import Lattice, Rng
+    dims, N, beta = 4, (8, 8, 8, 8), 1.1
+    args = [4, 1, 10, 1, 1, 2]
+    lat = Lattice(ctx, dims, N, beta)
+    rng = Rng(ctx, 21)
+    lat.cold_start()
+    for _ in range(300):
+        lat.update(rng, 1, 4)
+    ours, ref, single = [], [], []
+    for k in range(10):
+        for _ in range(20):
+            lat.update(rng, 1, 4)
+        th = lat.export_angles()
+        ours.append(lat.multilevel(Rng(ctx, 500 + k), *args)[:3].real)
+        c = ref_gpu.run("multilevel", _inputs(dims, N, beta, 1.0, th, args=np.array(args)))["c"]
+        ref.append(c[0:6:2])
+        single.append(lat.poly_corr(True)[:3].real)
+    ours, ref, single = np.asarray(ours), np.asarray(ref), np.asarray(single)
+    n = len(ours)
+    mo, eo = ours.mean(0), ours.std(0, ddof=1) / np.sqrt(n)
+    mr, er = ref.mean(0), ref.std(0, ddof=1) / np.sqrt(n)
+    ms, es = single.mean(0), single.std(0, ddof=1) / np.sqrt(n)
+    assert np.all(mo > 0) and np.all(np.diff(mo) < 0), mo
+    assert np.all(np.abs(mo - mr) < 4 * np.hypot(eo, er)), (mo, eo, mr, er)
+    assert np.all(np.abs(mo - ms) < 4 * np.hypot(eo, es)), (mo, eo, ms, es)
+
+
 def test_throughput_vs_reference_cuda(ctx, ref_gpu):
     """UpdateLattice(1 Metropolis + 4 OR) at 32^4 on the same B200: the
     reference's CUDA build (FP64, after its own autotuning in the warm-up)
