@@ -141,6 +141,18 @@ def measured_peak() -> tuple[float, str]:
     return 6650.0, "fallback"
 
 
+def ncu_batch_traffic_per_link_sweep():
+    """DRAM bytes per link and sweep of the grouped batch from the committed
+    ncu summary, if any."""
+    p = ROOT / "profiles" / "k_batch_update_512chains.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("dram_bytes_per_link_sweep:"):
+            return float(line.split(":", 1)[1].split()[0])
+    return None
+
+
 def ncu_traffic_per_launch(N):
     """DRAM bytes per k_update launch from the committed ncu summary, if any."""
     p = ROOT / "profiles" / f"k_update_{geom_name(N).replace('^4', 'x4')}_traffic.txt"
@@ -512,6 +524,8 @@ def run_batched(args) -> None:
     alg_bytes = algorithmic_bytes_per_link_update(DIMS) * links // (2 * DIMS)
     achieved = alg_bytes / avg_launch_s / 1e9
     peak, peak_kind = measured_peak()
+    per_link = ncu_batch_traffic_per_link_sweep()
+    traffic = per_link * links / phases if per_link is not None else None
 
     # comparator: the same chains one at a time through the single-lattice API
     nseq = len(geoms)
@@ -554,7 +568,7 @@ def run_batched(args) -> None:
                    "l2": "flushed between timed steps (512 MiB device write)"},
         "roofline": {"bound": "hbm", "kernel": "k_batch_update (one (parity,mu) phase over all chains)",
                      "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "algorithmic_bytes_per_launch": alg_bytes,
+                     "frac": achieved / peak, "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes,
                      "avg_launch_us": avg_launch_s * 1e6},
         "update_only_ms_per_step": upd_ms / args.steps,
         "gpu_launches": int(launches),
