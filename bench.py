@@ -340,6 +340,7 @@ def run_ours(args) -> None:
         lc = Lattice(ctx, DIMS, N, beta, aniso)
         lc.set_metropolis(args.delta, args.nhits)
         lc.set_variant(lat.variant)
+        lc.set_block(lat.block)
         sc = torch.cuda.Stream()
         lc.set_stream(sc.cuda_stream)
         rc_ = Rng(ctx, 1234)
@@ -409,6 +410,7 @@ def run_ours(args) -> None:
                             "u1_lattice_synchronize of every chain"},
             "gpu_launches": int(launches),
             "update_variant": Lattice.VARIANTS.get(lat.variant, str(lat.variant)),
+            "update_block": lat.block,
             "clocks": clk,
             "wall_s_timed_region": t_wall,
             "update_ms_per_step": upd_ms / args.steps,

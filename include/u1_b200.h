@@ -106,12 +106,20 @@ int u1_lattice_get_variant(const u1_lattice *lat, int *variant);
 int u1_lattice_set_metropolis(u1_lattice *lat, double delta, int nhits);
 int u1_lattice_get_metropolis(const u1_lattice *lat, double *delta, int *nhits);
 /* Replaces the reference's autotuner (tuneLaunch, src/tune.cpp:306-416):
- * times every valid variant on a few sweeps of this lattice from a
- * backed-up state (links and rng pass restored afterwards), keeps the
- * fastest and caches it per (device, geometry); with U1_RESOURCE_PATH set
- * the cache persists in $U1_RESOURCE_PATH/u1b200_tunecache.tsv.
- * U1_TUNE=0 in the environment turns the automatic first-update tuning off. */
+ * times every valid variant 1-3 at 64, 128 and 256 threads per block on a
+ * few sweeps of this lattice from a backed-up state (links and rng pass
+ * restored afterwards), keeps the fastest pair and caches it per (device,
+ * geometry); with U1_RESOURCE_PATH set the cache persists in
+ * $U1_RESOURCE_PATH/u1b200_tunecache.tsv.  U1_TUNE=0 in the environment
+ * turns the automatic first-update tuning off.  *variant gets the variant;
+ * u1_lattice_get_block the block size. */
 int u1_tune(u1_lattice *lat, u1_rng *rng, int *variant);
+/* Threads per block of the phase kernels of variants 1-3 (32, 64, ..., 256;
+ * default 256; the reference's block.x, include/tune.h:143-260).  Every block
+ * size gives bit-identical links.  The measuring phases of a measured sweep
+ * and the persistent variant keep their own block sizes. */
+int u1_lattice_set_block(u1_lattice *lat, int threads);
+int u1_lattice_get_block(const u1_lattice *lat, int *threads);
 /* Device pointer of the float2 link array (V*dims float2). */
 int u1_lattice_links(u1_lattice *lat, void **dev_ptr);
 /* Copy all links of src into dst (same geometry). */

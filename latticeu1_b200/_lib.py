@@ -47,6 +47,8 @@ SIGNATURES = {
     "u1_lattice_set_graphs": [_vp, _i],
     "u1_lattice_set_variant": [_vp, _i],
     "u1_lattice_get_variant": [_vp, C.POINTER(_i)],
+    "u1_lattice_set_block": [_vp, _i],
+    "u1_lattice_get_block": [_vp, C.POINTER(_i)],
     "u1_lattice_set_metropolis": [_vp, C.c_double, _i],
     "u1_lattice_get_metropolis": [_vp, _dp, C.POINTER(_i)],
     "u1_tune": [_vp, _vp, C.POINTER(_i)],

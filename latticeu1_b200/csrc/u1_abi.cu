@@ -494,10 +494,11 @@ extern "C" int u1_hot_start(u1_lattice *lat, u1_rng *rng) {
 // may be scheduled before the previous kernel on the stream finishes and
 // waits for it in-kernel (griddepcontrol.wait) before reading links.
 template <class K>
-static int launch_pdl(K kernel, int blocks, cudaStream_t s, const UpdArgs &a, const char *what) {
+static int launch_pdl(K kernel, int blocks, cudaStream_t s, const UpdArgs &a, const char *what,
+                      int threads = 256) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)blocks);
-  cfg.blockDim = dim3(256);
+  cfg.blockDim = dim3((unsigned)threads);
   cfg.dynamicSmemBytes = 0;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
@@ -513,38 +514,42 @@ static int launch_pdl(K kernel, int blocks, cudaStream_t s, const UpdArgs &a, co
 
 // The phase kernel of the chosen variant; src: the Metropolis proposal
 // source (SRC_PHILOX, SRC_REPLAY or SRC_WINDOW; ignored for overrelaxation).
+// threads: block size (a multiple of 32 up to 256, the kernels' launch
+// bound); the kernels index sites from blockDim, so every block size gives
+// the same links.
 template <int D, int MU, int SRC>
-static int launch_variant(const UpdArgs &a, cudaStream_t s, bool met, int variant) {
+static int launch_variant(const UpdArgs &a, cudaStream_t s, bool met, int variant, int threads) {
   if (variant == U1V_PAIR32 || variant == U1V_PAIR) {
-    const int blocks = u1i::blocks_for(a.g.Vh / 2, 256);
+    const int blocks = u1i::blocks_for(a.g.Vh / 2, threads);
     if (variant == U1V_PAIR32)
-      return met ? launch_pdl(k_update_pair<D, MU, true, SRC>, blocks, s, a, "k_update_pair")
-                 : launch_pdl(k_update_pair<D, MU, false, SRC_PHILOX>, blocks, s, a, "k_update_pair");
-    return met ? launch_pdl(k_update_pair_free<D, MU, true, SRC>, blocks, s, a, "k_update_pair_free")
-               : launch_pdl(k_update_pair_free<D, MU, false, SRC_PHILOX>, blocks, s, a, "k_update_pair_free");
+      return met ? launch_pdl(k_update_pair<D, MU, true, SRC>, blocks, s, a, "k_update_pair", threads)
+                 : launch_pdl(k_update_pair<D, MU, false, SRC_PHILOX>, blocks, s, a, "k_update_pair", threads);
+    return met ? launch_pdl(k_update_pair_free<D, MU, true, SRC>, blocks, s, a, "k_update_pair_free", threads)
+               : launch_pdl(k_update_pair_free<D, MU, false, SRC_PHILOX>, blocks, s, a, "k_update_pair_free",
+                            threads);
   }
-  const int blocks = u1i::blocks_for(a.g.Vh, 256);
-  return met ? launch_pdl(k_update<D, MU, true, SRC>, blocks, s, a, "k_update")
-             : launch_pdl(k_update<D, MU, false, SRC_PHILOX>, blocks, s, a, "k_update");
+  const int blocks = u1i::blocks_for(a.g.Vh, threads);
+  return met ? launch_pdl(k_update<D, MU, true, SRC>, blocks, s, a, "k_update", threads)
+             : launch_pdl(k_update<D, MU, false, SRC_PHILOX>, blocks, s, a, "k_update", threads);
 }
 
 template <int D, int MU>
-static int launch_phase_mu(const UpdArgs &a, cudaStream_t s, bool met, int src, int variant) {
-  if (!met || src == SRC_PHILOX) return launch_variant<D, MU, SRC_PHILOX>(a, s, met, variant);
-  if (src == SRC_REPLAY) return launch_variant<D, MU, SRC_REPLAY>(a, s, met, variant);
-  return launch_variant<D, MU, SRC_WINDOW>(a, s, met, variant);
+static int launch_phase_mu(const UpdArgs &a, cudaStream_t s, bool met, int src, int variant, int threads) {
+  if (!met || src == SRC_PHILOX) return launch_variant<D, MU, SRC_PHILOX>(a, s, met, variant, threads);
+  if (src == SRC_REPLAY) return launch_variant<D, MU, SRC_REPLAY>(a, s, met, variant, threads);
+  return launch_variant<D, MU, SRC_WINDOW>(a, s, met, variant, threads);
 }
 
 template <int D>
-static int launch_phase(const UpdArgs &a, cudaStream_t s, bool met, int src, int variant) {
+static int launch_phase(const UpdArgs &a, cudaStream_t s, bool met, int src, int variant, int threads) {
   switch (a.mu) {
-    case 0: return launch_phase_mu<D, 0>(a, s, met, src, variant);
-    case 1: return launch_phase_mu<D, 1>(a, s, met, src, variant);
+    case 0: return launch_phase_mu<D, 0>(a, s, met, src, variant, threads);
+    case 1: return launch_phase_mu<D, 1>(a, s, met, src, variant, threads);
     case 2:
-      if constexpr (D > 2) return launch_phase_mu<D, 2>(a, s, met, src, variant);
+      if constexpr (D > 2) return launch_phase_mu<D, 2>(a, s, met, src, variant, threads);
       break;
     case 3:
-      if constexpr (D > 3) return launch_phase_mu<D, 3>(a, s, met, src, variant);
+      if constexpr (D > 3) return launch_phase_mu<D, 3>(a, s, met, src, variant, threads);
       break;
   }
   return fail(U1_ERR_INVALID, "k_update: direction out of range");
@@ -758,9 +763,9 @@ static int issue_sweep(u1_lattice *lat, float2 *links, u1_rng *rng, int metrop, 
       return D == 2 ? launch_meas_phase<2>(a, lat->stream, met, src == SRC_WINDOW, meas_partials)
            : D == 3 ? launch_meas_phase<3>(a, lat->stream, met, src == SRC_WINDOW, meas_partials)
                     : launch_meas_phase<4>(a, lat->stream, met, src == SRC_WINDOW, meas_partials);
-    return D == 2 ? launch_phase<2>(a, lat->stream, met, src, var)
-         : D == 3 ? launch_phase<3>(a, lat->stream, met, src, var)
-                  : launch_phase<4>(a, lat->stream, met, src, var);
+    return D == 2 ? launch_phase<2>(a, lat->stream, met, src, var, lat->block)
+         : D == 3 ? launch_phase<3>(a, lat->stream, met, src, var, lat->block)
+                  : launch_phase<4>(a, lat->stream, met, src, var, lat->block);
   };
   for (int m = 0; m < metrop; ++m)
     for (int p = 0; p < 2; ++p)
@@ -822,14 +827,18 @@ static int capture_graph(u1_lattice *lat, F fn, cudaGraphExec_t *exec) {
   return U1_OK;
 }
 
+// Block sizes the phase kernels accept: whole warps up to their launch bound.
+static bool block_valid(int threads) { return threads >= 32 && threads <= 256 && threads % 32 == 0; }
+
 // ---------------------------------------------------------------- tuner
 // Replaces the reference's block-size search (src/tune.cpp:306-416,
 // include/tune.h:143-260): the candidates are the compiled update-kernel
 // variants (two sites per thread with a 32-register cap, two sites
-// uncapped, one site), which give bit-identical links, so a trial never
-// changes the Markov chain.  Trials run real sweeps from a backed-up state
-// (links and pass counter restored afterwards, as the reference's
-// preTune/postTune do); the winner is cached per (device, geometry) in
+// uncapped, one site), each at 64, 128 and 256 threads per block; all give
+// bit-identical links, so a trial never changes the Markov chain.  Each
+// trial captures its sweep as a CUDA graph, as u1_update runs it, and times
+// replays of it from a backed-up state (links and pass counter restored
+// afterwards, as the reference's preTune/postTune do); the winner is cached per (device, geometry) in
 // memory and, when U1_RESOURCE_PATH names a directory, in
 // $U1_RESOURCE_PATH/u1b200_tunecache.tsv (the reference's tunecache.csv
 // location rule, src/tune.cpp:160-232).  U1_TUNE=0 disables tuning.
@@ -837,7 +846,7 @@ namespace {
 struct TuneCache {
   std::mutex mu;
   bool loaded = false;
-  std::map<std::string, int> best;
+  std::map<std::string, std::pair<int, int>> best;  // key -> (variant, threads per block)
 };
 TuneCache &tune_cache() {
   static TuneCache c;
@@ -868,17 +877,26 @@ void tune_load_locked(TuneCache &c) {
     if (line.empty() || line[0] == '#') continue;
     const size_t t1 = line.find('\t');
     if (t1 == std::string::npos) continue;
-    const size_t t2 = line.find('\t', t1 + 1);
-    const std::string key = line.substr(0, t1);
-    const int v = std::atoi(line.substr(t1 + 1, t2 == std::string::npos ? std::string::npos : t2 - t1 - 1).c_str());
-    if (v >= U1V_PAIR32 && v <= U1V_WAVE) c.best[key] = v;
+    // key <tab> variant <tab> microseconds per sweep [<tab> threads per block]
+    std::vector<std::string> col;
+    size_t a = 0;
+    while (true) {
+      const size_t t = line.find('\t', a);
+      col.push_back(line.substr(a, t == std::string::npos ? std::string::npos : t - a));
+      if (t == std::string::npos) break;
+      a = t + 1;
+    }
+    if (col.size() < 2) continue;
+    const int v = std::atoi(col[1].c_str());
+    const int threads = col.size() >= 4 ? std::atoi(col[3].c_str()) : 256;
+    if (v >= U1V_PAIR32 && v <= U1V_WAVE && block_valid(threads)) c.best[col[0]] = {v, threads};
   }
 }
-void tune_save(const std::string &key, int v, double us) {
+void tune_save(const std::string &key, int v, double us, int threads) {
   const std::string f = tune_file();
   if (f.empty()) return;
   std::ofstream out(f, std::ios::app);
-  if (out) out << key << '\t' << v << '\t' << us << '\n';
+  if (out) out << key << '\t' << v << '\t' << us << '\t' << threads << '\n';
 }
 }  // namespace
 
@@ -889,16 +907,18 @@ static int tune_update(u1_lattice *lat, u1_rng *rng, bool use_cache) {
     std::lock_guard<std::mutex> lock(c.mu);
     tune_load_locked(c);
     auto it = c.best.find(key);
-    if (it != c.best.end() && variant_valid(lat, it->second)) {
-      lat->variant = it->second;
+    if (it != c.best.end() && variant_valid(lat, it->second.first)) {
+      lat->variant = it->second.first;
+      lat->block = it->second.second;
       drop_graphs(lat);
       return U1_OK;
     }
   }
-  std::vector<int> cand;
+  std::vector<std::pair<int, int>> cand;  // (variant, threads per block)
   for (int v : {U1V_PAIR32, U1V_PAIR, U1V_SINGLE})  // the persistent sweep is opt-in (u1_wave.cuh)
-    if (variant_valid(lat, v)) cand.push_back(v);
-  int best = cand[0];
+    if (variant_valid(lat, v))
+      for (int t : {256, 128, 64}) cand.push_back({v, t});
+  std::pair<int, int> best = cand[0];
   double best_us = -1.0;
   if (cand.size() > 1) {
     const size_t n = (size_t)lat->g.V * lat->g.dims;
@@ -909,14 +929,21 @@ static int tune_update(u1_lattice *lat, u1_rng *rng, bool use_cache) {
     U1_CUDA_TRY(cudaEventCreate(&e0));
     U1_CUDA_TRY(cudaEventCreate(&e1));
     int rc = U1_OK;
-    for (int v : cand) {
-      lat->variant = v;
-      rc = issue_sweep(lat, lat->links, rng, 1, 4, 0);
+    for (const auto &vt : cand) {
+      lat->variant = vt.first;
+      lat->block = vt.second;
+      cudaGraphExec_t ex = nullptr;
+      rc = capture_graph(lat, [&]() { return issue_sweep(lat, lat->links, rng, 1, 4, 0); }, &ex);
+      auto replay = [&]() -> int {
+        const cudaError_t er = cudaGraphLaunch(ex, lat->stream);
+        return er == cudaSuccess ? U1_OK : u1i::cuda_fail(er, "cudaGraphLaunch");
+      };
+      for (int k = 0; k < 2 && !rc; ++k) rc = replay();  // warm-up
       if (!rc) {
         const cudaError_t er = cudaEventRecord(e0, lat->stream);
         if (er != cudaSuccess) rc = u1i::cuda_fail(er, "cudaEventRecord");
       }
-      for (int k = 0; k < 3 && !rc; ++k) rc = issue_sweep(lat, lat->links, rng, 1, 4, 0);
+      for (int k = 0; k < 5 && !rc; ++k) rc = replay();
       cudaEventRecord(e1, lat->stream);
       cudaError_t e = cudaEventSynchronize(e1);
       if (!rc && e != cudaSuccess) rc = u1i::cuda_fail(e, "tuning sweep");
@@ -925,26 +952,29 @@ static int tune_update(u1_lattice *lat, u1_rng *rng, bool use_cache) {
       cudaMemcpyAsync(lat->links, lat->backup, n * sizeof(float2), cudaMemcpyDeviceToDevice, lat->stream);
       cudaMemcpyAsync(rng->pass_dev, &pass0, sizeof(pass0), cudaMemcpyHostToDevice, lat->stream);
       cudaStreamSynchronize(lat->stream);
+      if (ex) cudaGraphExecDestroy(ex);
       if (rc) break;
-      const double us = 1e3 * ms / 3.0;
+      const double us = 1e3 * ms / 5.0;
       if (best_us < 0.0 || us < best_us) {
         best_us = us;
-        best = v;
+        best = vt;
       }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc) {
       lat->variant = U1V_AUTO;
+      lat->block = 256;
       return rc;
     }
   }
-  lat->variant = best;
+  lat->variant = best.first;
+  lat->block = best.second;
   drop_graphs(lat);
   std::lock_guard<std::mutex> lock(c.mu);
   tune_load_locked(c);
   c.best[key] = best;
-  tune_save(key, best, best_us);
+  tune_save(key, best.first, best_us, best.second);
   return U1_OK;
 }
 
@@ -970,6 +1000,21 @@ extern "C" int u1_lattice_set_variant(u1_lattice *lat, int variant) {
 extern "C" int u1_lattice_get_variant(const u1_lattice *lat, int *variant) {
   if (!lat || !variant) return fail(U1_ERR_INVALID, "u1_lattice_get_variant: null argument");
   *variant = lat->variant;
+  return U1_OK;
+}
+
+extern "C" int u1_lattice_set_block(u1_lattice *lat, int threads) {
+  if (!lat) return fail(U1_ERR_INVALID, "u1_lattice_set_block: null lattice");
+  if (!block_valid(threads))
+    return fail(U1_ERR_INVALID, "u1_lattice_set_block: threads per block must be 32, 64, ..., 256");
+  lat->block = threads;
+  drop_graphs(lat);
+  return U1_OK;
+}
+
+extern "C" int u1_lattice_get_block(const u1_lattice *lat, int *threads) {
+  if (!lat || !threads) return fail(U1_ERR_INVALID, "u1_lattice_get_block: null argument");
+  *threads = lat->block;
   return U1_OK;
 }
 
@@ -1083,9 +1128,9 @@ extern "C" int u1_update_phase(u1_lattice *lat, u1_rng *rng, int metropolis, int
   const int src = metropolis_src(lat, rng);
   const int var = sweep_variant(lat, src, 0);
   switch (lat->g.dims) {
-    case 2: return launch_phase<2>(a, lat->stream, met, src, var);
-    case 3: return launch_phase<3>(a, lat->stream, met, src, var);
-    default: return launch_phase<4>(a, lat->stream, met, src, var);
+    case 2: return launch_phase<2>(a, lat->stream, met, src, var, lat->block);
+    case 3: return launch_phase<3>(a, lat->stream, met, src, var, lat->block);
+    default: return launch_phase<4>(a, lat->stream, met, src, var, lat->block);
   }
 }
 

@@ -53,6 +53,7 @@ struct u1_lattice {
   std::map<std::tuple<int, int, uint64_t, uint64_t>, cudaGraphExec_t> graphs;
   bool use_graphs = true;
   int variant = U1V_AUTO;          // update kernel variant (U1V_AUTO: tune on first update)
+  int block = 256;                 // threads per block of the phase kernels (tuned with the variant)
   // Metropolis proposal: half-width delta (0: the reference's whole-circle
   // theta' = 2 pi u), win = delta/pi as used by the kernels, hits per link
   double delta = 0.0;

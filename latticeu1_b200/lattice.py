@@ -162,6 +162,16 @@ class Lattice:
     def set_variant(self, variant: int) -> None:
         check(lib.u1_lattice_set_variant(self._h, int(variant)), "u1_lattice_set_variant")
 
+    @property
+    def block(self) -> int:
+        """Threads per block of the phase kernels (tuned with the variant)."""
+        v = C.c_int()
+        check(lib.u1_lattice_get_block(self._h, C.byref(v)), "u1_lattice_get_block")
+        return int(v.value)
+
+    def set_block(self, threads: int) -> None:
+        check(lib.u1_lattice_set_block(self._h, int(threads)), "u1_lattice_set_block")
+
     def set_metropolis(self, delta: float = 0.0, nhits: int = 1) -> None:
         """Metropolis proposal: nhits hits per link and pass, each proposing
         theta' = theta + delta (2u - 1), or theta' = 2 pi u for delta = 0

@@ -54,6 +54,29 @@ def test_variants_bit_identical(ctx, geom):
         assert np.array_equal(th, base), f"variant {v} differs from the one-site kernel"
 
 
+@pytest.mark.parametrize("geom", VARIANT_GEOMS[:3], ids=lambda g: f"{g[0]}d-{'x'.join(map(str, g[1]))}")
+def test_block_sizes_bit_identical(ctx, geom):
+    """Every threads-per-block setting of the phase kernels gives the same
+    links (the kernels index sites from blockDim; ragged last blocks)."""
+    pair_ok = (geom[1][0] // 2) % 2 == 0
+    base = _run(ctx, geom, 3)[0].export_angles()
+    for v in ((1, 2, 3) if pair_ok else (3,)):
+        for t in (32, 64, 96, 128, 224):
+            dims, N, beta, aniso = geom
+            lat = Lattice(ctx, dims, N, beta, aniso)
+            lat.set_variant(v)
+            lat.set_block(t)
+            assert lat.block == t
+            rng = Rng(ctx, 77)
+            lat.hot_start(rng)
+            for m, o in ((1, 4), (2, 0), (0, 3)):
+                lat.update(rng, m, o)
+            assert np.array_equal(lat.export_angles(), base), (v, t)
+    for bad in (0, 16, 48, 288, 512):
+        with pytest.raises(U1Error):
+            Lattice(ctx, *geom[:2], geom[2], geom[3]).set_block(bad)
+
+
 def test_graphs_and_variants_agree(ctx):
     geom = (4, (8, 8, 8, 8), 1.0, 1.0)
     a, _ = _run(ctx, geom, 1)
@@ -79,13 +102,14 @@ def test_tune_restores_state_and_caches(ctx, tmp_path, monkeypatch):
     st0 = rng.state
     best = lat.tune(rng)
     assert best in (1, 2, 3)
-    assert lat.variant == best
+    assert lat.variant == best and lat.block in (64, 128, 256)
     assert np.array_equal(lat.export_angles(), th0)
     assert rng.state == st0
     cache = tmp_path / "u1b200_tunecache.tsv"
     assert cache.exists()
     lines = [ln.split("\t") for ln in cache.read_text().splitlines()]
-    assert any(ln[0].endswith("|update|4|8x8x8x12") and int(ln[1]) == best for ln in lines)
+    assert any(ln[0].endswith("|update|4|8x8x8x12") and int(ln[1]) == best and int(ln[3]) == lat.block
+               for ln in lines)
     # the tuned lattice continues the same chain as an untuned one
     ref = Lattice(ctx, 4, (8, 8, 8, 12), 1.0)
     ref.set_variant(3)
