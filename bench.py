@@ -321,6 +321,16 @@ def run_ours(args) -> None:
         clk = clocks.stop()
         if clk is not None:
             clk["window"] = f"timed region + {CLOCK_WINDOW_S:.1f} s of the same step"
+        # the same sweep without the measurement (not the headline; it shows what the measurement costs)
+        ev2 = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
+        lat.update(rng, METROP, OVRN)
+        for k in range(args.steps):
+            flush.zero_()
+            ev2[k][0].record(stream)
+            lat.update(rng, METROP, OVRN)
+            ev2[k][1].record(stream)
+        torch.cuda.synchronize()
+        sweep_only_ms = sum(e[0].elapsed_time(e[1]) for e in ev2) / args.steps
     step_ms = sum(e[0].elapsed_time(e[1]) for e in ev)
     upd_ms = step_ms  # the measurement runs inside the sweep's last phase
     step_ms_max = replicas.max_over_ranks(step_ms)
@@ -414,6 +424,7 @@ def run_ours(args) -> None:
             "clocks": clk,
             "wall_s_timed_region": t_wall,
             "update_ms_per_step": upd_ms / args.steps,
+            "sweep_only_ms_per_step": sweep_only_ms,
             "observables": {"plaq_ss_re": float(ob[:, 0].mean()), "plaq_st_re": float(ob[:, 2].mean()),
                             "abs_L": float(np.abs(ob[:, 4] + 1j * ob[:, 5]).mean()),
                             "per_chain_plaq_ss_st": per_chain},

@@ -725,9 +725,20 @@ static int launch_poly_finish(u1_lattice *lat, int variant, double *dev_out) {
   const double normL = 1.0 / (double)g.Vs;
   const int nbp = meas_slot_entries(lat, variant);
   double *poly = lat->partials + (size_t)(D - 1) * nbp * 2;
-  k_poly_finish<D><<<m.nb_poly, kRedThreads, 0, lat->stream>>>(lat->links, g, m, lat->partials, nbp, poly,
-                                                               lat->counter, dev_out, normSS, normST, normL);
-  U1_LAUNCH_CHECK("k_poly_finish");
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)m.nb_poly);
+  cfg.blockDim = dim3(kRedThreads);
+  cfg.stream = lat->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, k_poly_finish<D>, (const float2 *)lat->links, g, m,
+                                           (const double *)lat->partials, nbp, poly, lat->counter, dev_out, normSS,
+                                           normST, normL);
+  u1i::g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (e != cudaSuccess) return u1i::cuda_fail(e, "k_poly_finish");
   return U1_OK;
 }
 

@@ -55,6 +55,7 @@ static __global__ void __launch_bounds__(kRedThreads)
   __shared__ float2 lp[kRedThreads];
   __shared__ bool am_last;
   float vs[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  pdl_wait_prior_grid();  // launched early (programmatic dependent launch): wait for the sweep's last phase
   measure_block_values<D>(lat, g, (int)blockIdx.x + m.nb_plaq, m, vs, lp);  // Polyakov blocks only
   const double tot = measure_block_total(vs, false, smem);                 // threads 4, 5
   if (threadIdx.x >= 4 && threadIdx.x < 6) {
