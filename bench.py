@@ -141,6 +141,11 @@ def measured_peak() -> tuple[float, str]:
     return 6650.0, "fallback"
 
 
+# update kernel of each variant (u1_lattice_set_variant)
+KERNEL_OF_VARIANT = {1: "k_update_pair", 2: "k_update_pair_free", 3: "k_update", 4: "k_sweep_wave",
+                     5: "k_update_quad"}
+
+
 def ncu_batch_traffic_per_link_sweep():
     """DRAM bytes per link and sweep of the grouped batch from the committed
     ncu summary, if any."""
@@ -153,15 +158,17 @@ def ncu_batch_traffic_per_link_sweep():
     return None
 
 
-def ncu_traffic_per_launch(N):
-    """DRAM bytes per k_update launch from the committed ncu summary, if any."""
+def ncu_traffic_per_launch(N, kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if
+    there is one for this geometry and kernel."""
     p = ROOT / "profiles" / f"k_update_{geom_name(N).replace('^4', 'x4')}_traffic.txt"
     if not p.exists():
         return None
-    for line in p.read_text().splitlines():
-        if line.startswith("dram_bytes_per_launch:"):
-            return float(line.split(":", 1)[1].split()[0])
-    return None
+    fields = dict(line.split(":", 1) for line in p.read_text().splitlines()
+                  if ":" in line and not line.startswith("#"))
+    if fields.get("kernel", "").strip() != kernel or "dram_bytes_per_launch" not in fields:
+        return None
+    return float(fields["dram_bytes_per_launch"].split()[0])
 
 
 # ------------------------------------------------------------------ CPU baselines
@@ -276,6 +283,9 @@ def run_ours(args) -> None:
     ctx = Context(local)
     lat = Lattice(ctx, DIMS, N, beta, aniso)
     lat.set_metropolis(args.delta, args.nhits)
+    if args.variant:  # otherwise the tuner chooses at the first update
+        lat.set_variant(args.variant)
+        lat.set_block(args.block)
     stream = torch.cuda.Stream()
     lat.set_stream(stream.cuda_stream)
     rng = Rng(ctx, 1234)
@@ -400,13 +410,15 @@ def run_ours(args) -> None:
         avg_launch_s = upd_ms * 1e-3 / (args.steps * upd_launches)
         alg_bytes = algorithmic_bytes_per_link_update(DIMS) * volume(N) // 2
         achieved = alg_bytes / avg_launch_s / 1e9
-        traffic = ncu_traffic_per_launch(N)
+        traffic = ncu_traffic_per_launch(N, KERNEL_OF_VARIANT.get(lat.variant, "k_update"))
         line = {
             "metric": metric_for(N), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": workload_config(N, beta, aniso, args.delta, args.nhits),
-            "roofline": {"bound": "hbm", "kernel": "k_update_pair (one (parity,mu) phase; step average)",
+            "roofline": {"bound": "hbm",
+                         "kernel": KERNEL_OF_VARIANT.get(lat.variant, "k_update") +
+                                   " (one (parity,mu) phase; step average)",
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "algorithmic_bytes_per_launch": alg_bytes,
@@ -618,6 +630,9 @@ def main() -> None:
     ap.add_argument("--delta", type=float, default=0.0,
                     help="Metropolis proposal half-width (0: the reference's whole-circle proposal)")
     ap.add_argument("--nhits", type=int, default=1, help="Metropolis hits per link and pass")
+    ap.add_argument("--variant", type=int, default=0,
+                    help="update kernel variant (0: tuned; 1 pair32, 2 pair, 3 single, 4 wave, 5 quad)")
+    ap.add_argument("--block", type=int, default=256, help="threads per block with --variant")
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU baseline sampling")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["update32", "multilevel", "batched"], default="update32")

@@ -84,8 +84,10 @@ int u1_lattice_set_coupling(u1_lattice *lat, double beta, double aniso);
 int u1_lattice_set_graphs(u1_lattice *lat, int enable);
 /* Update kernel variants, all giving bit-identical links: 1 = two sites per
  * thread (32-register cap, 8 CTAs/SM), 2 = two sites per thread (no cap),
- * 3 = one site per thread; 0 = auto (tuned at the first u1_update among 1-3).
- * The two-site variants need Nx/2 even.  4 = the whole sweep as one
+ * 3 = one site per thread, 5 = four sites per thread (64-register cap,
+ * 256-bit loads); 0 = auto (tuned at the first u1_update among 1, 2, 3, 5).
+ * The two-site variants need Nx/2 even, the four-site one Nx/2 a multiple
+ * of 4.  4 = the whole sweep as one
  * persistent cooperative kernel with neighbour-local phase synchronisation
  * (4D, (Nx/2)*Ny/2 a multiple of 32 in [64, 256], every (z, t) tile resident
  * at once; opt-in, slower than 1 on B200 at 32^4). */
@@ -106,7 +108,7 @@ int u1_lattice_get_variant(const u1_lattice *lat, int *variant);
 int u1_lattice_set_metropolis(u1_lattice *lat, double delta, int nhits);
 int u1_lattice_get_metropolis(const u1_lattice *lat, double *delta, int *nhits);
 /* Replaces the reference's autotuner (tuneLaunch, src/tune.cpp:306-416):
- * times every valid variant 1-3 at 64, 128 and 256 threads per block on a
+ * times every valid variant (1, 2, 3, 5) at 64, 128 and 256 threads per block on a
  * few sweeps of this lattice from a backed-up state (links and rng pass
  * restored afterwards), keeps the fastest pair and caches it per (device,
  * geometry); with U1_RESOURCE_PATH set the cache persists in
@@ -114,7 +116,7 @@ int u1_lattice_get_metropolis(const u1_lattice *lat, double *delta, int *nhits);
  * turns the automatic first-update tuning off.  *variant gets the variant;
  * u1_lattice_get_block the block size. */
 int u1_tune(u1_lattice *lat, u1_rng *rng, int *variant);
-/* Threads per block of the phase kernels of variants 1-3 (32, 64, ..., 256;
+/* Threads per block of the phase kernels of variants 1, 2, 3, 5 (32, ..., 256;
  * default 256; the reference's block.x, include/tune.h:143-260).  Every block
  * size gives bit-identical links.  The measuring phases of a measured sweep
  * and the persistent variant keep their own block sizes. */

@@ -519,6 +519,11 @@ static int launch_pdl(K kernel, int blocks, cudaStream_t s, const UpdArgs &a, co
 // the same links.
 template <int D, int MU, int SRC>
 static int launch_variant(const UpdArgs &a, cudaStream_t s, bool met, int variant, int threads) {
+  if (variant == U1V_QUAD) {
+    const int blocks = u1i::blocks_for(a.g.Vh / 4, threads);
+    return met ? launch_pdl(k_update_quad<D, MU, true, SRC>, blocks, s, a, "k_update_quad", threads)
+               : launch_pdl(k_update_quad<D, MU, false, SRC_PHILOX>, blocks, s, a, "k_update_quad", threads);
+  }
   if (variant == U1V_PAIR32 || variant == U1V_PAIR) {
     const int blocks = u1i::blocks_for(a.g.Vh / 2, threads);
     if (variant == U1V_PAIR32)
@@ -587,7 +592,8 @@ static bool wave_usable(u1_lattice *lat) {
 static bool variant_valid(u1_lattice *lat, int v) {
   const GeomK &g = lat->g;
   if (v == U1V_WAVE) return wave_usable(lat);
-  return v == U1V_SINGLE || ((v == U1V_PAIR32 || v == U1V_PAIR) && (g.hN0 & 1) == 0);
+  return v == U1V_SINGLE || ((v == U1V_PAIR32 || v == U1V_PAIR) && (g.hN0 & 1) == 0) ||
+         (v == U1V_QUAD && (g.hN0 & 3) == 0);
 }
 
 // One sweep as a single cooperative launch of k_sweep_wave (see u1_wave.cuh).
@@ -900,7 +906,7 @@ void tune_load_locked(TuneCache &c) {
     if (col.size() < 2) continue;
     const int v = std::atoi(col[1].c_str());
     const int threads = col.size() >= 4 ? std::atoi(col[3].c_str()) : 256;
-    if (v >= U1V_PAIR32 && v <= U1V_WAVE && block_valid(threads)) c.best[col[0]] = {v, threads};
+    if (v >= U1V_PAIR32 && v <= U1V_QUAD && block_valid(threads)) c.best[col[0]] = {v, threads};
   }
 }
 void tune_save(const std::string &key, int v, double us, int threads) {
@@ -926,7 +932,7 @@ static int tune_update(u1_lattice *lat, u1_rng *rng, bool use_cache) {
     }
   }
   std::vector<std::pair<int, int>> cand;  // (variant, threads per block)
-  for (int v : {U1V_PAIR32, U1V_PAIR, U1V_SINGLE})  // the persistent sweep is opt-in (u1_wave.cuh)
+  for (int v : {U1V_PAIR32, U1V_QUAD, U1V_PAIR, U1V_SINGLE})  // the persistent sweep is opt-in (u1_wave.cuh)
     if (variant_valid(lat, v))
       for (int t : {256, 128, 64}) cand.push_back({v, t});
   std::pair<int, int> best = cand[0];

@@ -29,7 +29,7 @@ struct u1_rng {
 };
 
 // Update kernel variants (all bit-identical; the tuner picks the fastest).
-enum : int { U1V_AUTO = 0, U1V_PAIR32 = 1, U1V_PAIR = 2, U1V_SINGLE = 3, U1V_WAVE = 4 };
+enum : int { U1V_AUTO = 0, U1V_PAIR32 = 1, U1V_PAIR = 2, U1V_SINGLE = 3, U1V_WAVE = 4, U1V_QUAD = 5 };
 
 struct u1_lattice {
   u1_ctx *ctx = nullptr;

@@ -394,6 +394,140 @@ __device__ __forceinline__ void update_pair_body(const UpdArgs a, int i, float2 
   }
 }
 
+// ---------------------------------------------------------------------------
+// Four sites per thread.  When N0/2 is a multiple of 4, EO sites 4t..4t+3 of
+// a phase lie in one x0-row: they share x1..x3 and every step along them,
+// and those steps are multiples of N0/2, so the four neighbour links along
+// x1..x3 are consecutive and 32-byte aligned: one 256-bit load serves the
+// four sites.  Steps along x0 differ per site (a shift of 0 or 1 within the
+// row, wrapping at its end), so x0-shifted neighbours are loaded per site.
+// The site decode and the steps are computed once for four sites.
+struct Quad2 {
+  float2 s[4];
+};
+
+// Four consecutive links from a 32-byte aligned address (idx % 4 == 0).
+// Non-coherent (read-only path): a phase kernel never reads what it writes.
+// volatile + "memory" keep the load after the grid-dependency wait.
+__device__ __forceinline__ Quad2 ld_quad(const float2 *base, int idx) {
+  Quad2 q;
+  asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=f"(q.s[0].x), "=f"(q.s[0].y), "=f"(q.s[1].x), "=f"(q.s[1].y), "=f"(q.s[2].x), "=f"(q.s[2].y),
+                 "=f"(q.s[3].x), "=f"(q.s[3].y)
+               : "l"(base + idx)
+               : "memory");
+  return q;
+}
+// The same through the coherent path (the thread's own links, stored later).
+__device__ __forceinline__ Quad2 ld_quad_own(const float2 *p) {
+  Quad2 q;
+  asm volatile("ld.global.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=f"(q.s[0].x), "=f"(q.s[0].y), "=f"(q.s[1].x), "=f"(q.s[1].y), "=f"(q.s[2].x), "=f"(q.s[2].y),
+                 "=f"(q.s[3].x), "=f"(q.s[3].y)
+               : "l"(p)
+               : "memory");
+  return q;
+}
+__device__ __forceinline__ void st_quad(float2 *p, const float2 n[4]) {
+  asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "f"(n[0].x), "f"(n[0].y), "f"(n[1].x),
+               "f"(n[1].y), "f"(n[2].x), "f"(n[2].y), "f"(n[3].x), "f"(n[3].y)
+               : "memory");
+}
+// Per-site links at base + i + s + sh[s], s = 0..3.
+__device__ __forceinline__ Quad2 ld_shifted(const float2 *base, int i, const int sh[4]) {
+  Quad2 q;
+#pragma unroll
+  for (int s = 0; s < 4; ++s) q.s[s] = __ldg(base + i + s + sh[s]);
+  return q;
+}
+
+// Body of the four-sites-per-thread update for EO sites i..i+3 (i a multiple
+// of 4) of the phase (a.p, MU); every site's staple and update use the same
+// operations in the same order as the other bodies (bit-identical links).
+template <int D, int MU, bool MET, int SRC>
+__device__ __forceinline__ void update_quad_body(const UpdArgs a, int i) {
+  int x[4], k;
+  eo_decode_fast<D>(a.g, i, a.p, x, k);
+  phase_entry<MET>(a);
+  if (i >= a.g.Vh) return;
+  if (MU != 3 && a.ml > 0 && (x[D - 1] & (a.ml - 1)) == 0) return;  // freeze rule, src/multilevel.cu:41
+  int fwd[4], bwd[4];
+  eo_steps<D>(a.g, x, k, fwd, bwd);  // steps of site i; sites i+1..i+3 share those along x1..x3
+  const int odd = x[0] & 1;
+  int f0[4], b0[4];  // x0 steps of the four sites (k multiple of 4: only site 3 can end the row, site 0 start it)
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    f0[s] = odd ? ((s == 3 && k + 3 == a.g.hN0 - 1) ? a.g.wrapf[0] : 1) : 0;
+    b0[s] = odd ? 0 : ((s == 0 && k == 0) ? a.g.wrapb[0] : -1);
+  }
+  const int q = 1 - a.p;
+  const int V = a.g.V, Vh = a.g.Vh;
+  const float2 *lat = a.lat;
+  const float2 *Lq_mu = lat + MU * V + q * Vh;
+  float2 ss[4], st[4];
+#pragma unroll
+  for (int s = 0; s < 4; ++s) ss[s] = st[s] = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int nu = 0; nu < D; ++nu) {
+    if (nu == MU) continue;
+    const float2 *Lp_nu = lat + nu * V + a.p * Vh;
+    const float2 *Lq_nu = lat + nu * V + q * Vh;
+    Quad2 A, B, C, Dd, E, F;
+    C = ld_quad(Lp_nu, i);
+    if (MU == 0) {  // nu != 0: steps along nu shared, along x0 per site
+      A = ld_shifted(Lq_nu, i, f0);
+      B = ld_quad(Lq_mu, i + fwd[nu]);
+      Dd = ld_shifted(Lp_nu, i + bwd[nu], f0);
+      E = ld_quad(Lq_mu, i + bwd[nu]);
+      F = ld_quad(Lq_nu, i + bwd[nu]);
+    } else if (nu == 0) {  // MU != 0
+      A = ld_quad(Lq_nu, i + fwd[MU]);
+      B = ld_shifted(Lq_mu, i, f0);
+      Dd = ld_shifted(Lp_nu, i + fwd[MU], b0);
+      E = ld_shifted(Lq_mu, i, b0);
+      F = ld_shifted(Lq_nu, i, b0);
+    } else {  // MU != 0, nu != 0: every load 256-bit
+      A = ld_quad(Lq_nu, i + fwd[MU]);
+      B = ld_quad(Lq_mu, i + fwd[nu]);
+      Dd = ld_quad(Lp_nu, i + fwd[MU] + bwd[nu]);
+      E = ld_quad(Lq_mu, i + bwd[nu]);
+      F = ld_quad(Lq_nu, i + bwd[nu]);
+    }
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      const float2 t =
+          cadd(cmulc(cmulc(A.s[s], B.s[s]), C.s[s]), cmul(cconjmul(Dd.s[s], E.s[s]), F.s[s]));
+      if (MU == D - 1 || nu == D - 1)
+        st[s] = cadd(st[s], t);
+      else
+        ss[s] = cadd(ss[s], t);
+    }
+  }
+  float2 *own = a.lat + MU * V + a.p * Vh + i;
+  const Quad2 U = ld_quad_own(own);
+  // sites i, i+1 and i+2, i+3 share one Philox block each
+  Philox4 blk0, blk1;
+  if (MET && SRC != SRC_REPLAY) {
+    const unsigned long long pass = *a.pass_dev + (unsigned long long)a.hit;
+    blk0 = u1_metropolis_block((uint32_t)(a.p * Vh + i), MU, a.chain, pass, a.key0, a.key1);
+    blk1 = u1_metropolis_block((uint32_t)(a.p * Vh + i + 2), MU, a.chain, pass, a.key0, a.key1);
+  }
+  float2 N[4];
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+    N[s] = update_one<D, MU, MET, SRC>(a, i + s, cweigh(ss[s], a.c.w_ss, st[s], a.c.w_st), U.s[s],
+                                       s < 2 ? &blk0 : &blk1);
+  st_quad(own, N);
+  pdl_release_dependents();
+}
+
+// Four sites per thread, register budget capped at 64 so 4 CTAs of 256
+// threads fit an SM (a 32^4 phase is then a single wave).
+template <int D, int MU, bool MET, int SRC>
+__global__ void __launch_bounds__(256, 4) k_update_quad(const UpdArgs a) {
+  update_quad_body<D, MU, MET, SRC>(a, 4 * (blockIdx.x * blockDim.x + threadIdx.x));
+}
+
 // Two sites per thread, register budget capped at 32 so 8 CTAs of 256
 // threads fit an SM (a 32^4 phase is then a single wave).
 template <int D, int MU, bool MET, int SRC>

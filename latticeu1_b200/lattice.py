@@ -151,7 +151,7 @@ class Lattice:
     def set_graphs(self, enable: bool) -> None:
         check(lib.u1_lattice_set_graphs(self._h, int(bool(enable))), "u1_lattice_set_graphs")
 
-    VARIANTS = {0: "auto", 1: "pair32", 2: "pair", 3: "single", 4: "wave"}
+    VARIANTS = {0: "auto", 1: "pair32", 2: "pair", 3: "single", 4: "wave", 5: "quad"}
 
     @property
     def variant(self) -> int:

@@ -19,6 +19,7 @@ pytestmark = pytest.mark.gpu
 # (dims, N, beta, aniso); Nx = 6 gives Nx/2 odd (two-site kernels invalid)
 VARIANT_GEOMS = [
     (4, (8, 8, 8, 8), 1.0, 1.0),
+    (4, (16, 6, 4, 4), 1.05, 1.5),  # N0/2 = 8: quads inside and at the ends of a row
     (4, (12, 8, 4, 6), 0.9, 1.3),
     (4, (6, 4, 4, 8), 1.1, 1.0),
     (3, (8, 8, 0, 12), 1.2, 0.8),
@@ -41,9 +42,10 @@ def _run(ctx, geom, variant, seed=77, chain=0, sweeps=((1, 4), (2, 0), (0, 3))):
 @pytest.mark.parametrize("geom", VARIANT_GEOMS, ids=lambda g: f"{g[0]}d-{'x'.join(map(str, g[1]))}")
 def test_variants_bit_identical(ctx, geom):
     pair_ok = (geom[1][0] // 2) % 2 == 0
+    quad_ok = (geom[1][0] // 2) % 4 == 0
     results = {}
-    for v in (1, 2, 3):
-        if not pair_ok and v in (1, 2):
+    for v in (1, 2, 3, 5):
+        if (not pair_ok and v in (1, 2)) or (not quad_ok and v == 5):
             with pytest.raises(U1Error):
                 Lattice(ctx, *geom[:2], geom[2], geom[3]).set_variant(v)
             continue
@@ -59,8 +61,9 @@ def test_block_sizes_bit_identical(ctx, geom):
     """Every threads-per-block setting of the phase kernels gives the same
     links (the kernels index sites from blockDim; ragged last blocks)."""
     pair_ok = (geom[1][0] // 2) % 2 == 0
+    quad_ok = (geom[1][0] // 2) % 4 == 0
     base = _run(ctx, geom, 3)[0].export_angles()
-    for v in ((1, 2, 3) if pair_ok else (3,)):
+    for v in ((1, 2, 3) if pair_ok else (3,)) + ((5,) if quad_ok else ()):
         for t in (32, 64, 96, 128, 224):
             dims, N, beta, aniso = geom
             lat = Lattice(ctx, dims, N, beta, aniso)
@@ -101,7 +104,7 @@ def test_tune_restores_state_and_caches(ctx, tmp_path, monkeypatch):
     th0 = lat.export_angles()
     st0 = rng.state
     best = lat.tune(rng)
-    assert best in (1, 2, 3)
+    assert best in (1, 2, 3, 5)
     assert lat.variant == best and lat.block in (64, 128, 256)
     assert np.array_equal(lat.export_angles(), th0)
     assert rng.state == st0
@@ -129,7 +132,7 @@ def test_auto_variant_tunes_on_first_update(ctx, monkeypatch, tmp_path):
     rng = Rng(ctx, 9)
     lat.hot_start(rng)
     lat.update(rng, 1, 1)
-    assert lat.variant in (1, 2, 3)
+    assert lat.variant in (1, 2, 3, 5)
     ref, _ = _run(ctx, (4, (8, 8, 8, 8), 1.0, 1.0), 3, seed=9, sweeps=((1, 1),))
     assert np.array_equal(lat.export_angles(), ref.export_angles())
 
