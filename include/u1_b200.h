@@ -84,8 +84,8 @@ int u1_lattice_set_coupling(u1_lattice *lat, double beta, double aniso);
 int u1_lattice_set_graphs(u1_lattice *lat, int enable);
 /* Update kernel variants, all giving bit-identical links: 1 = two sites per
  * thread (32-register cap, 8 CTAs/SM), 2 = two sites per thread (no cap),
- * 3 = one site per thread, 5 = four sites per thread (64-register cap,
- * 256-bit loads); 0 = auto (tuned at the first u1_update among 1, 2, 3, 5).
+ * 3 = one site per thread, 5 = four sites per thread (72-register cap,
+ * 256-bit loads, at most 128 threads per block: larger settings run 128); 0 = auto (tuned at the first u1_update among 1, 2, 3, 5).
  * The two-site variants need Nx/2 even, the four-site one Nx/2 a multiple
  * of 4.  4 = the whole sweep as one
  * persistent cooperative kernel with neighbour-local phase synchronisation

@@ -11,6 +11,7 @@
 // status codes instead of exit(), explicit streams, no per-op device
 // synchronisation except where a host result is returned, and whole sweeps
 // replayed as CUDA graphs.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -520,6 +521,7 @@ static int launch_pdl(K kernel, int blocks, cudaStream_t s, const UpdArgs &a, co
 template <int D, int MU, int SRC>
 static int launch_variant(const UpdArgs &a, cudaStream_t s, bool met, int variant, int threads) {
   if (variant == U1V_QUAD) {
+    threads = std::min(threads, 128);  // the kernel's launch bound
     const int blocks = u1i::blocks_for(a.g.Vh / 4, threads);
     return met ? launch_pdl(k_update_quad<D, MU, true, SRC>, blocks, s, a, "k_update_quad", threads)
                : launch_pdl(k_update_quad<D, MU, false, SRC_PHILOX>, blocks, s, a, "k_update_quad", threads);
@@ -934,7 +936,8 @@ static int tune_update(u1_lattice *lat, u1_rng *rng, bool use_cache) {
   std::vector<std::pair<int, int>> cand;  // (variant, threads per block)
   for (int v : {U1V_PAIR32, U1V_QUAD, U1V_PAIR, U1V_SINGLE})  // the persistent sweep is opt-in (u1_wave.cuh)
     if (variant_valid(lat, v))
-      for (int t : {256, 128, 64}) cand.push_back({v, t});
+      for (int t : {256, 128, 64})
+        if (v != U1V_QUAD || t <= 128) cand.push_back({v, t});
   std::pair<int, int> best = cand[0];
   double best_us = -1.0;
   if (cand.size() > 1) {

@@ -521,10 +521,10 @@ __device__ __forceinline__ void update_quad_body(const UpdArgs a, int i) {
   pdl_release_dependents();
 }
 
-// Four sites per thread, register budget capped at 64 so 4 CTAs of 256
-// threads fit an SM (a 32^4 phase is then a single wave).
+// Four sites per thread, at most 128 threads per block and a register budget
+// of 72, so 7 CTAs fit an SM (a 32^4 phase, 1024 CTAs, is then a single wave).
 template <int D, int MU, bool MET, int SRC>
-__global__ void __launch_bounds__(256, 4) k_update_quad(const UpdArgs a) {
+__global__ void __launch_bounds__(128, 7) k_update_quad(const UpdArgs a) {
   update_quad_body<D, MU, MET, SRC>(a, 4 * (blockIdx.x * blockDim.x + threadIdx.x));
 }
 
