@@ -35,6 +35,7 @@ struct BatchChain {
   uint32_t chain;
   int first_pair;   // first block in the pair (two sites / thread) table
   int first_site;   // first block in the site (one site / thread) table
+  int first_quad;   // first block in the quad (four sites / thread) table
   int first_meas;   // first block in the measurement table
   MeasK meas;       // measurement layout (plaquette blocks, then Polyakov blocks)
   int nb_meas;
@@ -58,6 +59,37 @@ __device__ __forceinline__ void stage_chain(const BatchChain *__restrict__ chain
   uint32_t *dst = reinterpret_cast<uint32_t *>(&sch);
   for (int w = threadIdx.x; w < words; w += blockDim.x) dst[w] = __ldg(src + w);
   __syncthreads();
+}
+
+// The kernel arguments of block `blk` of a batch phase (the block's chain
+// staged in shared memory).
+__device__ __forceinline__ UpdArgs batch_args(const BatchChain &sch, const BatchPhase &ph, int mu) {
+  UpdArgs a{};
+  a.lat = sch.links;
+  a.g = sch.g;
+  a.c = sch.c;
+  a.p = ph.p;
+  a.mu = mu;
+  a.key0 = ph.key0;
+  a.key1 = ph.key1;
+  a.chain = sch.chain;
+  a.pass_dev = ph.pass_dev;
+  a.hit = ph.hit;
+  a.bump_ptr = ph.bump_ptr;
+  a.bump_by = ph.bump_by;
+  return a;
+}
+
+// Four sites per thread (every chain of the launch's group has N0/2 a
+// multiple of 4), 128 threads and 512 sites per block, as k_update_quad.
+template <int D, int MU, bool MET>
+__global__ void __launch_bounds__(128, 7)
+    k_batch_update_quad(const BatchChain *__restrict__ chains, const int *__restrict__ block_chain, BatchPhase ph) {
+  __shared__ BatchChain sch;
+  const int blk = (int)blockIdx.x + ph.block_base;
+  stage_chain(chains, __ldg(block_chain + blk), sch);
+  const UpdArgs a = batch_args(sch, ph, MU);
+  update_quad_body<D, MU, MET, SRC_PHILOX>(a, 4 * ((blk - sch.first_quad) * (int)blockDim.x + (int)threadIdx.x));
 }
 
 template <int D, int MU, bool MET, bool PAIR>
@@ -148,15 +180,16 @@ struct u1_batch {
   BatchChain *d_chains = nullptr;
   float2 *links = nullptr;
   size_t total_links = 0;
-  int *d_tab_pair = nullptr, *d_tab_site = nullptr, *d_tab_meas = nullptr;
-  int nb_pair = 0, nb_site = 0, nb_meas = 0;
+  int *d_tab_pair = nullptr, *d_tab_site = nullptr, *d_tab_meas = nullptr, *d_tab_quad = nullptr;
+  int nb_pair = 0, nb_site = 0, nb_meas = 0, nb_quad = 0;
   double *partials = nullptr, *d_out = nullptr, *h_out = nullptr;
   std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
   // Chain groups swept one after another: consecutive chains whose links
   // together fit comfortably in L2, so that after a group's first phase its
   // links are served from L2.  Each: first pair block, pair blocks, first
-  // site block, site blocks.
-  std::vector<std::array<int, 4>> groups;
+  // site block, site blocks, first quad block, quad blocks (0 unless every
+  // chain of the group takes four sites per thread).
+  std::vector<std::array<int, 6>> groups;
 };
 
 using u1i::cuda_fail;
@@ -178,6 +211,7 @@ extern "C" int u1_batch_destroy(u1_batch *b) {
   cudaFree(b->d_tab_pair);
   cudaFree(b->d_tab_site);
   cudaFree(b->d_tab_meas);
+  cudaFree(b->d_tab_quad);
   cudaFree(b->partials);
   cudaFree(b->d_out);
   cudaFree(b->pass_dev);
@@ -199,7 +233,7 @@ extern "C" int u1_batch_create(u1_ctx *ctx, int nchains, const u1_geom *geoms, u
   b->n = nchains;
   b->seed = seed;
   b->h_chains.resize(nchains);
-  std::vector<int> tab_pair, tab_site, tab_meas;
+  std::vector<int> tab_pair, tab_site, tab_meas, tab_quad;
   size_t off = 0;
   std::vector<size_t> offsets(nchains);
   for (int c = 0; c < nchains; ++c) {
@@ -234,8 +268,11 @@ extern "C" int u1_batch_create(u1_ctx *ctx, int nchains, const u1_geom *geoms, u
     ch.norm[1] = 1.0 / ((double)g.V * nST);
     ch.norm[2] = 1.0 / (double)g.Vs;
     const int np = nblocks(g.Vh / 2, 256), ns = nblocks(g.Vh, 256);
+    const int nq = (g.hN0 & 3) == 0 ? nblocks(g.Vh / 4, 128) : 0;
     ch.first_pair = (int)tab_pair.size();
     ch.first_site = (int)tab_site.size();
+    ch.first_quad = (int)tab_quad.size();
+    tab_quad.insert(tab_quad.end(), nq, c);
     ch.first_meas = (int)tab_meas.size();
     ch.meas = measure_layout(g);
     ch.nb_meas = ch.meas.nb_plaq + ch.meas.nb_poly;
@@ -247,6 +284,7 @@ extern "C" int u1_batch_create(u1_ctx *ctx, int nchains, const u1_geom *geoms, u
   b->nb_pair = (int)tab_pair.size();
   b->nb_site = (int)tab_site.size();
   b->nb_meas = (int)tab_meas.size();
+  b->nb_quad = (int)tab_quad.size();
   {
     // groups of at most U1_BATCH_GROUP_MB (default 64) MiB of links; a
     // single chain may exceed it; 0 puts every chain in one group
@@ -255,13 +293,20 @@ extern "C" int u1_batch_create(u1_ctx *ctx, int nchains, const u1_geom *geoms, u
       const long long mb = std::atoll(env);
       kGroupBytes = mb > 0 ? (size_t)mb << 20 : SIZE_MAX;
     }
+    // U1_BATCH_QUAD=0 keeps every group on the two-site (or one-site) kernel
+    const char *qenv = std::getenv("U1_BATCH_QUAD");
+    const bool quad_enabled = !(qenv && qenv[0] == '0');
     size_t bytes = 0;
     int c0 = 0;
     auto close_group = [&](int c1) {
       const BatchChain &a = b->h_chains[c0];
       const int pair_end = c1 < nchains ? b->h_chains[c1].first_pair : b->nb_pair;
       const int site_end = c1 < nchains ? b->h_chains[c1].first_site : b->nb_site;
-      b->groups.push_back({a.first_pair, pair_end - a.first_pair, a.first_site, site_end - a.first_site});
+      bool quad = quad_enabled;
+      for (int c = c0; c < c1; ++c) quad = quad && (b->h_chains[c].g.hN0 & 3) == 0;
+      const int quad_end = c1 < nchains ? b->h_chains[c1].first_quad : b->nb_quad;
+      b->groups.push_back({a.first_pair, pair_end - a.first_pair, a.first_site, site_end - a.first_site,
+                           a.first_quad, quad ? quad_end - a.first_quad : 0});
     };
     for (int c = 0; c < nchains; ++c) {
       const size_t cb = (size_t)b->h_chains[c].g.V * b->h_chains[c].g.dims * sizeof(float2);
@@ -281,6 +326,7 @@ extern "C" int u1_batch_create(u1_ctx *ctx, int nchains, const u1_geom *geoms, u
   if (e == cudaSuccess) e = cudaMalloc(&b->d_tab_pair, sizeof(int) * tab_pair.size());
   if (e == cudaSuccess) e = cudaMalloc(&b->d_tab_site, sizeof(int) * tab_site.size());
   if (e == cudaSuccess) e = cudaMalloc(&b->d_tab_meas, sizeof(int) * tab_meas.size());
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_tab_quad, sizeof(int) * std::max<size_t>(1, tab_quad.size()));
   if (e == cudaSuccess) e = cudaMalloc(&b->partials, sizeof(double) * 6 * tab_meas.size());
   if (e == cudaSuccess) e = cudaMalloc(&b->d_out, sizeof(double) * 6 * nchains);
   if (e == cudaSuccess) e = cudaMallocHost(&b->h_out, sizeof(double) * 6 * nchains);
@@ -297,6 +343,8 @@ extern "C" int u1_batch_create(u1_ctx *ctx, int nchains, const u1_geom *geoms, u
     e = cudaMemcpy(b->d_tab_pair, tab_pair.data(), sizeof(int) * tab_pair.size(), cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
     e = cudaMemcpy(b->d_tab_site, tab_site.data(), sizeof(int) * tab_site.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !tab_quad.empty())
+    e = cudaMemcpy(b->d_tab_quad, tab_quad.data(), sizeof(int) * tab_quad.size(), cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
     e = cudaMemcpy(b->d_tab_meas, tab_meas.data(), sizeof(int) * tab_meas.size(), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
@@ -354,9 +402,29 @@ extern "C" int u1_batch_hot_start(u1_batch *b) {
   return U1_OK;
 }
 
+template <int D, int MU, bool MET>
+static int batch_launch_quad(u1_batch *b, BatchPhase ph, int group) {
+  const std::array<int, 6> &gr = b->groups[group];
+  ph.block_base = gr[4];
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)gr[5]);
+  cfg.blockDim = dim3(128);
+  cfg.stream = b->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaError_t e = cudaLaunchKernelEx(&cfg, k_batch_update_quad<D, MU, MET>, (const BatchChain *)b->d_chains,
+                                     (const int *)b->d_tab_quad, ph);
+  u1i::g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (e != cudaSuccess) return cuda_fail(e, "k_batch_update_quad");
+  return U1_OK;
+}
+
 template <int D, int MU, bool MET, bool PAIR>
 static int batch_launch(u1_batch *b, BatchPhase ph, int group) {
-  const std::array<int, 4> &gr = b->groups[group];
+  const std::array<int, 6> &gr = b->groups[group];
   ph.block_base = PAIR ? gr[0] : gr[2];
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(PAIR ? gr[1] : gr[3]));
@@ -376,6 +444,8 @@ static int batch_launch(u1_batch *b, BatchPhase ph, int group) {
 
 template <int D, int MU>
 static int batch_launch_mu(u1_batch *b, const BatchPhase &ph, bool met, int group) {
+  if (b->groups[group][5] > 0)
+    return met ? batch_launch_quad<D, MU, true>(b, ph, group) : batch_launch_quad<D, MU, false>(b, ph, group);
   if (b->pair_ok)
     return met ? batch_launch<D, MU, true, true>(b, ph, group) : batch_launch<D, MU, false, true>(b, ph, group);
   return met ? batch_launch<D, MU, true, false>(b, ph, group) : batch_launch<D, MU, false, false>(b, ph, group);
