@@ -562,6 +562,16 @@ static int launch_phase(const UpdArgs &a, cudaStream_t s, bool met, int src, int
   return fail(U1_ERR_INVALID, "k_update: direction out of range");
 }
 
+// SM count for the block-order remap of the phase kernels (sm_local_block);
+// U1_REMAP=0 in the environment keeps the launch order.
+static int sm_remap(const u1_lattice *lat) {
+  static const bool off = [] {
+    const char *r = std::getenv("U1_REMAP");
+    return r && r[0] == '0';
+  }();
+  return off ? 0 : lat->ctx->prop.multiProcessorCount;
+}
+
 // The proposal settings of `lat` into the kernel arguments.
 static void set_proposal(UpdArgs &a, const u1_lattice *lat) {
   a.win = lat->win;
@@ -769,6 +779,7 @@ static int issue_sweep(u1_lattice *lat, float2 *links, u1_rng *rng, int metrop, 
   a.replay_base = rng->replay_base;
   a.ml = ml;
   set_proposal(a, lat);
+  a.sms = sm_remap(lat);
   const int src = metropolis_src(lat, rng);
   const int var = sweep_variant(lat, src, ml);
   if (var == U1V_WAVE) return launch_wave(lat, links, rng, metrop, ovrn, meas_partials);
@@ -1145,6 +1156,7 @@ extern "C" int u1_update_phase(u1_lattice *lat, u1_rng *rng, int metropolis, int
   a.replay = rng->replay_dev;
   a.replay_base = rng->replay_base;
   set_proposal(a, lat);
+  a.sms = sm_remap(lat);
   const int src = metropolis_src(lat, rng);
   const int var = sweep_variant(lat, src, 0);
   switch (lat->g.dims) {

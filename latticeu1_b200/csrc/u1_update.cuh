@@ -106,7 +106,21 @@ struct UpdArgs {
   int ml;                              // multilevel freeze period (0 = none)
   float win;                           // SRC_WINDOW: proposal half-width / pi (0: whole circle)
   int nhits;                           // SRC_WINDOW: Metropolis hits per link and pass
+  int sms;                             // k_update_quad: > 0 remaps the block order over this many SMs
 };
+
+// Work item of launch-order block b of G when the blocks of a single wave
+// are handed to S SMs round-robin: the blocks that share SM s (b = s, s+S,
+// s+2S, ...) get consecutive items, so neighbouring x2-planes of the
+// lattice meet in the same SM's L1.  A bijection of [0, G) for any G, S.
+// Measured on B200 at 32^4: 1.7 % faster for the four-site kernel, 2.5 %
+// slower for the two-site kernel, which therefore keeps the launch order.
+__device__ __forceinline__ int sm_local_block(int b, int G, int S) {
+  if (S <= 0) return b;
+  const int q = G / S, rem = G - q * S;
+  const int s = b % S, r = b / S;
+  return s * q + min(s, rem) + r;
+}
 
 // Where a Metropolis kernel takes its proposals from.
 enum : int {
@@ -525,7 +539,8 @@ __device__ __forceinline__ void update_quad_body(const UpdArgs a, int i) {
 // of 72, so 7 CTAs fit an SM (a 32^4 phase, 1024 CTAs, is then a single wave).
 template <int D, int MU, bool MET, int SRC>
 __global__ void __launch_bounds__(128, 7) k_update_quad(const UpdArgs a) {
-  update_quad_body<D, MU, MET, SRC>(a, 4 * (blockIdx.x * blockDim.x + threadIdx.x));
+  const int b = sm_local_block((int)blockIdx.x, (int)gridDim.x, a.sms);
+  update_quad_body<D, MU, MET, SRC>(a, 4 * (b * (int)blockDim.x + (int)threadIdx.x));
 }
 
 // Two sites per thread, register budget capped at 32 so 8 CTAs of 256
