@@ -679,10 +679,11 @@ static int sweep_variant(const u1_lattice *lat, int src, int ml) {
 // Phase (1, MU) of the last pass with the measurement terms (u1_fused.cuh),
 // writing the per-block partials of slot MU-1 into `partials`.
 template <int D, int MU>
-static int launch_meas_phase_mu(const UpdArgs &a, cudaStream_t s, bool met, bool win, double *partials) {
+static int launch_meas_phase_mu(const UpdArgs &a, cudaStream_t s, bool met, bool win, bool quad,
+                                double *partials) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)meas_phase_blocks(a.g));
-  cfg.blockDim = dim3(256);
+  cfg.blockDim = dim3(quad ? 128 : 256);  // quad: four sites per thread, the same 512 sites per block
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -691,7 +692,11 @@ static int launch_meas_phase_mu(const UpdArgs &a, cudaStream_t s, bool met, bool
   cfg.numAttrs = 1;
   double *slot = partials + (size_t)(MU - 1) * meas_phase_blocks(a.g) * 2;
   cudaError_t e;
-  if ((a.g.hN0 & 1) == 0)
+  if (quad)
+    e = !met ? cudaLaunchKernelEx(&cfg, k_update_quad_meas<D, MU, false>, a, slot)
+        : win ? cudaLaunchKernelEx(&cfg, k_update_quad_meas<D, MU, true, SRC_WINDOW>, a, slot)
+              : cudaLaunchKernelEx(&cfg, k_update_quad_meas<D, MU, true>, a, slot);
+  else if ((a.g.hN0 & 1) == 0)
     e = !met ? cudaLaunchKernelEx(&cfg, k_update_pair_meas<D, MU, false>, a, slot)
         : win ? cudaLaunchKernelEx(&cfg, k_update_pair_meas<D, MU, true, SRC_WINDOW>, a, slot)
               : cudaLaunchKernelEx(&cfg, k_update_pair_meas<D, MU, true>, a, slot);
@@ -705,14 +710,14 @@ static int launch_meas_phase_mu(const UpdArgs &a, cudaStream_t s, bool met, bool
 }
 
 template <int D>
-static int launch_meas_phase(const UpdArgs &a, cudaStream_t s, bool met, bool win, double *partials) {
+static int launch_meas_phase(const UpdArgs &a, cudaStream_t s, bool met, bool win, bool quad, double *partials) {
   switch (a.mu) {
-    case 1: return launch_meas_phase_mu<D, 1>(a, s, met, win, partials);
+    case 1: return launch_meas_phase_mu<D, 1>(a, s, met, win, quad, partials);
     case 2:
-      if constexpr (D > 2) return launch_meas_phase_mu<D, 2>(a, s, met, win, partials);
+      if constexpr (D > 2) return launch_meas_phase_mu<D, 2>(a, s, met, win, quad, partials);
       break;
     case 3:
-      if constexpr (D > 3) return launch_meas_phase_mu<D, 3>(a, s, met, win, partials);
+      if constexpr (D > 3) return launch_meas_phase_mu<D, 3>(a, s, met, win, quad, partials);
       break;
   }
   return fail(U1_ERR_INVALID, "measuring phase: direction out of range");
@@ -790,9 +795,9 @@ static int issue_sweep(u1_lattice *lat, float2 *links, u1_rng *rng, int metrop, 
     ++phase;
     // the last pass is phases total-2D+1 .. total; its parity-1 half with mu >= 1 measures
     if (meas_partials && phase > total - 2 * D && a.p == 1 && a.mu >= 1)
-      return D == 2 ? launch_meas_phase<2>(a, lat->stream, met, src == SRC_WINDOW, meas_partials)
-           : D == 3 ? launch_meas_phase<3>(a, lat->stream, met, src == SRC_WINDOW, meas_partials)
-                    : launch_meas_phase<4>(a, lat->stream, met, src == SRC_WINDOW, meas_partials);
+      return D == 2 ? launch_meas_phase<2>(a, lat->stream, met, src == SRC_WINDOW, var == U1V_QUAD, meas_partials)
+           : D == 3 ? launch_meas_phase<3>(a, lat->stream, met, src == SRC_WINDOW, var == U1V_QUAD, meas_partials)
+                    : launch_meas_phase<4>(a, lat->stream, met, src == SRC_WINDOW, var == U1V_QUAD, meas_partials);
     return D == 2 ? launch_phase<2>(a, lat->stream, met, src, var, lat->block)
          : D == 3 ? launch_phase<3>(a, lat->stream, met, src, var, lat->block)
                   : launch_phase<4>(a, lat->stream, met, src, var, lat->block);

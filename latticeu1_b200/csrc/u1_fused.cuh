@@ -37,6 +37,19 @@ static __global__ void __launch_bounds__(256) k_update_meas(const UpdArgs a, dou
   if (threadIdx.x < 2) partials[2 * blockIdx.x + threadIdx.x] = v[0];
 }
 
+// Four sites per thread, 128 threads (512 sites) per block: the same blocks
+// and partial slots as k_update_pair_meas.
+template <int D, int MU, bool MET, int SRC = SRC_PHILOX>
+static __global__ void __launch_bounds__(128, 7) k_update_quad_meas(const UpdArgs a, double *partials) {
+  __shared__ double smem[kRedWarps * 2];
+  float2 m = make_float2(0.f, 0.f);
+  const int b = sm_local_block((int)blockIdx.x, (int)gridDim.x, a.sms);
+  update_quad_body<D, MU, MET, SRC, true>(a, 4 * (b * (int)blockDim.x + (int)threadIdx.x), &m);
+  double v[2] = {(double)m.x, (double)m.y};
+  block_sum<2>(v, smem);
+  if (threadIdx.x < 2) partials[2 * blockIdx.x + threadIdx.x] = v[0];
+}
+
 // Blocks of one measuring phase (pair kernels when N0/2 is even).
 __host__ inline int meas_phase_blocks(const GeomK &g) {
   const int threads = (g.hN0 & 1) ? g.Vh : g.Vh / 2;

@@ -458,13 +458,15 @@ __device__ __forceinline__ Quad2 ld_shifted(const float2 *base, int i, const int
 // Body of the four-sites-per-thread update for EO sites i..i+3 (i a multiple
 // of 4) of the phase (a.p, MU); every site's staple and update use the same
 // operations in the same order as the other bodies (bit-identical links).
-template <int D, int MU, bool MET, int SRC>
-__device__ __forceinline__ void update_quad_body(const UpdArgs a, int i) {
+// MEAS: also add the plaquettes (nu < MU, MU) of the four sites from their
+// staple terms into *meas (as update_pair_body).
+template <int D, int MU, bool MET, int SRC, bool MEAS = false>
+__device__ __forceinline__ void update_quad_body(const UpdArgs a, int i, float2 *meas = nullptr) {
   int x[4], k;
   eo_decode_fast<D>(a.g, i, a.p, x, k);
   phase_entry<MET>(a);
   if (i >= a.g.Vh) return;
-  if (MU != 3 && a.ml > 0 && (x[D - 1] & (a.ml - 1)) == 0) return;  // freeze rule, src/multilevel.cu:41
+  if (!MEAS && MU != 3 && a.ml > 0 && (x[D - 1] & (a.ml - 1)) == 0) return;  // freeze rule, src/multilevel.cu:41
   int fwd[4], bwd[4];
   eo_steps<D>(a.g, x, k, fwd, bwd);  // steps of site i; sites i+1..i+3 share those along x1..x3
   const int odd = x[0] & 1;
@@ -478,9 +480,9 @@ __device__ __forceinline__ void update_quad_body(const UpdArgs a, int i) {
   const int V = a.g.V, Vh = a.g.Vh;
   const float2 *lat = a.lat;
   const float2 *Lq_mu = lat + MU * V + q * Vh;
-  float2 ss[4], st[4];
+  float2 ss[4], st[4], mA[4], mD[4];  // mA, mD: measurement sums (MEAS), see update_single_body
 #pragma unroll
-  for (int s = 0; s < 4; ++s) ss[s] = st[s] = make_float2(0.f, 0.f);
+  for (int s = 0; s < 4; ++s) ss[s] = st[s] = mA[s] = mD[s] = make_float2(0.f, 0.f);
 #pragma unroll
   for (int nu = 0; nu < D; ++nu) {
     if (nu == MU) continue;
@@ -509,12 +511,16 @@ __device__ __forceinline__ void update_quad_body(const UpdArgs a, int i) {
     }
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
-      const float2 t =
-          cadd(cmulc(cmulc(A.s[s], B.s[s]), C.s[s]), cmul(cconjmul(Dd.s[s], E.s[s]), F.s[s]));
+      const float2 up = cmulc(cmulc(A.s[s], B.s[s]), C.s[s]), lo = cmul(cconjmul(Dd.s[s], E.s[s]), F.s[s]);
+      const float2 t = cadd(up, lo);
       if (MU == D - 1 || nu == D - 1)
         st[s] = cadd(st[s], t);
       else
         ss[s] = cadd(ss[s], t);
+      if (MEAS && nu < MU) {
+        if (MU != D - 1) mA[s] = cadd(mA[s], t);  // for MU = D-1 every nu < MU term is in st
+        mD[s] = cadd(mD[s], csub(up, lo));
+      }
     }
   }
   float2 *own = a.lat + MU * V + a.p * Vh + i;
@@ -533,6 +539,15 @@ __device__ __forceinline__ void update_quad_body(const UpdArgs a, int i) {
                                        s < 2 ? &blk0 : &blk1);
   st_quad(own, N);
   pdl_release_dependents();
+  if (MEAS) {
+    float re = 8.f * MU, im = 0.f;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      re -= cre_mul((MU == D - 1) ? st[s] : mA[s], N[s]);
+      im += cim_mul(mD[s], N[s]);
+    }
+    *meas = make_float2(re, im);
+  }
 }
 
 // Four sites per thread, at most 128 threads per block and a register budget

@@ -357,13 +357,20 @@ def test_errors_are_status_codes(ctx):
 
 @pytest.mark.parametrize("dims,N,beta,aniso,metrop,ovrn", [(4, (8, 8, 8, 8), 1.0, 1.0, 1, 4), (4, (6, 4, 4, 12), 0.9, 1.5, 1, 2),
                                                            (4, (8, 6, 6, 8), 1.1, 1.0, 2, 0), (3, (8, 6, 0, 10), 2.0, 1.0, 1, 3),
-                                                           (2, (16, 0, 0, 6), 3.0, 1.0, 1, 1)])
-def test_fused_measurement_sweep(ctx, dims, N, beta, aniso, metrop, ovrn):
+                                                           (2, (16, 0, 0, 6), 3.0, 1.0, 1, 1),
+                                                           (4, (16, 8, 6, 8), 1.05, 1.3, 1, 2)])
+@pytest.mark.parametrize("variant", [0, 5])
+def test_fused_measurement_sweep(ctx, dims, N, beta, aniso, metrop, ovrn, variant):
     """u1_update_measure: links bit-identical to u1_update, observables equal
-    to u1_measure of the same configuration within the FP32 tolerance."""
+    to u1_measure of the same configuration within the FP32 tolerance
+    (variant 0: tuned; 5: four sites per thread, measuring phases included)."""
     import torch
+    if variant == 5 and (N[0] // 2) % 4:
+        pytest.skip("four sites per thread need N0/2 a multiple of 4")
     a = Lattice(ctx, dims, N, beta, aniso)
     b = Lattice(ctx, dims, N, beta, aniso)
+    if variant:
+        a.set_variant(variant)
     ra, rb = Rng(ctx, 17), Rng(ctx, 17)
     a.hot_start(ra)
     b.hot_start(rb)
