@@ -606,6 +606,90 @@ def run_batched(args) -> None:
     b.close()
 
 
+def run_kernels(args) -> None:
+    """The library's other kernels, one line of evidence each: every entry is
+    one public call, timed with CUDA events over args.steps calls after
+    args.warmup untimed ones (synchronous calls include their small result
+    copies), with its algorithmic bytes (each input and output array once)
+    and the fraction of the measured HBM bandwidth that implies.  32^4 at
+    beta = 1 unless stated; the ncu summary of the same command gives each
+    kernel's own duration and DRAM bytes."""
+    import numpy as np
+    import torch
+
+    from latticeu1_b200 import Context, Lattice, Rng, launch_count
+    from latticeu1_b200.action import WilsonAction
+    from latticeu1_b200.lattice import convert_order
+    ctx = Context(0)
+    stream = torch.cuda.Stream()
+    peak, peak_kind = measured_peak()
+    N = (32, 32, 32, 32)
+    V = volume(N)
+    lat = Lattice(ctx, 4, N, 1.0)
+    lat.set_stream(stream.cuda_stream)
+    rng = Rng(ctx, 77)
+    Vs, R = V // N[3], N[0] // 2
+    nl = lat.nlinks
+    rows = []
+
+    def timed(name, kernels, fn, alg_bytes, note=""):
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                fn()
+            torch.cuda.synchronize()
+            ts = []
+            for _ in range(args.steps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ts.append(e0.elapsed_time(e1) * 1e3)
+        us = float(np.median(ts))
+        gbs = alg_bytes / (us * 1e-6) / 1e9
+        rows.append({"call": name, "kernels": kernels, "us_median": us, "algorithmic_bytes": int(alg_bytes),
+                     "achieved_gbs": gbs, "frac_of_peak": gbs / peak, **({"note": note} if note else {})})
+
+    n0 = launch_count()
+    lat.hot_start(rng)
+    timed("u1_hot_start", "k_hot_start", lambda: lat.hot_start(rng), 8 * nl, "writes every link")
+    for _ in range(20):
+        lat.update(rng, 1, 4)
+    timed("u1_measure (plaquette + Polyakov)", "k_measure", lambda: lat.measure(), 8 * nl,
+          "reads every link once; 48 B result copy")
+    timed("u1_poly_corr(multihit=0)", "k_poly_field<4,0>, k_poly_corr", lambda: lat.poly_corr(False),
+          8 * V + 16 * Vs, "temporal links, then the P field")
+    timed("u1_poly_corr(multihit=1)", "k_poly_field<4,1>, k_poly_corr", lambda: lat.poly_corr(True),
+          8 * nl + 16 * Vs, "every link (staples of the temporal links), then the P field")
+    th = torch.empty(nl, dtype=torch.float64, device="cuda")
+    timed("u1_lattice_export_angles (device FP64)", "k_export_angles", lambda: lat.export_angles(th), 16 * nl)
+    timed("u1_lattice_import_angles (device FP64)", "k_import_angles", lambda: lat.import_angles(th), 16 * nl)
+    timed("u1_convert_order (EO -> NO, FP64)", "k_convert_order<1>", lambda: convert_order(th, 4, N, True),
+          16 * nl)
+    timed("u1_plaquette_fields (space-time)", "k_plaquette_fields<1>", lambda: lat.plaquette_fields(True),
+          8 * nl + 96 * V, "reads every link, writes 6 complex FP64 per site")
+    S4 = WilsonAction(4, N, 1.0)
+    t4 = th.to(torch.float32).reshape(1, -1)
+    timed("u1_wilson_action (4D 32^4, float32, batch 1)", "k_action<4,float>, k_action_finish",
+          lambda: S4(t4), 4 * nl)
+    t4g = t4.clone().requires_grad_(True)
+    timed("u1_wilson_action + u1_wilson_action_grad (4D 32^4)", "k_action, k_action_grad<4,float>",
+          lambda: S4(t4g).sum().backward(), 4 * nl * 3, "action reads theta; adjoint reads theta, writes grad")
+    L2d, B2d = 32, 1024
+    S2 = WilsonAction(2, (L2d, 0, 0, L2d), 6.0)
+    t2 = torch.rand((B2d, 2 * L2d * L2d), device="cuda") * 6.2831853
+    timed("u1_wilson_action (2D 32^2, float32, batch 1024)", "k_action<2,float>, k_action_finish",
+          lambda: S2(t2), 4 * t2.numel())
+    launches = launch_count() - n0
+    line = {"metric": "per-call device time and algorithmic bandwidth of the non-update kernels",
+            "value": None, "unit": "GB/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "data": "synthetic", "dtype": "f32/f64",
+            "config": {"workload": "kernels: one public call per entry, 32^4 beta = 1 after 20 sweeps unless stated"},
+            "peak_gbs": peak, "peak_kind": peak_kind, "gpu_launches": int(launches), "entries": rows}
+    print(json.dumps(line), flush=True)
+    lat.close()
+
+
 def geometry(args):
     """(N, beta, aniso) of the update workload: --geom Nx,Ny,Nz,Nt or --L for L^4."""
     if args.geom:
@@ -635,7 +719,7 @@ def main() -> None:
     ap.add_argument("--block", type=int, default=256, help="threads per block with --variant")
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU baseline sampling")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["update32", "multilevel", "batched"], default="update32")
+    ap.add_argument("--workload", choices=["update32", "multilevel", "batched", "kernels"], default="update32")
     ap.add_argument("--n2", type=int, default=200, help="level-2 sub-updates per step (multilevel)")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -646,6 +730,8 @@ def main() -> None:
         run_multilevel(args)
     elif args.workload == "batched":
         run_batched(args)
+    elif args.workload == "kernels":
+        run_kernels(args)
     else:
         run_ours(args)
 

@@ -44,9 +44,11 @@ __device__ __forceinline__ int spatial_shift(const GeomK &g, const int x[4], int
 }
 
 // T2[x, r, i, slab] += prod_{t in slab} mh(x,t) * prod_{t in slab} conj(mh(x + r e_i, t)),
-// slabs of thickness 2.  One thread per (x, r, i).
+// slabs of thickness 2.  One thread per (x, r, i).  T2 does not alias mh,
+// and the slabs' read-modify-writes touch distinct elements, so four of
+// them are unrolled with their loads in flight together.
 static __global__ void __launch_bounds__(256)
-    k_ml_T2(const float2 *__restrict__ mh, GeomK g, int R, double2 *T2) {
+    k_ml_T2(const float2 *__restrict__ mh, GeomK g, int R, double2 *__restrict__ T2) {
   const size_t size = (size_t)g.Vs * R * g.tdir;
   const size_t id = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= size) return;
@@ -58,6 +60,7 @@ static __global__ void __launch_bounds__(256)
   spatial_decode(g, s, x);
   const int sp = spatial_shift(g, x, dir, r);
   const int nl2 = g.N[g.tdir] / 2;
+#pragma unroll 4
   for (int l = 0; l < nl2; ++l) {
     double2 p0 = make_double2(1.0, 0.0), p1 = make_double2(1.0, 0.0);
 #pragma unroll
