@@ -94,41 +94,48 @@ __global__ void __launch_bounds__(kRedThreads)
   double v[12];
 #pragma unroll
   for (int k = 0; k < 12; ++k) v[k] = 0.0;
+  // Thread t owns natural-order site t (spacetime) or spatial site t (time
+  // averages), so a warp writes 32 consecutive FP64 complex values of each
+  // component (coalesced) and reads the links of both parities in two
+  // contiguous runs.
   if (SPACETIME) {
     if (t < g.V) {
-      const int p = t >= g.Vh ? 1 : 0;
-      const int i = t - p * g.Vh;
+      int x[4];
+      int r = t;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        x[k] = r % g.N[k];
+        r /= g.N[k];
+      }
+      const int p = (x[0] + x[1] + x[2] + x[3]) & 1;
       float2 c[6];
 #pragma unroll
       for (int d = 0; d < 6; ++d) c[d] = make_float2(0.f, 0.f);
-      six_plaquettes(lat, g, i, p, c);
-      int x[4], k;
-      eo_decode_fast<4>(g, i, p, x, k);
-      const int lex = x[0] + g.N[0] * (x[1] + g.N[1] * (x[2] + g.N[2] * x[3]));
+      six_plaquettes(lat, g, eo_index(g, x), p, c);
 #pragma unroll
       for (int d = 0; d < 6; ++d) {
-        field[(size_t)d * g.V + lex] = make_double2(c[d].x, c[d].y);
+        field[(size_t)d * g.V + t] = make_double2(c[d].x, c[d].y);
         v[2 * d] = c[d].x;
         v[2 * d + 1] = c[d].y;
       }
     }
   } else if (t < g.Vs) {
-    // t = spatial EO index + parity * V_s/2 on the t = 0 slice
-    const int hs = g.Vs / 2;
-    const int p0 = t >= hs ? 1 : 0;
-    const int i0 = t - p0 * hs;
+    int x[4];
+    x[0] = t % g.N[0];
+    x[1] = (t / g.N[0]) % g.N[1];
+    x[2] = t / (g.N[0] * g.N[1]);
+    x[3] = 0;
+    const int p0 = (x[0] + x[1] + x[2]) & 1;
+    const int i0 = eo_index(g, x);  // the site on the t = 0 slice; (x, tt) is i0 + tt * es[3]
     float2 c[6];
 #pragma unroll
     for (int d = 0; d < 6; ++d) c[d] = make_float2(0.f, 0.f);
     for (int tt = 0; tt < g.N[3]; ++tt) six_plaquettes(lat, g, i0 + tt * g.es[3], (p0 + tt) & 1, c);
-    int x[4], k;
-    eo_decode_fast<4>(g, i0, p0, x, k);
-    const int lex = x[0] + g.N[0] * (x[1] + g.N[1] * x[2]);
     const double inv = 1.0 / g.N[3];
 #pragma unroll
     for (int d = 0; d < 6; ++d) {
       const double2 m = make_double2(c[d].x * inv, c[d].y * inv);
-      field[(size_t)d * g.Vs + lex] = m;
+      field[(size_t)d * g.Vs + t] = m;
       v[2 * d] = m.x;
       v[2 * d + 1] = m.y;
     }
