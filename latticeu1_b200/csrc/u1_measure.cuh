@@ -251,8 +251,18 @@ __device__ __forceinline__ void measure_block_values(const float2 *__restrict__ 
     const int est = g.es[D - 1];
     const float2 *base = lat + (D - 1) * g.V + i;
     const int t0 = c * Lc;
-#pragma unroll 8
-    for (int t = t0; t < t0 + Lc; ++t) L = cmul(L, __ldg(base + ((p + t) & 1) * g.Vh + t * est));
+    // eight loads in flight, then their products in time order (a padded
+    // factor is 1 + 0i, which leaves the product bit for bit unchanged)
+    for (int tb = t0; tb < t0 + Lc; tb += 8) {
+      float2 u[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int t = tb + k;
+        u[k] = (t < t0 + Lc) ? __ldg(base + ((p + t) & 1) * g.Vh + t * est) : make_float2(1.f, 0.f);
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) L = cmul(L, u[k]);
+    }
   }
   lp[threadIdx.x] = L;
   __syncthreads();
