@@ -155,6 +155,35 @@ def test_five_sweeps_every_phase_shared_stream(ctx, dims, N, beta, aniso, start)
     assert np.mean(or_err < ANGLE_TOL) > (0.98 if start == "hot" else 0.995), np.mean(or_err < ANGLE_TOL)
 
 
+@pytest.mark.parametrize("dims,N,beta,aniso", [(4, (8, 8, 8, 8), 1.0, 1.0), (4, (16, 4, 6, 8), 1.1, 2.0),
+                                                (3, (8, 6, 0, 8), 2.0, 1.5), (2, (16, 0, 0, 8), 4.0, 1.0)])
+def test_quad_kernel_phases_vs_oracle(ctx, dims, N, beta, aniso):
+    """The four-sites-per-thread kernel (variant 5) phase by phase against
+    the FP64 oracle: replayed and Philox Metropolis phases, overrelaxation
+    phases, each from the GPU's own configuration."""
+    lat, o = _pair(ctx, dims, N, beta, aniso)
+    lat.set_variant(5)
+    rng = Rng(ctx, 8)
+    lat.hot_start(rng)
+    for _ in range(10):
+        lat.update(rng, 1, 4)
+    D, Vh = lat.dims, lat.Vh
+    flips = 0
+    seed, p0 = rng.state
+    for p in (0, 1):
+        for mu in range(D):
+            flips += check_phase(lat, o, rng, True, p, mu, seed=seed, pass_=p0)[0]
+    rs = np.random.default_rng(5)
+    pairs = np.stack([rs.uniform(0, 2 * np.pi, lat.nlinks), rs.uniform(0, 1, lat.nlinks)], -1)
+    rng.set_replay(pairs)
+    for p in (0, 1):
+        for mu in range(D):
+            k0 = (p * D + mu) * Vh
+            flips += check_phase(lat, o, rng, True, p, mu, pairs=pairs[k0:k0 + Vh])[0]
+            check_phase(lat, o, rng, False, p, mu)
+    assert flips <= 2, flips
+
+
 @pytest.mark.parametrize("dims,N,beta", [(4, (8, 8, 8, 8), 1.0), (4, (6, 4, 4, 12), 0.9), (3, (8, 6, 0, 8), 2.0)])
 def test_philox_phases_vs_oracle(ctx, dims, N, beta):
     """Production (Philox) Metropolis: GPU and oracle draw the same numbers

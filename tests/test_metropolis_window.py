@@ -98,7 +98,7 @@ def test_window_variants_graphs_and_fused_measurement_bit_identical(ctx):
     from latticeu1_b200 import Lattice, Rng
     geom = (4, (8, 8, 8, 8), 1.0)
     ref = None
-    for variant, graphs in [(1, True), (2, True), (3, True), (1, False)]:
+    for variant, graphs in [(1, True), (2, True), (3, True), (5, True), (1, False)]:
         lat = Lattice(ctx, *geom)
         lat.set_variant(variant)
         lat.set_graphs(graphs)
