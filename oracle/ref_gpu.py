@@ -13,7 +13,6 @@ tasks: measure | or_pass | poly2 | multilevel | multilevel_timing | timing | cha
 from __future__ import annotations
 
 import ctypes as C
-import json
 import subprocess
 import sys
 import tempfile

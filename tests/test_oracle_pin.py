@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 from scipy import special
 
-from oracle.oracle import Oracle, Ref, wrap_diff
+from oracle.oracle import Oracle, Ref
 from tests.conftest import GOLDEN_NAMES, load_golden
 
 
