@@ -102,8 +102,13 @@ __global__ void __launch_bounds__(kRedThreads)
   if (threadIdx.x == 1) out[b * 2 + 1] = w[0] * 0.15915494309189533577;  // 1/(2 pi)
 }
 
-// Thread per link t = mu*V + parity*V/2 + eo.
-// grad = scale * beta * sum_{nu != mu} w [sin theta_{mu nu}(x) - sin theta_{mu nu}(x - nu)].
+// Thread per site r = parity*V/2 + eo, computing the gradients of its d
+// links (x, mu):
+//   grad = scale * beta * sum_{nu != mu} w [sin theta_{mu nu}(x) - sin theta_{mu nu}(x - nu)].
+// Each forward plaquette theta_{mu nu}(x), mu < nu, is evaluated once and
+// enters link (x, mu) with + and link (x, nu) with - (theta_{nu mu} =
+// -theta_{mu nu}); the backward plaquettes theta_{mu nu}(x - nu) are per
+// link.  d(d-1)/2 + d(d-1) sines per site instead of 2(d-1) per link.
 template <int D, typename T>
 __global__ void __launch_bounds__(kActThreads)
     k_action_grad(const T *__restrict__ theta, GeomK g, T beta, T w_ss, T w_st, const double *__restrict__ scale,
@@ -111,10 +116,8 @@ __global__ void __launch_bounds__(kActThreads)
   const int b = blockIdx.y;
   const size_t n = (size_t)g.V * D;
   const T *th = theta + (size_t)b * n;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (int)n) return;
-  const int mu = t / g.V;
-  const int r = t - mu * g.V;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= g.V) return;
   const int p = r >= g.Vh ? 1 : 0;
   const int i = r - p * g.Vh;
   const int q = 1 - p;
@@ -122,24 +125,36 @@ __global__ void __launch_bounds__(kActThreads)
   eo_decode_fast<D>(g, i, p, x, k);
   int fwd[4], bwd[4];
   eo_steps<D>(g, x, k, fwd, bwd);
-  const T own = th[t];
-  T acc = 0;
+  T own[D], acc[D];
 #pragma unroll
-  for (int nu = 0; nu < D; ++nu) {
-    if (nu == mu) continue;
-    const T w = (mu == D - 1 || nu == D - 1) ? w_st : w_ss;
-    // theta_{mu nu}(x) = theta_mu(x) + theta_nu(x+mu) - theta_mu(x+nu) - theta_nu(x)
-    const T a = th[nu * g.V + q * g.Vh + i + fwd[mu]];
-    const T bb = th[mu * g.V + q * g.Vh + i + fwd[nu]];
-    const T c = th[nu * g.V + p * g.Vh + i];
-    // theta_{mu nu}(x-nu) = theta_mu(x-nu) + theta_nu(x-nu+mu) - theta_mu(x) - theta_nu(x-nu)
-    const T d = th[mu * g.V + q * g.Vh + i + bwd[nu]];
-    const T e = th[nu * g.V + p * g.Vh + i + fwd[mu] + bwd[nu]];
-    const T f = th[nu * g.V + q * g.Vh + i + bwd[nu]];
-    acc += w * (dsin(own + a - bb - c) - dsin(d + e - own - f));
+  for (int mu = 0; mu < D; ++mu) {
+    own[mu] = th[mu * g.V + p * g.Vh + i];
+    acc[mu] = 0;
   }
-  const T s = scale ? (T)scale[b] : T(1);
-  grad[(size_t)b * n + t] = s * beta * acc;
+#pragma unroll
+  for (int mu = 0; mu < D; ++mu) {
+#pragma unroll
+    for (int nu = 0; nu < D; ++nu) {
+      if (nu == mu) continue;
+      const T w = (mu == D - 1 || nu == D - 1) ? w_st : w_ss;
+      if (mu < nu) {
+        // theta_{mu nu}(x) = theta_mu(x) + theta_nu(x+mu) - theta_mu(x+nu) - theta_nu(x)
+        const T a = th[nu * g.V + q * g.Vh + i + fwd[mu]];
+        const T bb = th[mu * g.V + q * g.Vh + i + fwd[nu]];
+        const T sf = w * dsin(own[mu] + a - bb - own[nu]);
+        acc[mu] += sf;
+        acc[nu] -= sf;
+      }
+      // theta_{mu nu}(x-nu) = theta_mu(x-nu) + theta_nu(x-nu+mu) - theta_mu(x) - theta_nu(x-nu)
+      const T d = th[mu * g.V + q * g.Vh + i + bwd[nu]];
+      const T e = th[nu * g.V + p * g.Vh + i + fwd[mu] + bwd[nu]];
+      const T f = th[nu * g.V + q * g.Vh + i + bwd[nu]];
+      acc[mu] -= w * dsin(d + e - own[mu] - f);
+    }
+  }
+  const T sc = scale ? (T)scale[b] : T(1);
+#pragma unroll
+  for (int mu = 0; mu < D; ++mu) grad[(size_t)b * n + mu * g.V + p * g.Vh + i] = sc * beta * acc[mu];
 }
 
 int afail(int code, const std::string &msg) {
@@ -174,8 +189,7 @@ int launch_action(const GeomK &g, const u1_geom *geom, const void *theta, int ba
 template <int D, typename T>
 int launch_grad(const GeomK &g, const u1_geom *geom, const void *theta, int batch, const double *scale, void *grad,
                 cudaStream_t s) {
-  const long long n = (long long)g.V * D;
-  const int nb = (int)((n + kActThreads - 1) / kActThreads);
+  const int nb = (int)(((long long)g.V + kActThreads - 1) / kActThreads);  // one thread per site
   k_action_grad<D, T><<<dim3(nb, batch), kActThreads, 0, s>>>(static_cast<const T *>(theta), g, (T)geom->beta,
                                                               (T)(1.0 / geom->aniso), (T)geom->aniso, scale,
                                                               static_cast<T *>(grad));
