@@ -1,0 +1,44 @@
+"""bench.py's host-side plumbing, without a GPU: the algorithmic-bytes model,
+the workload naming and the DRAM-traffic figures it reads from the committed
+ncu summaries (each tied to the kernel it was measured on)."""
+import importlib.util
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def _bench():
+    spec = importlib.util.spec_from_file_location("bench_module", ROOT / "bench.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def test_algorithmic_bytes_model():
+    b = _bench()
+    # read+write the updated link, the opposite-parity mu link and all (d-1) nu links of both parities
+    assert [b.algorithmic_bytes_per_link_update(d) for d in (2, 3, 4)] == [40, 56, 72]
+    N = (32, 32, 32, 32)
+    assert b.volume(N) == 32 ** 4
+    assert b.link_updates_per_step(N) == 32 ** 4 * 4 * 5  # 1 Metropolis + 4 OR passes
+
+
+def test_workload_names():
+    b = _bench()
+    assert "32^4" in b.metric_for((32, 32, 32, 32))
+    assert "24x24x24x48" in b.metric_for((24, 24, 24, 48))
+    cfg = b.workload_config((32, 32, 32, 32))
+    assert cfg["lattice"] == "32^4" and "metropolis" not in cfg
+    cfg = b.workload_config((32, 32, 32, 32), delta=1.5, nhits=3)
+    assert cfg["metropolis"] == {"delta": 1.5, "nhits": 3}
+
+
+def test_traffic_figures_follow_the_profiled_kernel():
+    b = _bench()
+    quad = b.ncu_traffic_per_launch((32, 32, 32, 32), "k_update_quad")
+    assert quad is not None and 0 < quad < 37.75e6  # L2-resident: far below the algorithmic bytes
+    assert b.ncu_traffic_per_launch((32, 32, 32, 32), "k_update_pair") is None
+    assert b.ncu_traffic_per_launch((48, 48, 48, 48), "k_update_quad") is None
+    per_link = b.ncu_batch_traffic_per_link_sweep()
+    assert per_link is not None and 0 < per_link < 72 * 5
+    assert b.KERNEL_OF_VARIANT[5] == "k_update_quad" and b.KERNEL_OF_VARIANT[1] == "k_update_pair"
