@@ -462,11 +462,10 @@ __device__ __forceinline__ Quad2 ld_shifted(const float2 *base, int i, const int
 // staple terms into *meas (as update_pair_body).
 template <int D, int MU, bool MET, int SRC, bool MEAS = false>
 __device__ __forceinline__ void update_quad_body(const UpdArgs a, int i, float2 *meas = nullptr) {
+  // site decode and neighbour steps (pure arithmetic) before the wait for
+  // the previous phase, overlapping its tail
   int x[4], k;
   eo_decode_fast<D>(a.g, i, a.p, x, k);
-  phase_entry<MET>(a);
-  if (i >= a.g.Vh) return;
-  if (!MEAS && MU != 3 && a.ml > 0 && (x[D - 1] & (a.ml - 1)) == 0) return;  // freeze rule, src/multilevel.cu:41
   int fwd[4], bwd[4];
   eo_steps<D>(a.g, x, k, fwd, bwd);  // steps of site i; sites i+1..i+3 share those along x1..x3
   const int odd = x[0] & 1;
@@ -476,6 +475,9 @@ __device__ __forceinline__ void update_quad_body(const UpdArgs a, int i, float2 
     f0[s] = odd ? ((s == 3 && k + 3 == a.g.hN0 - 1) ? a.g.wrapf[0] : 1) : 0;
     b0[s] = odd ? 0 : ((s == 0 && k == 0) ? a.g.wrapb[0] : -1);
   }
+  phase_entry<MET>(a);
+  if (i >= a.g.Vh) return;
+  if (!MEAS && MU != 3 && a.ml > 0 && (x[D - 1] & (a.ml - 1)) == 0) return;  // freeze rule, src/multilevel.cu:41
   const int q = 1 - a.p;
   const int V = a.g.V, Vh = a.g.Vh;
   const float2 *lat = a.lat;
