@@ -487,3 +487,21 @@ def test_multilevel_graphs_equal_direct(ctx):
         res.append((lat.multilevel(rng, 2, 1, 3, 1, 1, 2), rng.state))
     assert np.array_equal(res[0][0], res[1][0])
     assert res[0][1] == res[1][1]
+
+
+@pytest.mark.parametrize("N", [(8, 8, 8, 8), (16, 4, 4, 8)])
+def test_multilevel_variants_equal(ctx, N):
+    """Multilevel sub-updates (freeze rule) give the same C(r) bit for bit with
+    the one-, two- and four-site update kernels."""
+    res = []
+    for variant in (3, 1, 5):
+        lat = Lattice(ctx, 4, N, 1.0)
+        lat.set_variant(variant)
+        rng = Rng(ctx, 13)
+        lat.hot_start(rng)
+        lat.update(rng, 1, 2)
+        res.append((lat.multilevel(rng, 2, 1, 3, 1, 1, 2), rng.state, lat.export_angles()))
+    for c, st, th in res[1:]:
+        assert np.array_equal(c, res[0][0])
+        assert st == res[0][1]
+        assert np.array_equal(th, res[0][2])
