@@ -108,7 +108,7 @@ int u1_lattice_get_variant(const u1_lattice *lat, int *variant);
 int u1_lattice_set_metropolis(u1_lattice *lat, double delta, int nhits);
 int u1_lattice_get_metropolis(const u1_lattice *lat, double *delta, int *nhits);
 /* Replaces the reference's autotuner (tuneLaunch, src/tune.cpp:306-416):
- * times every valid variant (1, 2, 3, 5) at 64, 128 and 256 threads per block on a
+ * times every valid variant (1, 2, 3, 5) at 64, 96, 128, 192 and 256 threads per block (5: up to 128) on a
  * few sweeps of this lattice from a backed-up state (links and rng pass
  * restored afterwards), keeps the fastest pair and caches it per (device,
  * geometry); with U1_RESOURCE_PATH set the cache persists in

@@ -871,7 +871,9 @@ static bool block_valid(int threads) { return threads >= 32 && threads <= 256 &&
 // Replaces the reference's block-size search (src/tune.cpp:306-416,
 // include/tune.h:143-260): the candidates are the compiled update-kernel
 // variants (two sites per thread with a 32-register cap, two sites
-// uncapped, one site), each at 64, 128 and 256 threads per block; all give
+// uncapped, one site), each at 64, 96, 128, 192 and 256 threads per block
+// (the four-site kernel up to 128): block counts that fill the SMs evenly
+// differ with the lattice size; all give
 // bit-identical links, so a trial never changes the Markov chain.  Each
 // trial captures its sweep as a CUDA graph, as u1_update runs it, and times
 // replays of it from a backed-up state (links and pass counter restored
@@ -954,7 +956,7 @@ static int tune_update(u1_lattice *lat, u1_rng *rng, bool use_cache) {
   std::vector<std::pair<int, int>> cand;  // (variant, threads per block)
   for (int v : {U1V_PAIR32, U1V_QUAD, U1V_PAIR, U1V_SINGLE})  // the persistent sweep is opt-in (u1_wave.cuh)
     if (variant_valid(lat, v))
-      for (int t : {256, 128, 64})
+      for (int t : {256, 192, 128, 96, 64})
         if (v != U1V_QUAD || t <= 128) cand.push_back({v, t});
   std::pair<int, int> best = cand[0];
   double best_us = -1.0;
