@@ -31,6 +31,20 @@ def test_library_exports_symbol(name):
     assert hasattr(_lib.lib, name), f"{name} declared in include/ but not exported"
 
 
+def test_every_exported_entry_point_is_declared_and_bound():
+    """The reverse direction: every extern "C" u1_* definition in the sources
+    is declared in include/ and has argtypes in the ctypes stub."""
+    csrc = Path(__file__).resolve().parents[1] / "latticeu1_b200" / "csrc"
+    defined = set()
+    for f in list(csrc.glob("*.cu")) + list(csrc.glob("*.cpp")):
+        defined |= set(re.findall(r'extern "C"\s+(?:const\s+)?\w+\s*\**\s*(u1_\w+)\s*\(', f.read_text()))
+    assert len(defined) > 25
+    declared = set(declared_symbols())
+    assert not defined - declared, sorted(defined - declared)
+    assert not defined - set(_lib.SIGNATURES) - set(getattr(_lib, "_RET", {})), \
+        sorted(defined - set(_lib.SIGNATURES))
+
+
 def _geom(dims, N, beta=1.0, aniso=1.0):
     return _lib.u1_geom(dims=dims, N=(C.c_int * 4)(*N), beta=beta, aniso=aniso)
 
