@@ -298,6 +298,8 @@ class Ref:
                 "ref_gpu_poly2": (None, [_dp, i, _dp]),
                 "ref_gpu_multilevel": (None, [_dp, i, i, i, i, i, i, i, _dp]),
                 "ref_gpu_chain": (None, [_dp, i, i, i, i, _dp]),
+                "ref_gpu_convert": (None, [_dp, i, _dp]),
+                "ref_gpu_plaq_fields": (None, [_dp, i, _dp, _dp]),
             }
             for name, (ret, args) in sig.items():
                 f = getattr(lib, name)

@@ -13,7 +13,8 @@
 // directly, mirroring SetupLatticeParameters (src/parameters.cu:146-208),
 // because that function also writes __constant__ memory (needs a GPU).
 // GPU side (B200 box only): UpdateLattice, Plaquette, Polyakov, Poly2,
-// MultiLevelField through the reference's public API.
+// MultiLevelField, LatticeConvert and PlaquetteFields through the
+// reference's public API.
 #include <omp.h>
 
 #include <cmath>
@@ -41,6 +42,8 @@
 namespace U1 {
 void metropolis(double *lat);       // src/update.cu:51
 void overrelaxation(double *lat);   // src/update.cu:84
+// src/convertOrder.cu:135-145 (defined there, declared in no header)
+Array<double> *LatticeConvert(Array<double> *lat, bool eo_to_no);
 }  // namespace U1
 
 using namespace U1;
@@ -235,6 +238,38 @@ void ref_gpu_multilevel(const double *lat_in, int n4, int k4, int n2, int k2, in
   }
   delete res;
   delete rng;
+  delete lat;
+}
+
+// LatticeConvert (src/convertOrder.cu:135-145): the reference's EO -> natural
+// order conversion of a whole lattice (V * dirs FP64 angles in and out).
+// Only eo_to_no = 1 runs: the reference's NO -> EO kernel writes
+// out[id + parity * V/2 + dir * V] with the natural-order index id < V
+// (src/convertOrder.cu:49-58), past the end of its output array.
+void ref_gpu_convert(const double *lat_in, int eo_to_no, double *out) {
+  if (eo_to_no != 1) return;
+  Array<double> *lat = upload(lat_in);
+  Array<double> *res = LatticeConvert(lat, eo_to_no != 0);
+  const size_t n = (size_t)Volume() * Dirs();
+  cudaMemcpy(out, res->getPtr(), n * sizeof(double), cudaMemcpyDeviceToHost);
+  delete res;
+  delete lat;
+}
+
+// PlaquetteFields(lat, arg, spacetime, evenoddOrder = true)
+// (src/plaquette_comps.cu:216-227): the six plaquette components per site
+// (spacetime) or time-averaged per spatial site, natural site order,
+// complexd[6 * size] with component d at [d * size]; means[12] = the six
+// component means (re, im).  The lattice is in the library's EO order.
+void ref_gpu_plaq_fields(const double *lat_in, int spacetime, double *field, double *means) {
+  Array<double> *lat = upload(lat_in);
+  PlaqFieldArg arg;
+  PlaquetteFields(lat, &arg, spacetime != 0, true);
+  cudaMemcpy(field, arg.plaqfield, 6 * arg.size * sizeof(complexd), cudaMemcpyDeviceToHost);
+  for (int i = 0; i < 6; ++i) {
+    means[2 * i] = arg.plaq[i].real();
+    means[2 * i + 1] = arg.plaq[i].imag();
+  }
   delete lat;
 }
 

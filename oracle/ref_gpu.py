@@ -8,7 +8,8 @@ tune cache) and exits on CUDA errors, so every task runs in a fresh child:
 
     python -m oracle.ref_gpu <task> <in.npz> <out.npz>
 
-tasks: measure | or_pass | poly2 | multilevel | multilevel_timing | timing | chain
+tasks: measure | or_pass | poly2 | multilevel | multilevel_timing | timing | chain |
+       convert | plaq_fields
 """
 from __future__ import annotations
 
@@ -84,6 +85,23 @@ def _child(task: str, fin: str, fout: str) -> None:
         lib.ref_gpu_chain(lat.ctypes.data_as(_dp), int(d["metrop"]), int(d["ovrn"]), n, int(d.get("seed", 1234)),
                           o.ctypes.data_as(_dp))
         out["obs"] = o.reshape(n, 6)
+    elif task == "convert":
+        # only EO -> NO: the reference's NO -> EO kernel writes past the end of
+        # its output (src/convertOrder.cu:49-58), so it is never run
+        if int(d["eo_to_no"]) != 1:
+            raise SystemExit("convert: only eo_to_no = 1 (the reference's NO -> EO direction writes out of bounds)")
+        o = np.zeros_like(lat)
+        lib.ref_gpu_convert(lat.ctypes.data_as(_dp), int(d["eo_to_no"]), o.ctypes.data_as(_dp))
+        out["lat"] = o
+    elif task == "plaq_fields":
+        st = int(d["spacetime"])
+        V = int(np.prod([n for n in N if n > 0]))
+        size = V if st else V // N[3]
+        f = np.zeros(12 * size)
+        m = np.zeros(12)
+        lib.ref_gpu_plaq_fields(lat.ctypes.data_as(_dp), st, f.ctypes.data_as(_dp), m.ctypes.data_as(_dp))
+        out["field"] = (f[0::2] + 1j * f[1::2]).reshape(6, size)
+        out["means"] = m[0::2] + 1j * m[1::2]
     elif task == "timing":
         warm, n = int(d["warmup"]), int(d["sweeps"])
         ms = lib.ref_gpu_update(lat.ctypes.data_as(_dp), None, int(d["metrop"]), int(d["ovrn"]), warm, n, 1234)

@@ -3,9 +3,11 @@ the same B200 as the sm_100a kernels: results on identical configurations,
 and throughput of its UpdateLattice on the 32^4 workload.
 
 Deterministic comparisons (no RNG involved): the fused measurement, one
-overrelaxation pass, Poly2 (plain and multihit) and MultiLevel with no
+overrelaxation pass, Poly2 (plain and multihit), MultiLevel with no
 updates (metrop = ovrn = 0), which pins the multilevel tensor contraction
-to the reference implementation itself.
+to the reference implementation itself, and the format kernels
+(LatticeConvert, src/convertOrder.cu:32-63,135-145; PlaquetteFields,
+src/plaquette_comps.cu:34-107,216-227).
 """
 import json
 import os
@@ -59,6 +61,48 @@ def test_measure_or_poly2_vs_reference_cuda(ctx, ref_gpu, dims, N, beta, aniso):
         want = c[f"c{mh}"][0::2] + 1j * c[f"c{mh}"][1::2]
         got = lat.poly_corr(bool(mh))
         np.testing.assert_allclose(got, want, rtol=0, atol=3e-5 * np.abs(want).max())
+
+
+@pytest.mark.parametrize("dims,N", [(4, (8, 6, 4, 10)), (3, (6, 8, 0, 4)), (2, (10, 0, 0, 6))])
+def test_convert_order_vs_reference_cuda(ctx, ref_gpu, dims, N):
+    """u1_convert_order EO -> NO against the reference's LatticeConvert(lat,
+    true), bit for bit (a permutation of FP64 angles); NO -> EO is its exact
+    inverse.  The reference's NO -> EO direction is not run: it writes
+    out[id + parity V/2 + dir V] with the natural-order index id < V
+    (src/convertOrder.cu:49-58), a wrong permutation that runs past the end of
+    the output array by up to V/2 elements."""
+    import torch
+    from latticeu1_b200.lattice import convert_order
+    n = int(np.prod([v for v in N if v > 0])) * dims
+    th = np.random.default_rng(11 + dims).uniform(0, 2 * np.pi, n)
+    want_no = ref_gpu.run("convert", _inputs(dims, N, 1.0, 1.0, th, eo_to_no=1))["lat"]
+    t = torch.tensor(th, dtype=torch.float64, device="cuda")
+    got_no = convert_order(t, dims, N, eo_to_no=True)
+    assert np.array_equal(got_no.cpu().numpy(), want_no)
+    back = convert_order(torch.tensor(want_no, dtype=torch.float64, device="cuda"), dims, N, eo_to_no=False)
+    assert torch.equal(back, t)
+
+
+@pytest.mark.parametrize("spacetime", [True, False])
+def test_plaquette_fields_vs_reference_cuda(ctx, ref_gpu, spacetime):
+    """u1_plaquette_fields against the reference's PlaquetteFields
+    (evenoddOrder = true: the lattice in the EO layout, fields in natural
+    site order), per site and time-averaged per spatial site: every
+    component within 1e-6 (FP32 links against FP64 angles) and the six
+    component means within 1e-6."""
+    from latticeu1_b200 import Lattice, Rng
+    N = (8, 6, 4, 10)
+    lat = Lattice(ctx, 4, N, 1.0)
+    rng = Rng(ctx, 6)
+    lat.hot_start(rng)
+    lat.update(rng, 1, 3)
+    th = lat.export_angles()
+    r = ref_gpu.run("plaq_fields", _inputs(4, N, 1.0, 1.0, th, spacetime=int(spacetime)))
+    f, m = lat.plaquette_fields(spacetime=spacetime)
+    f = f.cpu().numpy()
+    assert f.shape == r["field"].shape
+    assert np.abs(f - r["field"]).max() < 1e-6
+    assert np.abs(m - r["means"]).max() < 1e-6
 
 
 def _jackknife_mean(x, nbins=25):
