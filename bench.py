@@ -40,6 +40,7 @@ DIMS = 4
 METRIC = "link-updates/s at 32^4 (1 Metropolis + 4 OR per sweep)"
 UNIT = "link-updates/s"
 CLOCK_WINDOW_S = 1.5
+E2E_CHAINS = 3  # chains in flight in the end-to-end leg
 
 
 def algorithmic_bytes_per_link_update(d: int) -> int:
@@ -158,17 +159,33 @@ def ncu_batch_traffic_per_link_sweep():
     return None
 
 
-def ncu_traffic_per_launch(N, kernel: str):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary, if
-    there is one for this geometry and kernel."""
-    p = ROOT / "profiles" / f"k_update_{geom_name(N).replace('^4', 'x4')}_traffic.txt"
+# Sources the update kernels compile from: a committed ncu figure counts only
+# while their digest matches the one recorded beside it.
+UPDATE_KERNEL_SOURCES = ("u1_update.cuh", "u1_geom.cuh", "u1_cplx.cuh", "u1_philox.h")
+
+
+def update_kernel_digest() -> str:
+    import hashlib
+    h = hashlib.sha256()
+    for name in UPDATE_KERNEL_SOURCES:
+        h.update((ROOT / "latticeu1_b200" / "csrc" / name).read_bytes())
+    return h.hexdigest()[:16]
+
+
+def ncu_traffic_per_launch(N, kernel: str, profiles: Path | None = None) -> tuple[float | None, str]:
+    """DRAM bytes per launch of `kernel` from the committed ncu summary for
+    this geometry, and a note; None when there is no summary for this
+    geometry and kernel or it was made from other kernel sources."""
+    p = (profiles or ROOT / "profiles") / f"k_update_{geom_name(N).replace('^4', 'x4')}_traffic.txt"
     if not p.exists():
-        return None
-    fields = dict(line.split(":", 1) for line in p.read_text().splitlines()
-                  if ":" in line and not line.startswith("#"))
-    if fields.get("kernel", "").strip() != kernel or "dram_bytes_per_launch" not in fields:
-        return None
-    return float(fields["dram_bytes_per_launch"].split()[0])
+        return None, f"no committed ncu summary for {geom_name(N)}"
+    fields = {k.strip(): v.strip() for k, v in (line.split(":", 1) for line in p.read_text().splitlines()
+                                                if ":" in line and not line.startswith("#"))}
+    if fields.get("kernel") != kernel or "dram_bytes_per_launch" not in fields:
+        return None, f"the committed ncu summary is for {fields.get('kernel')}, not {kernel}"
+    if fields.get("source_digest") != update_kernel_digest():
+        return None, "the committed ncu summary was made from other update-kernel sources (stale)"
+    return float(fields["dram_bytes_per_launch"].split()[0]), f"ncu, profiles/{p.name}"
 
 
 # ------------------------------------------------------------------ CPU baselines
@@ -262,6 +279,108 @@ def run_reference(args) -> None:
 
 
 # ------------------------------------------------------------------ our arm
+def hbm_resident_line(ctx, L: int, steps: int, warmup: int, flush, peak: float) -> dict:
+    """The measured step (1 Metropolis + 4 OR + measurement) on an L^4
+    lattice larger than L2, tuned as the headline lattice: device time per
+    step (CUDA events, L2 flushed between steps), link-updates/s and the
+    update kernel's algorithmic bandwidth against the measured HBM peak."""
+    import torch
+
+    from latticeu1_b200 import Lattice, Rng
+    N = (L,) * 4
+    lat = Lattice(ctx, DIMS, N, BETA)
+    stream = torch.cuda.Stream()
+    lat.set_stream(stream.cuda_stream)
+    rng = Rng(ctx, 4321)
+    obs = torch.zeros(6, dtype=torch.float64, device="cuda")
+    with torch.cuda.stream(stream):
+        lat.hot_start(rng)
+        for _ in range(warmup):
+            flush.zero_()
+            lat.update_measure(rng, METROP, OVRN, obs.data_ptr())
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(steps)]
+        for k in range(steps):
+            flush.zero_()
+            ev[k][0].record(stream)
+            lat.update_measure(rng, METROP, OVRN, obs.data_ptr())
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+    ms = sum(e[0].elapsed_time(e[1]) for e in ev) / steps
+    launches = 2 * DIMS * (METROP + OVRN)
+    alg = algorithmic_bytes_per_link_update(DIMS) * volume(N) // 2
+    achieved = alg / (ms * 1e-3 / launches) / 1e9
+    line = {"lattice": geom_name(N), "link_bytes": lat.nlinks * 8, "ms_per_step": ms,
+            "value": link_updates_per_step(N) / (ms * 1e-3), "unit": UNIT, "achieved_gbs": achieved,
+            "frac": achieved / peak, "update_variant": Lattice.VARIANTS.get(lat.variant, str(lat.variant)),
+            "update_block": lat.block, "steps": steps}
+    lat.close()
+    rng.close()
+    return line
+
+
+def e2e_rate(ctx, lat, rng, stream, N, beta, aniso, args, rank, world):
+    """End-to-end rate through the C ABI with host buffers (see the comment
+    below); returns (link-updates/s, steps, observables finite)."""
+    import torch
+
+    from latticeu1_b200 import Lattice, Rng, replicas
+    lu = link_updates_per_step(N)
+    # e2e: C ABI with host buffers.  Three chains in flight (triple
+    # buffering: host-to-device copy, sweep, device-to-host copy), each on
+    # its own stream with its FP64 configuration in pinned host memory; every
+    # step takes one chain through import (H2D), the measured sweep, the D2H
+    # read of its 6 observables and the export of its configuration (D2H), so
+    # one chain's host-to-device copy overlaps another's sweep and a third's
+    # device-to-host copy (PCIe is full duplex).  Each chain's configuration
+    # makes the round trip through host memory every time it steps.
+    lats, rngs, streams = [lat], [rng], [stream]
+    for c in range(1, E2E_CHAINS):
+        lc = Lattice(ctx, DIMS, N, beta, aniso)
+        lc.set_metropolis(args.delta, args.nhits)
+        lc.set_variant(lat.variant)
+        lc.set_block(lat.block)
+        sc = torch.cuda.Stream()
+        lc.set_stream(sc.cuda_stream)
+        rc_ = Rng(ctx, 1234)
+        rc_.set_chain(replicas.chain_id(c * world + rank))
+        lc.hot_start(rc_)
+        lats.append(lc)
+        rngs.append(rc_)
+        streams.append(sc)
+    hosts = [torch.empty(lat.nlinks, dtype=torch.float64, pin_memory=True) for _ in range(E2E_CHAINS)]
+    obs_dev = torch.zeros((E2E_CHAINS, 6), dtype=torch.float64, device="cuda")
+    obs_host = torch.zeros((E2E_CHAINS, 6), dtype=torch.float64, pin_memory=True)
+    for lc, h in zip(lats, hosts):
+        lc.export_angles(h)
+
+    def e2e_step(k):
+        c = k % E2E_CHAINS
+        lats[c].import_angles_async(hosts[c])
+        lats[c].update_measure(rngs[c], METROP, OVRN, obs_dev[c].data_ptr())
+        with torch.cuda.stream(streams[c]):
+            obs_host[c].copy_(obs_dev[c], non_blocking=True)  # D2H of the step's observables
+        lats[c].export_angles_async(hosts[c])
+
+    for k in range(2 * E2E_CHAINS):
+        e2e_step(k)
+    for lc in lats:
+        lc.synchronize()
+    e2e_steps = E2E_CHAINS * max(2, min(args.steps, 15))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(e2e_steps):
+        e2e_step(k)
+    for lc in lats:
+        lc.synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2e_value = world * e2e_steps * lu / replicas.max_over_ranks(e2e_s)
+    e2e_obs_ok = bool(torch.isfinite(obs_host).all())
+    for lc, rc_ in zip(lats[1:], rngs[1:]):
+        lc.close()
+        rc_.close()
+    return e2e_value, e2e_steps, e2e_obs_ok
+
+
 def run_ours(args) -> None:
     import numpy as np
     import torch
@@ -346,60 +465,10 @@ def run_ours(args) -> None:
     step_ms_max = replicas.max_over_ranks(step_ms)
     value = world * args.steps * lu / (step_ms_max * 1e-3)
 
-    # e2e: C ABI with host buffers.  Three chains in flight (triple
-    # buffering: host-to-device copy, sweep, device-to-host copy), each on
-    # its own stream with its FP64 configuration in pinned host memory; every
-    # step takes one chain through import (H2D), the measured sweep, the D2H
-    # read of its 6 observables and the export of its configuration (D2H), so
-    # one chain's host-to-device copy overlaps another's sweep and a third's
-    # device-to-host copy (PCIe is full duplex).  Each chain's configuration
-    # makes the round trip through host memory every time it steps.
-    E2E_CHAINS = 3
-    lats, rngs, streams = [lat], [rng], [stream]
-    for c in range(1, E2E_CHAINS):
-        lc = Lattice(ctx, DIMS, N, beta, aniso)
-        lc.set_metropolis(args.delta, args.nhits)
-        lc.set_variant(lat.variant)
-        lc.set_block(lat.block)
-        sc = torch.cuda.Stream()
-        lc.set_stream(sc.cuda_stream)
-        rc_ = Rng(ctx, 1234)
-        rc_.set_chain(replicas.chain_id(c * world + rank))
-        lc.hot_start(rc_)
-        lats.append(lc)
-        rngs.append(rc_)
-        streams.append(sc)
-    hosts = [torch.empty(lat.nlinks, dtype=torch.float64, pin_memory=True) for _ in range(E2E_CHAINS)]
-    obs_dev = torch.zeros((E2E_CHAINS, 6), dtype=torch.float64, device="cuda")
-    obs_host = torch.zeros((E2E_CHAINS, 6), dtype=torch.float64, pin_memory=True)
-    for lc, h in zip(lats, hosts):
-        lc.export_angles(h)
-
-    def e2e_step(k):
-        c = k % E2E_CHAINS
-        lats[c].import_angles_async(hosts[c])
-        lats[c].update_measure(rngs[c], METROP, OVRN, obs_dev[c].data_ptr())
-        with torch.cuda.stream(streams[c]):
-            obs_host[c].copy_(obs_dev[c], non_blocking=True)  # D2H of the step's observables
-        lats[c].export_angles_async(hosts[c])
-
-    for k in range(2 * E2E_CHAINS):
-        e2e_step(k)
-    for lc in lats:
-        lc.synchronize()
-    e2e_steps = E2E_CHAINS * max(2, min(args.steps, 15))
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for k in range(e2e_steps):
-        e2e_step(k)
-    for lc in lats:
-        lc.synchronize()
-    e2e_s = time.perf_counter() - t0
-    e2e_value = world * e2e_steps * lu / replicas.max_over_ranks(e2e_s)
-    e2e_obs_ok = bool(torch.isfinite(obs_host).all())
-    for lc, rc_ in zip(lats[1:], rngs[1:]):
-        lc.close()
-        rc_.close()
+    if args.no_e2e:
+        e2e_value, e2e_steps, e2e_obs_ok = None, 0, None
+    else:
+        e2e_value, e2e_steps, e2e_obs_ok = e2e_rate(ctx, lat, rng, stream, N, beta, aniso, args, rank, world)
     bytes_cfg = lat.nlinks * 8
 
     ob = obs[args.warmup:].cpu().numpy()
@@ -410,7 +479,9 @@ def run_ours(args) -> None:
         avg_launch_s = upd_ms * 1e-3 / (args.steps * upd_launches)
         alg_bytes = algorithmic_bytes_per_link_update(DIMS) * volume(N) // 2
         achieved = alg_bytes / avg_launch_s / 1e9
-        traffic = ncu_traffic_per_launch(N, KERNEL_OF_VARIANT.get(lat.variant, "k_update"))
+        traffic, traffic_note = ncu_traffic_per_launch(N, KERNEL_OF_VARIANT.get(lat.variant, "k_update"))
+        l2_bytes = torch.cuda.get_device_properties(local).L2_cache_size
+        resident = bytes_cfg < l2_bytes  # float2 links: 8 B each, as the FP64 angles
         line = {
             "metric": metric_for(N), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms_max / args.steps, "higher_is_better": True,
@@ -420,10 +491,16 @@ def run_ours(args) -> None:
                          "kernel": KERNEL_OF_VARIANT.get(lat.variant, "k_update") +
                                    " (one (parity,mu) phase; step average)",
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
+                         "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_note,
+                         "dram_frac": (traffic / alg_bytes) if traffic else None,
+                         "residency": (f"L2: the {bytes_cfg / 2 ** 20:.1f} MiB of links stay in the "
+                                       f"{l2_bytes / 2 ** 20:.0f} MiB L2 across a sweep's phases, so `frac` is "
+                                       "algorithmic bytes over the HBM peak while DRAM moves only `dram_frac` "
+                                       "of them; `hbm_resident` measures lattices beyond L2")
+                         if resident else "HBM: the links exceed L2",
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "avg_launch_us": avg_launch_s * 1e6},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_cfg,
+            "e2e": None if e2e_value is None else {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_cfg,
                     "d2h_bytes_per_step": bytes_cfg + 48, "steps": e2e_steps, "chains_in_flight": E2E_CHAINS,
                     "observables_finite": e2e_obs_ok,
                     "path": "per step, one of three chains (own stream, own pinned host FP64 configuration): "
@@ -441,6 +518,11 @@ def run_ours(args) -> None:
                             "abs_L": float(np.abs(ob[:, 4] + 1j * ob[:, 5]).mean()),
                             "per_chain_plaq_ss_st": per_chain},
         }
+        if world == 1 and args.hbm_check and args.delta == 0.0 and args.nhits == 1:
+            hb = [hbm_resident_line(ctx, L, max(3, min(args.steps, 10)), args.warmup, flush, peak)
+                  for L in args.hbm_check]
+            line["hbm_resident"] = {"lattices": hb, "note": "the same measured step on lattices beyond the "
+                                                            "126 MB L2, each tuned on its first update"}
         if world == 1 and not args.no_cpu_baseline and args.delta == 0.0 and args.nhits == 1:
             # the reference's CPU update has only the whole-circle single-hit proposal
             line["cpu_baseline"] = cpu_reference_rate(N, beta, aniso, args.cpu_budget)
@@ -505,7 +587,8 @@ def batched_geoms(seed: int = 20240):
 def run_batched(args) -> None:
     """Config: 512 independent chains advanced together (one launch per
     (parity, mu) phase for all of them, whole sweep + per-chain measurement
-    captured in one CUDA graph).  A step is one sweep (1 Metropolis + 4 OR)
+    captured in one CUDA graph), after u1_batch_tune has chosen the
+    chain-group size and each group's kernel and block size.  A step is one sweep (1 Metropolis + 4 OR)
     of every chain plus its plaquette/Polyakov measurement.  The comparator
     advances the same chains one by one (one lattice object per chain, its
     own graph-captured sweep), as a caller of the single-lattice API would."""
@@ -518,6 +601,10 @@ def run_batched(args) -> None:
     stream = torch.cuda.Stream()
     b = Batch(ctx, geoms, seed=1234)
     b.set_stream(stream.cuda_stream)
+    t_tune = time.perf_counter()
+    group_mb = b.tune()  # group size and per-group kernel / block size (cached in $U1_RESOURCE_PATH if set)
+    t_tune = time.perf_counter() - t_tune
+    layout = b.layout()
     links = b.total_links
     lu = links * (METROP + OVRN)
     flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device="cuda")
@@ -596,6 +683,9 @@ def run_batched(args) -> None:
                      "frac": achieved / peak, "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes,
                      "avg_launch_us": avg_launch_s * 1e6},
         "update_only_ms_per_step": upd_ms / args.steps,
+        "tuned": {"group_mb": group_mb, "groups": len(layout), "seconds": t_tune,
+                  "kernels": {f"{Batch.VARIANTS.get(v, v)}@{t}": sum(1 for g in layout if (g[2], g[3]) == (v, t))
+                              for v, t in sorted({(g[2], g[3]) for g in layout})}},
         "gpu_launches": int(launches),
         "one_by_one": {"value": seq_value, "unit": UNIT, "steps": seq_steps,
                        "path": "one Lattice per chain, graph-captured u1_update_measure each, same stream"},
@@ -719,6 +809,9 @@ def main() -> None:
     ap.add_argument("--block", type=int, default=256, help="threads per block with --variant")
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU baseline sampling")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--hbm-check", type=lambda v: [int(x) for x in v.split(",") if x], default=[48, 64],
+                    help="L^4 lattices beyond L2 timed beside the headline (empty: none)")
     ap.add_argument("--workload", choices=["update32", "multilevel", "batched", "kernels"], default="update32")
     ap.add_argument("--n2", type=int, default=200, help="level-2 sub-updates per step (multilevel)")
     args = ap.parse_args()

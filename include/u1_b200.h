@@ -51,6 +51,25 @@ const char *u1_last_error(void);
 /* Library version string. */
 const char *u1_version(void);
 
+/* Device allocator of the whole library.  Replaces the allocation layer of the
+ * reference's dev_malloc_ / dev_free_ (reference src/alloc.cpp:178-200,
+ * 321-340), which always call cudaMalloc / cudaFree and exit() on failure.
+ * alloc(user, bytes, &ptr) returns 0 and a device pointer, or nonzero on
+ * failure (the library then returns U1_ERR_NOMEM and the object it was
+ * working on stays usable); release(user, ptr) returns a block, and is called
+ * only after the device has finished all work (the library synchronises the
+ * device first, as cudaFree does).  Give both or
+ * neither (NULL, NULL restores cudaMalloc / cudaFree).  Lets a host framework
+ * place the library's memory in its own pool, and lets tests inject
+ * allocation failures on the host.  Refused with U1_ERR_STATE while the
+ * library holds blocks from the current allocator (destroy every object
+ * first).  Not for concurrent use with other calls of this library. */
+typedef int (*u1_dev_alloc_fn)(void *user, size_t bytes, void **out);
+typedef void (*u1_dev_free_fn)(void *user, void *ptr);
+int u1_set_device_allocator(u1_dev_alloc_fn alloc, u1_dev_free_fn release, void *user);
+/* Device blocks the library currently holds (all allocators; leak checks). */
+int u1_device_allocations(int64_t *live);
+
 /* Replaces Start(gpuid, ...) (reference src/cuda_error_check.cpp:24-45):
  * selects the device; no tune-cache side effects. */
 int u1_ctx_create(int device, u1_ctx **out);
@@ -94,6 +113,13 @@ int u1_lattice_set_graphs(u1_lattice *lat, int enable);
 int u1_lattice_set_variant(u1_lattice *lat, int variant);
 /* The variant in use: 0 while automatic and not yet tuned. */
 int u1_lattice_get_variant(const u1_lattice *lat, int *variant);
+/* Waits of the persistent sweep (variant 4; no counterpart in the reference):
+ * each neighbour wait polls at most spin_limit times (0: the default, about a
+ * second), and stall_tile >= 0 names a tile that never publishes its phases,
+ * a test hook whose neighbours' waits then run out.  A wait that runs out ends
+ * the sweep early and leaves the configuration invalid; the next synchronous
+ * call on the lattice returns U1_ERR_CUDA and clears the condition. */
+int u1_lattice_set_wave_wait(u1_lattice *lat, unsigned spin_limit, int stall_tile);
 /* Metropolis proposal (no reference counterpart; the reference proposes
  * theta' = 2 pi u on the whole circle, once per link and pass,
  * src/update.cu:181-182, and that stays the default: delta = 0, nhits = 1).
@@ -214,9 +240,10 @@ int u1_measure_async(u1_lattice *lat, double *dev_out);
  * loading the library keeps until exit.  links_dev: the V*dims float2 links
  * (this library's layout); out_dev: 6 doubles, as u1_measure; stream:
  * cudaStream_t as void* on the current device.  Lattices with V/2 above
- * 1,048,576 sites return U1_ERR_INVALID.  The first call on a device looks
- * up the array's address and should come before any stream capture; calls
- * that overlap on the GPU race on the shared array. */
+ * 1,048,576 sites return U1_ERR_INVALID.  The first call on a device (and
+ * the first after the device's CUDA context changes, e.g. cudaDeviceReset)
+ * looks up the array's address and should come before any stream capture;
+ * calls that overlap on the GPU race on the shared array. */
 int u1_measure_noalloc(const void *links_dev, const u1_geom *geom, double *out_dev, void *stream);
 
 /* Replaces Poly2 (reference src/polyakov.cu:618-654):
@@ -253,9 +280,29 @@ int u1_batch_info(const u1_batch *b, int64_t out[4]);
 /* Number of chain groups a sweep runs one after another (consecutive chains
  * whose links fit comfortably in L2, so that each group's sweep after its
  * first phase is served from L2).  The result is the same as one group.
- * The group size is U1_BATCH_GROUP_MB MiB (default 64; 0: one group), read
- * at u1_batch_create. */
+ * The untuned group size is U1_BATCH_GROUP_MB MiB (default 64; 0: one
+ * group), read at u1_batch_create. */
 int u1_batch_groups(const u1_batch *b, int *groups);
+/* Autotuner of the batch (replaces the reference's per-kernel block-size
+ * search, src/tune.cpp:306-416, for many chains per launch): the group size
+ * (32 ... 96 MiB of links) and, per group, the update kernel (four, two or
+ * one site per thread) and threads per block, timed as graph-replayed sweeps
+ * from a backed-up state (links and pass counter restored).  Every choice
+ * gives the same links bit for bit.  Cached per (device, dims, chain
+ * extents) in memory and in $U1_RESOURCE_PATH/u1b200_batch_tunecache.tsv;
+ * a cached result is applied without trials.  *group_mb (may be NULL) gets
+ * the chosen group size in MiB.  Synchronous; not inside a stream capture. */
+int u1_batch_tune(u1_batch *b, int *group_mb);
+/* Explicit layout (no counterpart in the reference): groups of at most
+ * group_mb MiB (<= 0: keep the current size); group k gets kernel
+ * variants[k] (5: four sites per thread, 1: two, 3: one) at threads[k]
+ * threads per block for k < ngroups; other groups, or choices a group's
+ * chains do not allow, take the default (four sites at 128 threads where
+ * every chain has Nx/2 a multiple of 4, else two sites at 256 where Nx/2 is
+ * even, else one site at 256). */
+int u1_batch_configure(u1_batch *b, int group_mb, int ngroups, const int *variants, const int *threads);
+/* Group `group`: out = {first chain, end chain, variant, threads per block}. */
+int u1_batch_group_info(const u1_batch *b, int group, int out[4]);
 /* Hot start of every chain (as u1_hot_start); advances the pass counter by 1. */
 int u1_batch_hot_start(u1_batch *b);
 /* One sweep of every chain: metrop Metropolis then ovrn overrelaxation
@@ -364,7 +411,7 @@ int u1_flow_layer_forward(const float *theta_in, float *theta_out, float *logdet
                           int K, int hidden, const float *W1, const float *B1, const float *W2, const float *B2,
                           float slope, void *stream);
 
-/* Backward of u1_flow_layer_forward (L up to 16): from theta_in and the
+/* Backward of u1_flow_layer_forward (L up to 32): from theta_in and the
  * upstream gradients grad_theta_out (batch x 2 x L x L) and grad_logdet
  * (batch; NULL for zero), writes grad_theta_in and the weight gradients
  * wgrad = (dW1[c][ci][ky][kx], dB1[c], dW2[o][ci][ky][kx], dB2[o]) summed over
@@ -374,6 +421,22 @@ int u1_flow_layer_backward(const float *theta_in, const float *grad_theta_out, c
                            float *grad_theta_in, float *wgrad_partials, float *wgrad, int batch, int L, int mu,
                            int off, int K, int hidden, const float *W1, const float *B1, const float *W2,
                            const float *B2, float slope, void *stream);
+
+/* The inverse coupling layer (no counterpart in the reference), arguments as
+ * u1_flow_layer_forward: the same context net (the context plaquettes hold no
+ * updated link, so the layer and its inverse see the same parameters), then
+ * the inverse mixture transform of each active plaquette by bisection, the
+ * link change that undoes a forward step, and logdet[b] = sum of log H' at the
+ * solutions (the forward layer's log-det at the returned configuration). */
+int u1_flow_layer_inverse(const float *theta_in, float *theta_out, float *logdet, int batch, int L, int mu, int off,
+                          int K, int hidden, const float *W1, const float *B1, const float *W2, const float *B2,
+                          float slope, void *stream);
+/* Backward of u1_flow_layer_inverse (implicit differentiation at the
+ * bisection solution), arguments as u1_flow_layer_backward. */
+int u1_flow_layer_inverse_backward(const float *theta_in, const float *grad_theta_out, const float *grad_logdet,
+                                   float *grad_theta_in, float *wgrad_partials, float *wgrad, int batch, int L,
+                                   int mu, int off, int K, int hidden, const float *W1, const float *B1,
+                                   const float *W2, const float *B2, float slope, void *stream);
 
 /* Number of kernels this library has launched in the calling process. */
 int u1_kernel_launch_count(uint64_t *out);

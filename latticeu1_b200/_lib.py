@@ -33,6 +33,11 @@ _vp = C.c_void_p
 _i = C.c_int
 _dp = C.POINTER(C.c_double)
 
+# u1_dev_alloc_fn / u1_dev_free_fn (include/u1_b200.h)
+DEV_ALLOC_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_size_t, C.POINTER(C.c_void_p))
+DEV_FREE_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_void_p)
+NO_ALLOC, NO_FREE = DEV_ALLOC_FN(), DEV_FREE_FN()  # NULL function pointers
+
 # name -> argtypes (all return int status unless listed in _RET)
 SIGNATURES = {
     "u1_ctx_create": [_i, C.POINTER(_vp)],
@@ -83,6 +88,9 @@ SIGNATURES = {
     "u1_batch_set_stream": [_vp, _vp],
     "u1_batch_info": [_vp, C.POINTER(C.c_int64)],
     "u1_batch_groups": [_vp, C.POINTER(_i)],
+    "u1_batch_tune": [_vp, C.POINTER(_i)],
+    "u1_batch_configure": [_vp, _i, _i, C.POINTER(_i), C.POINTER(_i)],
+    "u1_batch_group_info": [_vp, _i, C.POINTER(_i)],
     "u1_batch_hot_start": [_vp],
     "u1_batch_update": [_vp, _i, _i, _i],
     "u1_batch_measure": [_vp, _dp],
@@ -106,9 +114,15 @@ SIGNATURES = {
     "u1_ncp_inverse": [_vp, _vp, C.c_int64, _i, _vp, _vp, _vp, _vp],
     "u1_ncp_inverse_backward": [_vp, _vp, _vp, _vp, C.c_int64, _i, _vp, _vp, _vp],
     "u1_flow_layer_forward": [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, C.c_float, _vp],
+    "u1_flow_layer_inverse": [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, C.c_float, _vp],
+    "u1_flow_layer_inverse_backward": [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp,
+                                       C.c_float, _vp],
     "u1_flow_layer_backward": [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, C.c_float,
                                _vp],
     "u1_kernel_launch_count": [C.POINTER(C.c_uint64)],
+    "u1_set_device_allocator": [DEV_ALLOC_FN, DEV_FREE_FN, _vp],
+    "u1_device_allocations": [C.POINTER(C.c_int64)],
+    "u1_lattice_set_wave_wait": [_vp, C.c_uint, _i],
     "u1_last_error": [],
     "u1_version": [],
 }
@@ -138,6 +152,13 @@ def last_error() -> str:
 def check(rc: int, what: str = "") -> None:
     if rc != U1_OK:
         raise U1Error(rc, f"{what}: {last_error()}" if what else last_error())
+
+
+def device_allocations() -> int:
+    """Device blocks the library currently holds."""
+    v = C.c_int64(0)
+    check(lib.u1_device_allocations(C.byref(v)), "u1_device_allocations")
+    return int(v.value)
 
 
 def launch_count() -> int:

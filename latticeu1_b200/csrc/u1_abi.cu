@@ -37,7 +37,56 @@ static std::atomic<unsigned long long> g_rng_ids{1};
 void set_error(const std::string &msg) { g_err = msg; }
 int cuda_fail(cudaError_t e, const char *what) {
   set_error(std::string(what) + ": " + cudaGetErrorString(e));
-  return U1_ERR_CUDA;
+  return e == cudaErrorMemoryAllocation ? U1_ERR_NOMEM : U1_ERR_CUDA;
+}
+
+// The device allocator (u1_set_device_allocator).  live_allocs counts the
+// blocks handed out through dev_alloc and not yet returned, so the allocator
+// is never swapped while the library holds memory from the previous one.
+struct DevAllocator {
+  u1_dev_alloc_fn alloc = nullptr;
+  u1_dev_free_fn release = nullptr;
+  void *user = nullptr;
+};
+static std::mutex g_alloc_mu;
+static DevAllocator g_alloc;
+static std::atomic<long long> g_live_allocs{0};
+
+cudaError_t dev_alloc(void **p, size_t bytes) {
+  *p = nullptr;
+  DevAllocator a;
+  {
+    std::lock_guard<std::mutex> lock(g_alloc_mu);
+    a = g_alloc;
+  }
+  cudaError_t e;
+  if (a.alloc)
+    e = (a.alloc(a.user, bytes, p) == 0 && *p) ? cudaSuccess : cudaErrorMemoryAllocation;
+  else
+    e = cudaMalloc(p, bytes);
+  if (e == cudaSuccess)
+    g_live_allocs.fetch_add(1, std::memory_order_relaxed);
+  else
+    *p = nullptr;
+  return e;
+}
+
+cudaError_t dev_free(void *p) {
+  if (!p) return cudaSuccess;
+  DevAllocator a;
+  {
+    std::lock_guard<std::mutex> lock(g_alloc_mu);
+    a = g_alloc;
+  }
+  g_live_allocs.fetch_sub(1, std::memory_order_relaxed);
+  if (a.release) {
+    // cudaFree waits for the device; a caller's pool gets the same guarantee:
+    // no work of this library still uses the block when it is returned
+    cudaError_t e = cudaDeviceSynchronize();
+    a.release(a.user, p);
+    return e;
+  }
+  return cudaFree(p);
 }
 static int fail(int code, const std::string &msg) {
   set_error(msg);
@@ -50,23 +99,23 @@ int ensure_scratch(u1_lattice *lat, size_t partial_doubles, size_t out_doubles) 
     cudaStreamSynchronize(lat->stream);
     for (auto &kv : lat->graphs) cudaGraphExecDestroy(kv.second);
     lat->graphs.clear();
-    if (lat->partials) cudaFree(lat->partials);
+    if (lat->partials) u1i::dev_free(lat->partials);
     lat->partials = nullptr;
     lat->partials_cap = 0;
-    U1_CUDA_TRY(cudaMalloc(&lat->partials, partial_doubles * sizeof(double)));
+    U1_CUDA_TRY(u1i::dev_alloc(&lat->partials, partial_doubles * sizeof(double)));
     lat->partials_cap = partial_doubles;
   }
   if (!lat->counter) {
-    U1_CUDA_TRY(cudaMalloc(&lat->counter, sizeof(unsigned int)));
+    U1_CUDA_TRY(u1i::dev_alloc(&lat->counter, sizeof(unsigned int)));
     U1_CUDA_TRY(cudaMemset(lat->counter, 0, sizeof(unsigned int)));
   }
   if (out_doubles > lat->d_out_cap) {
-    if (lat->d_out) cudaFree(lat->d_out);
+    if (lat->d_out) u1i::dev_free(lat->d_out);
     if (lat->h_out) cudaFreeHost(lat->h_out);
     lat->d_out = nullptr;
     lat->h_out = nullptr;
     lat->d_out_cap = lat->h_out_cap = 0;
-    U1_CUDA_TRY(cudaMalloc(&lat->d_out, out_doubles * sizeof(double)));
+    U1_CUDA_TRY(u1i::dev_alloc(&lat->d_out, out_doubles * sizeof(double)));
     U1_CUDA_TRY(cudaMallocHost(&lat->h_out, out_doubles * sizeof(double)));
     lat->d_out_cap = lat->h_out_cap = out_doubles;
   }
@@ -85,6 +134,27 @@ extern "C" const char *u1_version(void) { return "latticeu1_b200 0.1 (sm_100a)";
 extern "C" int u1_kernel_launch_count(uint64_t *out) {
   if (!out) return fail(U1_ERR_INVALID, "u1_kernel_launch_count: null out");
   *out = u1i::g_launches.load();
+  return U1_OK;
+}
+
+extern "C" int u1_set_device_allocator(u1_dev_alloc_fn alloc, u1_dev_free_fn release, void *user) {
+  using namespace u1i;
+  if ((alloc == nullptr) != (release == nullptr))
+    return fail(U1_ERR_INVALID, "u1_set_device_allocator: give both functions or neither");
+  std::lock_guard<std::mutex> lock(g_alloc_mu);
+  const long long live = g_live_allocs.load();
+  if (live != 0)
+    return fail(U1_ERR_STATE, "u1_set_device_allocator: the library still holds " + std::to_string(live) +
+                                  " device allocations from the current allocator");
+  g_alloc.alloc = alloc;
+  g_alloc.release = release;
+  g_alloc.user = user;
+  return U1_OK;
+}
+
+extern "C" int u1_device_allocations(int64_t *live) {
+  if (!live) return fail(U1_ERR_INVALID, "u1_device_allocations: null argument");
+  *live = u1i::g_live_allocs.load();
   return U1_OK;
 }
 
@@ -206,10 +276,10 @@ extern "C" int u1_lattice_create(u1_ctx *ctx, const u1_geom *geom, u1_lattice **
   }
   lat->stream = ctx->stream ? ctx->stream : lat->own_stream;
   const size_t nl = (size_t)g.V * g.dims;
-  e = cudaMalloc(&lat->links, nl * sizeof(float2));
+  e = u1i::dev_alloc(&lat->links, nl * sizeof(float2));
   if (e != cudaSuccess) {
     u1_lattice_destroy(lat);
-    u1i::set_error(std::string("u1_lattice_create: cudaMalloc links: ") + cudaGetErrorString(e));
+    u1i::set_error(std::string("u1_lattice_create: link allocation: ") + cudaGetErrorString(e));
     return U1_ERR_NOMEM;
   }
   rc = u1_cold_start(lat);
@@ -226,15 +296,15 @@ extern "C" int u1_lattice_destroy(u1_lattice *lat) {
   cudaSetDevice(lat->ctx->device);
   cudaStreamSynchronize(lat->stream);
   drop_graphs(lat);
-  if (lat->links) cudaFree(lat->links);
-  if (lat->partials) cudaFree(lat->partials);
-  if (lat->counter) cudaFree(lat->counter);
-  if (lat->d_out) cudaFree(lat->d_out);
+  if (lat->links) u1i::dev_free(lat->links);
+  if (lat->partials) u1i::dev_free(lat->partials);
+  if (lat->counter) u1i::dev_free(lat->counter);
+  if (lat->d_out) u1i::dev_free(lat->d_out);
   if (lat->h_out) cudaFreeHost(lat->h_out);
-  if (lat->pfield) cudaFree(lat->pfield);
-  if (lat->stage) cudaFree(lat->stage);
-  if (lat->backup) cudaFree(lat->backup);
-  if (lat->wave_state) cudaFree(lat->wave_state);
+  if (lat->pfield) u1i::dev_free(lat->pfield);
+  if (lat->stage) u1i::dev_free(lat->stage);
+  if (lat->backup) u1i::dev_free(lat->backup);
+  if (lat->wave_state) u1i::dev_free(lat->wave_state);
   if (lat->own_stream) cudaStreamDestroy(lat->own_stream);
   delete lat;
   return U1_OK;
@@ -298,7 +368,7 @@ extern "C" int u1_cold_start(u1_lattice *lat) {
 }
 
 static int ensure_stage(u1_lattice *lat) {
-  if (!lat->stage) U1_CUDA_TRY(cudaMalloc(&lat->stage, (size_t)lat->g.V * lat->g.dims * sizeof(double)));
+  if (!lat->stage) U1_CUDA_TRY(u1i::dev_alloc(&lat->stage, (size_t)lat->g.V * lat->g.dims * sizeof(double)));
   return U1_OK;
 }
 
@@ -384,11 +454,11 @@ extern "C" int u1_rng_create(u1_ctx *ctx, uint64_t seed, u1_rng **out) {
   r->pass = 0;
   r->chain = 0;
   r->id = u1i::g_rng_ids.fetch_add(1);
-  cudaError_t e = cudaMalloc(&r->pass_dev, sizeof(unsigned long long));
+  cudaError_t e = u1i::dev_alloc(&r->pass_dev, sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMemset(r->pass_dev, 0, sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
-    if (r->pass_dev) cudaFree(r->pass_dev);
+    if (r->pass_dev) u1i::dev_free(r->pass_dev);
     delete r;
     return u1i::cuda_fail(e, "u1_rng_create");
   }
@@ -400,8 +470,8 @@ extern "C" int u1_rng_destroy(u1_rng *rng) {
   if (!rng) return U1_OK;
   cudaSetDevice(rng->ctx->device);
   cudaDeviceSynchronize();
-  if (rng->pass_dev) cudaFree(rng->pass_dev);
-  if (rng->replay_dev) cudaFree(rng->replay_dev);
+  if (rng->pass_dev) u1i::dev_free(rng->pass_dev);
+  if (rng->replay_dev) u1i::dev_free(rng->replay_dev);
   delete rng;
   return U1_OK;
 }
@@ -435,11 +505,11 @@ extern "C" int u1_rng_set_replay(u1_rng *rng, const double *pairs, size_t n_pair
   if (!rng) return fail(U1_ERR_INVALID, "u1_rng_set_replay: null rng");
   U1_CUDA_TRY(cudaSetDevice(rng->ctx->device));
   U1_CUDA_TRY(cudaDeviceSynchronize());
-  if (rng->replay_dev) cudaFree(rng->replay_dev);
+  if (rng->replay_dev) u1i::dev_free(rng->replay_dev);
   rng->replay_dev = nullptr;
   rng->replay_pairs = 0;
   if (!pairs || n_pairs == 0) return U1_OK;
-  U1_CUDA_TRY(cudaMalloc(&rng->replay_dev, n_pairs * 2 * sizeof(double)));
+  U1_CUDA_TRY(u1i::dev_alloc(&rng->replay_dev, n_pairs * 2 * sizeof(double)));
   U1_CUDA_TRY(cudaMemcpy(rng->replay_dev, pairs, n_pairs * 2 * sizeof(double), cudaMemcpyHostToDevice));
   rng->replay_pairs = n_pairs;
   rng->replay_base = rng->pass;
@@ -453,7 +523,7 @@ extern "C" int u1_rng_debug_uniforms(u1_lattice *lat, const u1_rng *rng, uint64_
     return fail(U1_ERR_INVALID, "u1_rng_debug_uniforms: bad parity/mu");
   U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
   float *d = nullptr;
-  U1_CUDA_TRY(cudaMalloc(&d, (size_t)lat->g.Vh * 2 * sizeof(float)));
+  U1_CUDA_TRY(u1i::dev_alloc(&d, (size_t)lat->g.Vh * 2 * sizeof(float)));
   k_rng_debug<<<u1i::blocks_for(lat->g.Vh, 256), 256, 0, lat->stream>>>(
       d, lat->g.Vh, parity, mu, (uint32_t)rng->seed, (uint32_t)(rng->seed >> 32), rng->chain, pass);
   u1i::g_launches++;
@@ -461,7 +531,7 @@ extern "C" int u1_rng_debug_uniforms(u1_lattice *lat, const u1_rng *rng, uint64_
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(out_host, d, (size_t)lat->g.Vh * 2 * sizeof(float), cudaMemcpyDeviceToHost, lat->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(lat->stream);
-  cudaFree(d);
+  u1i::dev_free(d);
   if (e != cudaSuccess) return u1i::cuda_fail(e, "k_rng_debug");
   return U1_OK;
 }
@@ -478,6 +548,7 @@ static int launch_hot(u1_lattice *lat, u1_rng *rng) {
 }
 
 extern "C" int u1_hot_start(u1_lattice *lat, u1_rng *rng) {
+  u1i::NvtxRange nvtx_range("u1_hot_start");
   if (!lat || !rng) return fail(U1_ERR_INVALID, "u1_hot_start: null argument");
   U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
   int rc;
@@ -562,14 +633,29 @@ static int launch_phase(const UpdArgs &a, cudaStream_t s, bool met, int src, int
   return fail(U1_ERR_INVALID, "k_update: direction out of range");
 }
 
-// SM count for the block-order remap of the phase kernels (sm_local_block);
-// U1_REMAP=0 in the environment keeps the launch order.
-static int sm_remap(const u1_lattice *lat) {
+// SM count for the block-order remap of the four-site phase kernels
+// (sm_local_block) when a phase's grid runs as a single wave, else 0 (launch
+// order).  Over several waves the remap hands each SM a distant slice of the
+// lattice, so a plane and its neighbour planes are loaded many waves apart
+// and miss in L2 (measured at 64^4: 1.5x the algorithmic DRAM reads, L2 hit
+// rate 22 %).  U1_REMAP=0 in the environment keeps the launch order always.
+static int sm_remap(u1_lattice *lat) {
   static const bool off = [] {
     const char *r = std::getenv("U1_REMAP");
     return r && r[0] == '0';
   }();
-  return off ? 0 : lat->ctx->prop.multiProcessorCount;
+  if (off) return 0;
+  if (lat->remap_block != lat->block) {
+    const int sms = lat->ctx->prop.multiProcessorCount;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_update_quad<4, 0, false, SRC_PHILOX>, lat->block,
+                                                      0) != cudaSuccess)
+      per_sm = 0;
+    const long long blocks = ((long long)lat->g.Vh / 4 + lat->block - 1) / lat->block;
+    lat->remap_sms = (per_sm > 0 && blocks <= (long long)per_sm * sms) ? sms : 0;
+    lat->remap_block = lat->block;
+  }
+  return lat->remap_sms;
 }
 
 // The proposal settings of `lat` into the kernel arguments.
@@ -595,7 +681,7 @@ static bool wave_usable(u1_lattice *lat) {
     return false;
   if ((long long)per_sm * lat->ctx->prop.multiProcessorCount < wave_tiles(lat->g)) return false;
   const size_t n = (size_t)wave_tiles(lat->g) + 2;  // flags, ticket, error word
-  if (cudaMalloc(&lat->wave_state, n * sizeof(unsigned int)) != cudaSuccess) return false;
+  if (u1i::dev_alloc(&lat->wave_state, n * sizeof(unsigned int)) != cudaSuccess) return false;
   if (cudaMemset(lat->wave_state, 0, n * sizeof(unsigned int)) != cudaSuccess) return false;
   lat->wave_ok = 1;
   return true;
@@ -626,6 +712,8 @@ static int launch_wave(u1_lattice *lat, float2 *links, u1_rng *rng, int metrop, 
   w.ticket = lat->wave_state + tiles;
   w.err = lat->wave_state + tiles + 1;
   w.pass_rw = rng->pass_dev;
+  w.spin_limit = lat->wave_spin_limit ? lat->wave_spin_limit : kWaveSpinLimit;
+  w.stall_tile = lat->wave_stall_tile;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)tiles);
   cfg.blockDim = dim3((unsigned)wave_threads(lat->g));
@@ -877,7 +965,9 @@ static bool block_valid(int threads) { return threads >= 32 && threads <= 256 &&
 // bit-identical links, so a trial never changes the Markov chain.  Each
 // trial captures its sweep as a CUDA graph, as u1_update runs it, and times
 // replays of it from a backed-up state (links and pass counter restored
-// afterwards, as the reference's preTune/postTune do); the winner is cached per (device, geometry) in
+// afterwards, as the reference's preTune/postTune do), in two rounds (the
+// second in reverse order, each candidate keeping its faster time); the
+// winner is cached per (device, geometry) in
 // memory and, when U1_RESOURCE_PATH names a directory, in
 // $U1_RESOURCE_PATH/u1b200_tunecache.tsv (the reference's tunecache.csv
 // location rule, src/tune.cpp:160-232).  U1_TUNE=0 disables tuning.
@@ -962,14 +1052,24 @@ static int tune_update(u1_lattice *lat, u1_rng *rng, bool use_cache) {
   double best_us = -1.0;
   if (cand.size() > 1) {
     const size_t n = (size_t)lat->g.V * lat->g.dims;
-    if (!lat->backup) U1_CUDA_TRY(cudaMalloc(&lat->backup, n * sizeof(float2)));
+    if (!lat->backup) U1_CUDA_TRY(u1i::dev_alloc(&lat->backup, n * sizeof(float2)));
     U1_CUDA_TRY(cudaMemcpyAsync(lat->backup, lat->links, n * sizeof(float2), cudaMemcpyDeviceToDevice, lat->stream));
     const unsigned long long pass0 = rng->pass;
     cudaEvent_t e0, e1;
     U1_CUDA_TRY(cudaEventCreate(&e0));
     U1_CUDA_TRY(cudaEventCreate(&e1));
     int rc = U1_OK;
-    for (const auto &vt : cand) {
+    // Two rounds over the candidates, the second in reverse order, keeping
+    // each candidate's faster time: a large lattice drives the GPU into its
+    // power cap during tuning, and one round would favour whichever
+    // candidates ran first (measured at 64^4: the two-site kernel at 96
+    // threads picked over the four-site one, 4.8 against 4.0 ms a step).
+    std::vector<double> cand_us(cand.size(), -1.0);
+    std::vector<size_t> order;
+    for (size_t k = 0; k < cand.size(); ++k) order.push_back(k);
+    for (size_t k = cand.size(); k-- > 0;) order.push_back(k);
+    for (size_t ci : order) {
+      const auto &vt = cand[ci];
       lat->variant = vt.first;
       lat->block = vt.second;
       cudaGraphExec_t ex = nullptr;
@@ -995,11 +1095,13 @@ static int tune_update(u1_lattice *lat, u1_rng *rng, bool use_cache) {
       if (ex) cudaGraphExecDestroy(ex);
       if (rc) break;
       const double us = 1e3 * ms / 5.0;
-      if (best_us < 0.0 || us < best_us) {
-        best_us = us;
-        best = vt;
-      }
+      if (cand_us[ci] < 0.0 || us < cand_us[ci]) cand_us[ci] = us;
     }
+    for (size_t k = 0; k < cand.size() && !rc; ++k)
+      if (best_us < 0.0 || cand_us[k] < best_us) {
+        best_us = cand_us[k];
+        best = cand[k];
+      }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc) {
@@ -1019,6 +1121,7 @@ static int tune_update(u1_lattice *lat, u1_rng *rng, bool use_cache) {
 }
 
 extern "C" int u1_tune(u1_lattice *lat, u1_rng *rng, int *variant) {
+  u1i::NvtxRange nvtx_range("u1_tune");
   if (!lat || !rng) return fail(U1_ERR_INVALID, "u1_tune: null argument");
   if (rng->replay_dev) return fail(U1_ERR_STATE, "u1_tune: not available while a replay stream is set");
   U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
@@ -1034,6 +1137,16 @@ extern "C" int u1_lattice_set_variant(u1_lattice *lat, int variant) {
     return fail(U1_ERR_INVALID, "u1_lattice_set_variant: variant not valid for this geometry (pair variants need Nx/2 even)");
   lat->variant = variant;
   drop_graphs(lat);
+  return U1_OK;
+}
+
+extern "C" int u1_lattice_set_wave_wait(u1_lattice *lat, unsigned spin_limit, int stall_tile) {
+  if (!lat) return fail(U1_ERR_INVALID, "u1_lattice_set_wave_wait: null lattice");
+  if (stall_tile >= wave_tiles(lat->g))
+    return fail(U1_ERR_INVALID, "u1_lattice_set_wave_wait: stall_tile " + std::to_string(stall_tile) +
+                                    " beyond the lattice's " + std::to_string(wave_tiles(lat->g)) + " tiles");
+  lat->wave_spin_limit = spin_limit;
+  lat->wave_stall_tile = stall_tile < 0 ? -1 : stall_tile;
   return U1_OK;
 }
 
@@ -1110,6 +1223,7 @@ static int update_impl(u1_lattice *lat, u1_rng *rng, int metrop, int ovrn, doubl
 }
 
 extern "C" int u1_update(u1_lattice *lat, u1_rng *rng, int metrop, int ovrn) {
+  u1i::NvtxRange nvtx_range("u1_update");
   if (!lat || !rng) return fail(U1_ERR_INVALID, "u1_update: null argument");
   if (metrop < 0 || ovrn < 0) return fail(U1_ERR_INVALID, "u1_update: negative pass count");
   if (metrop == 0 && ovrn == 0) return U1_OK;
@@ -1119,6 +1233,7 @@ extern "C" int u1_update(u1_lattice *lat, u1_rng *rng, int metrop, int ovrn) {
 static int measure_dispatch(u1_lattice *lat, double *dev_out);
 
 extern "C" int u1_update_measure(u1_lattice *lat, u1_rng *rng, int metrop, int ovrn, double *dev_out) {
+  u1i::NvtxRange nvtx_range("u1_update_measure");
   if (!lat || !rng || !dev_out) return fail(U1_ERR_INVALID, "u1_update_measure: null argument");
   if (metrop < 0 || ovrn < 0) return fail(U1_ERR_INVALID, "u1_update_measure: negative pass count");
   U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
@@ -1204,12 +1319,14 @@ static int measure_dispatch(u1_lattice *lat, double *dev_out) {
 }
 
 extern "C" int u1_measure_async(u1_lattice *lat, double *dev_out) {
+  u1i::NvtxRange nvtx_range("u1_measure_async");
   if (!lat || !dev_out) return fail(U1_ERR_INVALID, "u1_measure_async: null argument");
   U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
   return measure_dispatch(lat, dev_out);
 }
 
 extern "C" int u1_measure(u1_lattice *lat, double out[6]) {
+  u1i::NvtxRange nvtx_range("u1_measure");
   if (!lat || !out) return fail(U1_ERR_INVALID, "u1_measure: null argument");
   U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
   int rc = wave_check(lat);
@@ -1255,11 +1372,12 @@ static int launch_poly_field(u1_lattice *lat, const float2 *links, int multihit)
 }
 
 extern "C" int u1_poly_corr(u1_lattice *lat, int multihit, double *out, int out_len) {
+  u1i::NvtxRange nvtx_range("u1_poly_corr");
   if (!lat || !out) return fail(U1_ERR_INVALID, "u1_poly_corr: null argument");
   const int R = lat->g.N[0] / 2;
   if (out_len < 2 * R) return fail(U1_ERR_INVALID, "u1_poly_corr: out_len < 2*R (R = Grid[0]/2)");
   U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
-  if (!lat->pfield) U1_CUDA_TRY(cudaMalloc(&lat->pfield, (size_t)lat->g.Vs * sizeof(double2)));
+  if (!lat->pfield) U1_CUDA_TRY(u1i::dev_alloc(&lat->pfield, (size_t)lat->g.Vs * sizeof(double2)));
   const int nb = u1i::blocks_for(lat->g.Vs, kRedThreads);
   int rc = u1i::ensure_scratch(lat, (size_t)nb * 2 * R, (size_t)2 * R);
   if (rc) return rc;
@@ -1283,6 +1401,7 @@ extern "C" int u1_poly_corr(u1_lattice *lat, int multihit, double *out, int out_
 // ---------------------------------------------------------------- multilevel
 extern "C" int u1_multilevel(u1_lattice *lat, u1_rng *rng, int n4, int k4, int n2, int k2, int metrop,
                              int ovrn, double *out, int out_len) {
+  u1i::NvtxRange nvtx_range("u1_multilevel");
   if (!lat || !rng || !out) return fail(U1_ERR_INVALID, "u1_multilevel: null argument");
   const GeomK &g = lat->g;
   if (g.dims != 4) return fail(U1_ERR_INVALID, "u1_multilevel: requires a 4D lattice");
@@ -1295,27 +1414,27 @@ extern "C" int u1_multilevel(u1_lattice *lat, u1_rng *rng, int n4, int k4, int n
   U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
   const size_t size = (size_t)g.Vs * R * g.tdir;
   const int nl2 = g.N[g.tdir] / 2, nl4 = g.N[g.tdir] / 4;
-  float2 *work = nullptr, *mh = nullptr;
-  double2 *T2 = nullptr, *T4 = nullptr;
+  float2 *work = nullptr;
+  double2 *P2 = nullptr, *T2 = nullptr, *T4 = nullptr;
   int rc = U1_OK;
   auto cleanup = [&]() {
     cudaStreamSynchronize(lat->stream);
-    if (work) cudaFree(work);
-    if (mh) cudaFree(mh);
-    if (T2) cudaFree(T2);
-    if (T4) cudaFree(T4);
+    if (work) u1i::dev_free(work);
+    if (P2) u1i::dev_free(P2);
+    if (T2) u1i::dev_free(T2);
+    if (T4) u1i::dev_free(T4);
   };
-  cudaError_t e = cudaMalloc(&work, (size_t)g.V * g.dims * sizeof(float2));
-  if (e == cudaSuccess) e = cudaMalloc(&mh, (size_t)g.V * sizeof(float2));
-  if (e == cudaSuccess) e = cudaMalloc(&T2, size * nl2 * sizeof(double2));
-  if (e == cudaSuccess) e = cudaMalloc(&T4, size * nl4 * sizeof(double2));
+  cudaError_t e = u1i::dev_alloc(&work, (size_t)g.V * g.dims * sizeof(float2));
+  if (e == cudaSuccess) e = u1i::dev_alloc(&P2, (size_t)g.Vs * nl2 * sizeof(double2));
+  if (e == cudaSuccess) e = u1i::dev_alloc(&T2, size * nl2 * sizeof(double2));
+  if (e == cudaSuccess) e = u1i::dev_alloc(&T4, size * nl4 * sizeof(double2));
   if (e != cudaSuccess) {
     cleanup();
     u1i::set_error(std::string("u1_multilevel: allocation failed: ") + cudaGetErrorString(e));
     return U1_ERR_NOMEM;
   }
-  const int nb_ps = u1i::blocks_for((long long)size, 256);
   const int nb_s = u1i::blocks_for(g.Vs, kRedThreads);
+  const MlDims md{g.N[0], g.N[1], g.N[2], g.Vs, R, nl2, nl4};
   rc = u1i::ensure_scratch(lat, (size_t)nb_s * 2 * R, (size_t)2 * R);
   if (rc) {
     cleanup();
@@ -1338,9 +1457,9 @@ extern "C" int u1_multilevel(u1_lattice *lat, u1_rng *rng, int n4, int k4, int n
       int r = issue_sweep(lat, work, rng, metrop, ovrn, 2);
       if (r) return r;
     }
-    k_ml_mhit_field<4><<<u1i::blocks_for(g.V, 256), 256, 0, lat->stream>>>(work, g, lat->c, mh);
-    U1_LAUNCH_CHECK("k_ml_mhit_field");
-    k_ml_T2<<<nb_ps, 256, 0, lat->stream>>>(mh, g, R, T2);
+    k_ml_slab2<<<u1i::blocks_for((long long)g.Vs * nl2, 256), 256, 0, lat->stream>>>(work, g, lat->c, md, P2);
+    U1_LAUNCH_CHECK("k_ml_slab2");
+    k_ml_T2<<<u1i::blocks_for((long long)(size / 2) * nl2, 256), 256, 0, lat->stream>>>(P2, md, T2);
     U1_LAUNCH_CHECK("k_ml_T2");
     return U1_OK;
   };
@@ -1381,7 +1500,8 @@ extern "C" int u1_multilevel(u1_lattice *lat, u1_rng *rng, int n4, int k4, int n
         }
         rng->pass += (uint64_t)metrop * (uint64_t)k2;
       }
-      k_ml_T4<<<nb_ps, 256, 0, lat->stream>>>(T2, g, R, 1.0 / (double)n2, T4);
+      k_ml_T4<<<u1i::blocks_for((long long)(size / 2) * nl4, 256), 256, 0, lat->stream>>>(T2, md, 1.0 / (double)n2,
+                                                                                        T4);
       U1_LAUNCH_CHECK("k_ml_T4");
     }
     k_ml_final<<<nb_s, kRedThreads, 0, lat->stream>>>(T4, g, R, 1.0 / (double)n4, lat->partials, lat->counter,

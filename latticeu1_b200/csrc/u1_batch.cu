@@ -17,7 +17,10 @@
 #include <cstdlib>
 #include <array>
 #include <cstring>
+#include <fstream>
 #include <map>
+#include <mutex>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -33,9 +36,8 @@ struct BatchChain {
   GeomK g;
   CoupK c;
   uint32_t chain;
-  int first_pair;   // first block in the pair (two sites / thread) table
-  int first_site;   // first block in the site (one site / thread) table
-  int first_quad;   // first block in the quad (four sites / thread) table
+  int first_upd;    // first block of the chain in the update table (its group's variant and block size)
+  int first_site;   // first block in the hot-start table (one site per thread, 256 threads)
   int first_meas;   // first block in the measurement table
   MeasK meas;       // measurement layout (plaquette blocks, then Polyakov blocks)
   int nb_meas;
@@ -81,7 +83,7 @@ __device__ __forceinline__ UpdArgs batch_args(const BatchChain &sch, const Batch
 }
 
 // Four sites per thread (every chain of the launch's group has N0/2 a
-// multiple of 4), 128 threads and 512 sites per block, as k_update_quad.
+// multiple of 4), at most 128 threads per block, as k_update_quad.
 template <int D, int MU, bool MET>
 __global__ void __launch_bounds__(128, 7)
     k_batch_update_quad(const BatchChain *__restrict__ chains, const int *__restrict__ block_chain, BatchPhase ph) {
@@ -89,7 +91,7 @@ __global__ void __launch_bounds__(128, 7)
   const int blk = (int)blockIdx.x + ph.block_base;
   stage_chain(chains, __ldg(block_chain + blk), sch);
   const UpdArgs a = batch_args(sch, ph, MU);
-  update_quad_body<D, MU, MET, SRC_PHILOX>(a, 4 * ((blk - sch.first_quad) * (int)blockDim.x + (int)threadIdx.x));
+  update_quad_body<D, MU, MET, SRC_PHILOX>(a, 4 * ((blk - sch.first_upd) * (int)blockDim.x + (int)threadIdx.x));
 }
 
 template <int D, int MU, bool MET, bool PAIR>
@@ -112,7 +114,7 @@ __global__ void __launch_bounds__(256, 8)
   a.hit = ph.hit;
   a.bump_ptr = ph.bump_ptr;
   a.bump_by = ph.bump_by;
-  const int local = blk - (PAIR ? sch.first_pair : sch.first_site);
+  const int local = blk - sch.first_upd;
   if (PAIR)
     update_pair_body<D, MU, MET, SRC_PHILOX>(a, 2 * (local * blockDim.x + threadIdx.x));
   else
@@ -168,6 +170,16 @@ __global__ void __launch_bounds__(kRedThreads)
 
 }  // namespace
 
+// A group of consecutive chains [c0, c1) swept together, with the update
+// kernel variant (U1V_QUAD, U1V_PAIR32 or U1V_SINGLE: four, two or one site
+// per thread) and threads per block its launches use, and its range of the
+// update block table.
+struct BatchGroup {
+  int c0, c1;
+  int variant, threads;
+  int first_block, nblocks;
+};
+
 struct u1_batch {
   u1_ctx *ctx = nullptr;
   cudaStream_t stream = nullptr, own_stream = nullptr;
@@ -180,16 +192,19 @@ struct u1_batch {
   BatchChain *d_chains = nullptr;
   float2 *links = nullptr;
   size_t total_links = 0;
-  int *d_tab_pair = nullptr, *d_tab_site = nullptr, *d_tab_meas = nullptr, *d_tab_quad = nullptr;
-  int nb_pair = 0, nb_site = 0, nb_meas = 0, nb_quad = 0;
+  int *d_tab_upd = nullptr, *d_tab_site = nullptr, *d_tab_meas = nullptr;
+  int nb_upd = 0, nb_site = 0, nb_meas = 0;
+  size_t tab_upd_cap = 0;                  // ints allocated at d_tab_upd
   double *partials = nullptr, *d_out = nullptr, *h_out = nullptr;
   std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
   // Chain groups swept one after another: consecutive chains whose links
   // together fit comfortably in L2, so that after a group's first phase its
-  // links are served from L2.  Each: first pair block, pair blocks, first
-  // site block, site blocks, first quad block, quad blocks (0 unless every
-  // chain of the group takes four sites per thread).
-  std::vector<std::array<int, 6>> groups;
+  // links are served from L2; each group runs its own kernel variant and
+  // block size (u1_batch_tune).
+  std::vector<BatchGroup> groups;
+  size_t group_bytes = 64ull << 20;       // group size limit the groups were cut with
+  bool quad_enabled = true;               // four-site kernels allowed (U1_BATCH_QUAD=0: no)
+  float2 *backup = nullptr;               // link backup while tuning
 };
 
 using u1i::cuda_fail;
@@ -201,20 +216,109 @@ static int bfail(int code, const std::string &msg) {
   return code;
 }
 
+static int sites_per_thread(int variant) { return variant == U1V_QUAD ? 4 : variant == U1V_PAIR32 ? 2 : 1; }
+
+// Whether every chain of [c0, c1) fits `variant` (four sites per thread:
+// N0/2 a multiple of 4; two: N0/2 even) and `threads` suits its kernel.
+static bool group_allows(const u1_batch *b, int c0, int c1, int variant, int threads) {
+  if (threads < 32 || threads % 32) return false;
+  if (variant == U1V_QUAD) {
+    if (!b->quad_enabled || threads > 128) return false;
+  } else if (variant == U1V_PAIR32 || variant == U1V_SINGLE) {
+    if (threads > 256) return false;
+  } else {
+    return false;
+  }
+  for (int c = c0; c < c1; ++c) {
+    const int h = b->h_chains[c].g.hN0;
+    if ((variant == U1V_QUAD && (h & 3)) || (variant == U1V_PAIR32 && (h & 1))) return false;
+  }
+  return true;
+}
+
+// The untuned choice of a group: four sites per thread at 128 threads where
+// every chain allows it, else two sites at 256, else one site at 256.
+static std::pair<int, int> default_choice(const u1_batch *b, int c0, int c1) {
+  if (group_allows(b, c0, c1, U1V_QUAD, 128)) return {U1V_QUAD, 128};
+  if (group_allows(b, c0, c1, U1V_PAIR32, 256)) return {U1V_PAIR32, 256};
+  return {U1V_SINGLE, 256};
+}
+
+// Consecutive chains in groups of at most group_bytes of links (a single
+// chain may exceed it).
+static std::vector<std::pair<int, int>> split_groups(const u1_batch *b, size_t group_bytes) {
+  std::vector<std::pair<int, int>> out;
+  size_t bytes = 0;
+  int c0 = 0;
+  for (int c = 0; c < b->n; ++c) {
+    const size_t cb = (size_t)b->h_chains[c].g.V * b->h_chains[c].g.dims * sizeof(float2);
+    if (c > c0 && bytes + cb > group_bytes) {
+      out.push_back({c0, c});
+      c0 = c;
+      bytes = 0;
+    }
+    bytes += cb;
+  }
+  out.push_back({c0, b->n});
+  return out;
+}
+
+// Cut the chains into groups of at most group_bytes, give group k the
+// (variant, threads) choice[k] (defaults where choice is shorter or a choice
+// does not fit the group), lay out the update block table and upload it with
+// the chain descriptors.  Cached sweep graphs are dropped.  Every layout
+// gives the same links bit for bit: a chain's sites run the same update body
+// with the same Philox counters whichever thread takes them.
+static int batch_configure(u1_batch *b, size_t group_bytes, const std::vector<std::pair<int, int>> &choice) {
+  const std::vector<std::pair<int, int>> cuts = split_groups(b, group_bytes);
+  std::vector<BatchGroup> groups;
+  std::vector<int> tab;
+  for (size_t k = 0; k < cuts.size(); ++k) {
+    const int c0 = cuts[k].first, c1 = cuts[k].second;
+    std::pair<int, int> vt = k < choice.size() ? choice[k] : default_choice(b, c0, c1);
+    if (!group_allows(b, c0, c1, vt.first, vt.second)) vt = default_choice(b, c0, c1);
+    BatchGroup gr{c0, c1, vt.first, vt.second, (int)tab.size(), 0};
+    const int spt = sites_per_thread(vt.first);
+    for (int c = c0; c < c1; ++c) {
+      BatchChain &ch = b->h_chains[c];
+      ch.first_upd = (int)tab.size();
+      tab.insert(tab.end(), nblocks(ch.g.Vh / spt, vt.second), c);
+    }
+    gr.nblocks = (int)tab.size() - gr.first_block;
+    groups.push_back(gr);
+  }
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  b->graphs.clear();
+  if (tab.size() > b->tab_upd_cap) {
+    u1i::dev_free(b->d_tab_upd);
+    b->d_tab_upd = nullptr;
+    b->tab_upd_cap = 0;
+    U1_CUDA_TRY(u1i::dev_alloc(&b->d_tab_upd, sizeof(int) * tab.size()));
+    b->tab_upd_cap = tab.size();
+  }
+  U1_CUDA_TRY(cudaMemcpy(b->d_tab_upd, tab.data(), sizeof(int) * tab.size(), cudaMemcpyHostToDevice));
+  U1_CUDA_TRY(cudaMemcpy(b->d_chains, b->h_chains.data(), sizeof(BatchChain) * b->n, cudaMemcpyHostToDevice));
+  b->groups = groups;
+  b->nb_upd = (int)tab.size();
+  b->group_bytes = group_bytes;
+  return U1_OK;
+}
+
 extern "C" int u1_batch_destroy(u1_batch *b) {
   if (!b) return U1_OK;
   cudaSetDevice(b->ctx->device);
   cudaStreamSynchronize(b->stream);
   for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);
-  cudaFree(b->links);
-  cudaFree(b->d_chains);
-  cudaFree(b->d_tab_pair);
-  cudaFree(b->d_tab_site);
-  cudaFree(b->d_tab_meas);
-  cudaFree(b->d_tab_quad);
-  cudaFree(b->partials);
-  cudaFree(b->d_out);
-  cudaFree(b->pass_dev);
+  u1i::dev_free(b->links);
+  u1i::dev_free(b->d_chains);
+  u1i::dev_free(b->d_tab_upd);
+  u1i::dev_free(b->d_tab_site);
+  u1i::dev_free(b->d_tab_meas);
+  u1i::dev_free(b->backup);
+  u1i::dev_free(b->partials);
+  u1i::dev_free(b->d_out);
+  u1i::dev_free(b->pass_dev);
   if (b->h_out) cudaFreeHost(b->h_out);
   if (b->own_stream) cudaStreamDestroy(b->own_stream);
   delete b;
@@ -233,7 +337,7 @@ extern "C" int u1_batch_create(u1_ctx *ctx, int nchains, const u1_geom *geoms, u
   b->n = nchains;
   b->seed = seed;
   b->h_chains.resize(nchains);
-  std::vector<int> tab_pair, tab_site, tab_meas, tab_quad;
+  std::vector<int> tab_site, tab_meas;
   size_t off = 0;
   std::vector<size_t> offsets(nchains);
   for (int c = 0; c < nchains; ++c) {
@@ -267,70 +371,37 @@ extern "C" int u1_batch_create(u1_ctx *ctx, int nchains, const u1_geom *geoms, u
     ch.norm[0] = 1.0 / ((double)g.V * nSS);
     ch.norm[1] = 1.0 / ((double)g.V * nST);
     ch.norm[2] = 1.0 / (double)g.Vs;
-    const int np = nblocks(g.Vh / 2, 256), ns = nblocks(g.Vh, 256);
-    const int nq = (g.hN0 & 3) == 0 ? nblocks(g.Vh / 4, 128) : 0;
-    ch.first_pair = (int)tab_pair.size();
+    const int ns = nblocks(g.Vh, 256);
+    ch.first_upd = 0;  // set by batch_configure
     ch.first_site = (int)tab_site.size();
-    ch.first_quad = (int)tab_quad.size();
-    tab_quad.insert(tab_quad.end(), nq, c);
     ch.first_meas = (int)tab_meas.size();
     ch.meas = measure_layout(g);
     ch.nb_meas = ch.meas.nb_plaq + ch.meas.nb_poly;
-    tab_pair.insert(tab_pair.end(), np, c);
     tab_site.insert(tab_site.end(), ns, c);
     tab_meas.insert(tab_meas.end(), ch.nb_meas, c);
   }
   b->total_links = off;
-  b->nb_pair = (int)tab_pair.size();
   b->nb_site = (int)tab_site.size();
   b->nb_meas = (int)tab_meas.size();
-  b->nb_quad = (int)tab_quad.size();
-  {
-    // groups of at most U1_BATCH_GROUP_MB (default 64) MiB of links; a
-    // single chain may exceed it; 0 puts every chain in one group
-    size_t kGroupBytes = 64ull << 20;
-    if (const char *env = std::getenv("U1_BATCH_GROUP_MB")) {
-      const long long mb = std::atoll(env);
-      kGroupBytes = mb > 0 ? (size_t)mb << 20 : SIZE_MAX;
-    }
-    // U1_BATCH_QUAD=0 keeps every group on the two-site (or one-site) kernel
-    const char *qenv = std::getenv("U1_BATCH_QUAD");
-    const bool quad_enabled = !(qenv && qenv[0] == '0');
-    size_t bytes = 0;
-    int c0 = 0;
-    auto close_group = [&](int c1) {
-      const BatchChain &a = b->h_chains[c0];
-      const int pair_end = c1 < nchains ? b->h_chains[c1].first_pair : b->nb_pair;
-      const int site_end = c1 < nchains ? b->h_chains[c1].first_site : b->nb_site;
-      bool quad = quad_enabled;
-      for (int c = c0; c < c1; ++c) quad = quad && (b->h_chains[c].g.hN0 & 3) == 0;
-      const int quad_end = c1 < nchains ? b->h_chains[c1].first_quad : b->nb_quad;
-      b->groups.push_back({a.first_pair, pair_end - a.first_pair, a.first_site, site_end - a.first_site,
-                           a.first_quad, quad ? quad_end - a.first_quad : 0});
-    };
-    for (int c = 0; c < nchains; ++c) {
-      const size_t cb = (size_t)b->h_chains[c].g.V * b->h_chains[c].g.dims * sizeof(float2);
-      if (c > c0 && bytes + cb > kGroupBytes) {
-        close_group(c);
-        c0 = c;
-        bytes = 0;
-      }
-      bytes += cb;
-    }
-    close_group(nchains);
+  // groups of at most U1_BATCH_GROUP_MB (default 64) MiB of links; a single
+  // chain may exceed it; 0 puts every chain in one group
+  if (const char *env = std::getenv("U1_BATCH_GROUP_MB")) {
+    const long long mb = std::atoll(env);
+    b->group_bytes = mb > 0 ? (size_t)mb << 20 : SIZE_MAX;
   }
+  // U1_BATCH_QUAD=0 keeps every group on the two-site (or one-site) kernel
+  const char *qenv = std::getenv("U1_BATCH_QUAD");
+  b->quad_enabled = !(qenv && qenv[0] == '0');
   cudaError_t e = cudaStreamCreate(&b->own_stream);
   b->stream = ctx->stream ? ctx->stream : b->own_stream;
-  if (e == cudaSuccess) e = cudaMalloc(&b->links, b->total_links * sizeof(float2));
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_chains, sizeof(BatchChain) * nchains);
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_tab_pair, sizeof(int) * tab_pair.size());
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_tab_site, sizeof(int) * tab_site.size());
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_tab_meas, sizeof(int) * tab_meas.size());
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_tab_quad, sizeof(int) * std::max<size_t>(1, tab_quad.size()));
-  if (e == cudaSuccess) e = cudaMalloc(&b->partials, sizeof(double) * 6 * tab_meas.size());
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_out, sizeof(double) * 6 * nchains);
+  if (e == cudaSuccess) e = u1i::dev_alloc(&b->links, b->total_links * sizeof(float2));
+  if (e == cudaSuccess) e = u1i::dev_alloc(&b->d_chains, sizeof(BatchChain) * nchains);
+  if (e == cudaSuccess) e = u1i::dev_alloc(&b->d_tab_site, sizeof(int) * tab_site.size());
+  if (e == cudaSuccess) e = u1i::dev_alloc(&b->d_tab_meas, sizeof(int) * tab_meas.size());
+  if (e == cudaSuccess) e = u1i::dev_alloc(&b->partials, sizeof(double) * 6 * tab_meas.size());
+  if (e == cudaSuccess) e = u1i::dev_alloc(&b->d_out, sizeof(double) * 6 * nchains);
   if (e == cudaSuccess) e = cudaMallocHost(&b->h_out, sizeof(double) * 6 * nchains);
-  if (e == cudaSuccess) e = cudaMalloc(&b->pass_dev, sizeof(unsigned long long));
+  if (e == cudaSuccess) e = u1i::dev_alloc(&b->pass_dev, sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMemset(b->pass_dev, 0, sizeof(unsigned long long));
   if (e != cudaSuccess) {
     u1_batch_destroy(b);
@@ -338,18 +409,17 @@ extern "C" int u1_batch_create(u1_ctx *ctx, int nchains, const u1_geom *geoms, u
     return U1_ERR_NOMEM;
   }
   for (int c = 0; c < nchains; ++c) b->h_chains[c].links = b->links + offsets[c];
-  e = cudaMemcpy(b->d_chains, b->h_chains.data(), sizeof(BatchChain) * nchains, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess)
-    e = cudaMemcpy(b->d_tab_pair, tab_pair.data(), sizeof(int) * tab_pair.size(), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess)
-    e = cudaMemcpy(b->d_tab_site, tab_site.data(), sizeof(int) * tab_site.size(), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess && !tab_quad.empty())
-    e = cudaMemcpy(b->d_tab_quad, tab_quad.data(), sizeof(int) * tab_quad.size(), cudaMemcpyHostToDevice);
+  e = cudaMemcpy(b->d_tab_site, tab_site.data(), sizeof(int) * tab_site.size(), cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
     e = cudaMemcpy(b->d_tab_meas, tab_meas.data(), sizeof(int) * tab_meas.size(), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     u1_batch_destroy(b);
     return cuda_fail(e, "u1_batch_create: upload");
+  }
+  int rc = batch_configure(b, b->group_bytes, {});  // update table and chain descriptors
+  if (rc) {
+    u1_batch_destroy(b);
+    return rc;
   }
   // cold start
   for (int c = 0; c < nchains; ++c) {
@@ -404,11 +474,11 @@ extern "C" int u1_batch_hot_start(u1_batch *b) {
 
 template <int D, int MU, bool MET>
 static int batch_launch_quad(u1_batch *b, BatchPhase ph, int group) {
-  const std::array<int, 6> &gr = b->groups[group];
-  ph.block_base = gr[4];
+  const BatchGroup &gr = b->groups[group];
+  ph.block_base = gr.first_block;
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)gr[5]);
-  cfg.blockDim = dim3(128);
+  cfg.gridDim = dim3((unsigned)gr.nblocks);
+  cfg.blockDim = dim3((unsigned)gr.threads);
   cfg.stream = b->stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -416,7 +486,7 @@ static int batch_launch_quad(u1_batch *b, BatchPhase ph, int group) {
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   cudaError_t e = cudaLaunchKernelEx(&cfg, k_batch_update_quad<D, MU, MET>, (const BatchChain *)b->d_chains,
-                                     (const int *)b->d_tab_quad, ph);
+                                     (const int *)b->d_tab_upd, ph);
   u1i::g_launches.fetch_add(1, std::memory_order_relaxed);
   if (e != cudaSuccess) return cuda_fail(e, "k_batch_update_quad");
   return U1_OK;
@@ -424,11 +494,11 @@ static int batch_launch_quad(u1_batch *b, BatchPhase ph, int group) {
 
 template <int D, int MU, bool MET, bool PAIR>
 static int batch_launch(u1_batch *b, BatchPhase ph, int group) {
-  const std::array<int, 6> &gr = b->groups[group];
-  ph.block_base = PAIR ? gr[0] : gr[2];
+  const BatchGroup &gr = b->groups[group];
+  ph.block_base = gr.first_block;
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)(PAIR ? gr[1] : gr[3]));
-  cfg.blockDim = dim3(256);
+  cfg.gridDim = dim3((unsigned)gr.nblocks);
+  cfg.blockDim = dim3((unsigned)gr.threads);
   cfg.stream = b->stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -436,7 +506,7 @@ static int batch_launch(u1_batch *b, BatchPhase ph, int group) {
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   cudaError_t e = cudaLaunchKernelEx(&cfg, k_batch_update<D, MU, MET, PAIR>, (const BatchChain *)b->d_chains,
-                                     (const int *)(PAIR ? b->d_tab_pair : b->d_tab_site), ph);
+                                     (const int *)b->d_tab_upd, ph);
   u1i::g_launches.fetch_add(1, std::memory_order_relaxed);
   if (e != cudaSuccess) return cuda_fail(e, "k_batch_update");
   return U1_OK;
@@ -444,9 +514,10 @@ static int batch_launch(u1_batch *b, BatchPhase ph, int group) {
 
 template <int D, int MU>
 static int batch_launch_mu(u1_batch *b, const BatchPhase &ph, bool met, int group) {
-  if (b->groups[group][5] > 0)
+  const int v = b->groups[group].variant;
+  if (v == U1V_QUAD)
     return met ? batch_launch_quad<D, MU, true>(b, ph, group) : batch_launch_quad<D, MU, false>(b, ph, group);
-  if (b->pair_ok)
+  if (v == U1V_PAIR32)
     return met ? batch_launch<D, MU, true, true>(b, ph, group) : batch_launch<D, MU, false, true>(b, ph, group);
   return met ? batch_launch<D, MU, true, false>(b, ph, group) : batch_launch<D, MU, false, false>(b, ph, group);
 }
@@ -483,18 +554,19 @@ static int batch_measure_issue(u1_batch *b) {
   }
 }
 
-static int batch_issue_sweep(u1_batch *b, int metrop, int ovrn, bool measure) {
+// The sweep of groups [g0, g1) (all groups by default).
+static int batch_issue_sweep(u1_batch *b, int metrop, int ovrn, bool measure, int g0 = 0, int g1 = -1) {
   BatchPhase ph{};
   ph.key0 = (uint32_t)b->seed;
   ph.key1 = (uint32_t)(b->seed >> 32);
   ph.pass_dev = b->pass_dev;
   const int D = b->dims;
-  const int ngroups = (int)b->groups.size();
+  const int ngroups = g1 < 0 ? (int)b->groups.size() : g1;
   // Each chain group runs the whole sweep before the next starts.  Every
   // group's Metropolis phases read the same pass counter; the first
   // overrelaxation kernel of the last group (after all of them) bumps it.
   bool bumped = (metrop == 0);
-  for (int grp = 0; grp < ngroups; ++grp) {
+  for (int grp = g0; grp < ngroups; ++grp) {
     auto run = [&](int mu, bool met) {
       return D == 2 ? batch_phase<2>(b, ph, mu, met, grp)
            : D == 3 ? batch_phase<3>(b, ph, mu, met, grp)
@@ -531,6 +603,7 @@ static int batch_issue_sweep(u1_batch *b, int metrop, int ovrn, bool measure) {
 }
 
 extern "C" int u1_batch_update(u1_batch *b, int metrop, int ovrn, int measure) {
+  u1i::NvtxRange nvtx_range("u1_batch_update");
   if (!b) return bfail(U1_ERR_INVALID, "u1_batch_update: null batch");
   if (metrop < 0 || ovrn < 0) return bfail(U1_ERR_INVALID, "u1_batch_update: negative pass count");
   U1_CUDA_TRY(cudaSetDevice(b->ctx->device));
@@ -563,6 +636,7 @@ extern "C" int u1_batch_update(u1_batch *b, int metrop, int ovrn, int measure) {
 }
 
 extern "C" int u1_batch_measure(u1_batch *b, double *out_host) {
+  u1i::NvtxRange nvtx_range("u1_batch_measure");
   if (!b || !out_host) return bfail(U1_ERR_INVALID, "u1_batch_measure: null argument");
   U1_CUDA_TRY(cudaSetDevice(b->ctx->device));
   int rc = batch_measure_issue(b);
@@ -590,7 +664,7 @@ static int chain_io(u1_batch *b, int chain, double *host, bool import) {
   const BatchChain &ch = b->h_chains[chain];
   const size_t n = (size_t)ch.g.V * ch.g.dims;
   double *tmp = nullptr;
-  U1_CUDA_TRY(cudaMalloc(&tmp, n * sizeof(double)));
+  U1_CUDA_TRY(u1i::dev_alloc(&tmp, n * sizeof(double)));
   cudaError_t e = cudaSuccess;
   if (import) {
     e = cudaMemcpyAsync(tmp, host, n * sizeof(double), cudaMemcpyHostToDevice, b->stream);
@@ -605,7 +679,7 @@ static int chain_io(u1_batch *b, int chain, double *host, bool import) {
   }
   u1i::g_launches++;
   if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
-  cudaFree(tmp);
+  u1i::dev_free(tmp);
   if (e != cudaSuccess) return cuda_fail(e, "u1_batch angles");
   return U1_OK;
 }
@@ -630,5 +704,260 @@ extern "C" int u1_batch_import_angles(u1_batch *b, int chain, const double *angl
 extern "C" int u1_batch_get_pass(const u1_batch *b, uint64_t *pass) {
   if (!b || !pass) return bfail(U1_ERR_INVALID, "u1_batch_get_pass: null argument");
   *pass = b->pass;
+  return U1_OK;
+}
+
+// ---------------------------------------------------------------- tuner
+// The batch autotuner (no counterpart in the reference, which runs one
+// lattice per process; its block-size search is src/tune.cpp:306-416).  It
+// chooses the chain-group size (32 ... 96 MiB of links, the groups then
+// being swept one after another so each stays in L2) and, per group, the
+// update kernel (four, two or one site per thread) and threads per block.
+// Every choice gives the same links bit for bit, so trials never change the
+// Markov chains; each trial captures its sweep (1 Metropolis + 4 OR) as a
+// CUDA graph, as u1_batch_update runs it, and times 5 replays after 2
+// warm-up replays from a backed-up state (links and pass counter restored).
+// Stage 1 times whole sweeps for each group size with the default kernels;
+// stage 2 times each group's own sweep for each (kernel, threads) it
+// allows; the per-group choice is kept only if the whole sweep is faster.
+// The result is cached per (device, dims, chain extents) in memory and,
+// when U1_RESOURCE_PATH names a directory, in
+// $U1_RESOURCE_PATH/u1b200_batch_tunecache.tsv.
+namespace {
+struct BatchTuneRec {
+  size_t group_bytes;
+  std::vector<std::pair<int, int>> choice;
+};
+std::mutex g_btune_mu;
+bool g_btune_loaded = false;
+std::map<std::string, BatchTuneRec> g_btune;
+
+std::string batch_tune_file() {
+  const char *p = std::getenv("U1_RESOURCE_PATH");
+  return (p && *p) ? std::string(p) + "/u1b200_batch_tunecache.tsv" : std::string();
+}
+
+// Device, dims, chain count and an FNV-1a hash of every chain's extents.
+std::string batch_tune_key(const u1_batch *b) {
+  uint64_t h = 1469598103934665603ull;
+  for (const BatchChain &ch : b->h_chains)
+    for (int k = 0; k < 4; ++k) {
+      h ^= (uint64_t)(uint32_t)ch.g.N[k];
+      h *= 1099511628211ull;
+    }
+  std::ostringstream k;
+  k << b->ctx->prop.name << "|batch|" << b->dims << "|" << b->n << "|" << std::hex << h;
+  return k.str();
+}
+
+// key <tab> group MiB <tab> variant:threads,... <tab> microseconds per sweep
+void batch_tune_load_locked() {
+  if (g_btune_loaded) return;
+  g_btune_loaded = true;
+  const std::string f = batch_tune_file();
+  if (f.empty()) return;
+  std::ifstream in(f);
+  std::string line;
+  while (std::getline(in, line)) {
+    if (line.empty() || line[0] == '#') continue;
+    std::istringstream ls(line);
+    std::string key, mb, list;
+    if (!std::getline(ls, key, '\t') || !std::getline(ls, mb, '\t') || !std::getline(ls, list, '\t')) continue;
+    BatchTuneRec rec;
+    rec.group_bytes = (size_t)std::atoll(mb.c_str()) << 20;
+    std::istringstream li(list);
+    std::string item;
+    while (std::getline(li, item, ',')) {
+      const size_t c = item.find(':');
+      if (c == std::string::npos) continue;
+      rec.choice.push_back({std::atoi(item.substr(0, c).c_str()), std::atoi(item.substr(c + 1).c_str())});
+    }
+    if (rec.group_bytes > 0 && !rec.choice.empty()) g_btune[key] = rec;
+  }
+}
+
+void batch_tune_save(const std::string &key, const BatchTuneRec &rec, double us) {
+  const std::string f = batch_tune_file();
+  if (f.empty()) return;
+  std::ofstream out(f, std::ios::app);
+  if (!out) return;
+  out << key << '\t' << (rec.group_bytes >> 20) << '\t';
+  for (size_t k = 0; k < rec.choice.size(); ++k)
+    out << (k ? "," : "") << rec.choice[k].first << ':' << rec.choice[k].second;
+  out << '\t' << us << '\n';
+}
+
+std::vector<std::pair<int, int>> current_choice(const u1_batch *b) {
+  std::vector<std::pair<int, int>> c;
+  for (const BatchGroup &g : b->groups) c.push_back({g.variant, g.threads});
+  return c;
+}
+}  // namespace
+
+// Microseconds per sweep (1 Metropolis + 4 OR) of groups [g0, g1) in the
+// current layout: a captured graph, 2 warm-up and 5 timed replays; the
+// links and the pass counter are restored from the backup afterwards.
+static int batch_time_sweep(u1_batch *b, int g0, int g1, double *us) {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t ex = nullptr;
+  U1_CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  const unsigned long long launches0 = u1i::g_launches.load();
+  int rc = batch_issue_sweep(b, 1, 4, false, g0, g1);
+  u1i::g_launches.store(launches0);
+  cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "u1_batch_tune: capture");
+  e = cudaGraphInstantiate(&ex, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return cuda_fail(e, "u1_batch_tune: instantiate");
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  for (int k = 0; k < 2 && e == cudaSuccess; ++k) e = cudaGraphLaunch(ex, b->stream);
+  if (e == cudaSuccess) e = cudaEventRecord(e0, b->stream);
+  for (int k = 0; k < 5 && e == cudaSuccess; ++k) e = cudaGraphLaunch(ex, b->stream);
+  if (e == cudaSuccess) e = cudaEventRecord(e1, b->stream);
+  if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+  float ms = 0.f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+  const unsigned long long pass0 = b->pass;
+  cudaError_t r1 = cudaMemcpyAsync(b->links, b->backup, b->total_links * sizeof(float2), cudaMemcpyDeviceToDevice,
+                                   b->stream);
+  cudaError_t r2 = cudaMemcpyAsync(b->pass_dev, &pass0, sizeof(pass0), cudaMemcpyHostToDevice, b->stream);
+  cudaError_t r3 = cudaStreamSynchronize(b->stream);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaGraphExecDestroy(ex);
+  if (e == cudaSuccess) e = r1 != cudaSuccess ? r1 : r2 != cudaSuccess ? r2 : r3;
+  if (e != cudaSuccess) return cuda_fail(e, "u1_batch_tune: trial");
+  *us = 1e3 * ms / 5.0;
+  return U1_OK;
+}
+
+static int batch_tune(u1_batch *b) {
+  const std::string key = batch_tune_key(b);
+  {
+    std::lock_guard<std::mutex> lock(g_btune_mu);
+    batch_tune_load_locked();
+    auto it = g_btune.find(key);
+    if (it != g_btune.end()) return batch_configure(b, it->second.group_bytes, it->second.choice);
+  }
+  if (!b->backup) U1_CUDA_TRY(u1i::dev_alloc(&b->backup, b->total_links * sizeof(float2)));
+  U1_CUDA_TRY(cudaMemcpyAsync(b->backup, b->links, b->total_links * sizeof(float2), cudaMemcpyDeviceToDevice,
+                              b->stream));
+  U1_CUDA_TRY(cudaStreamSynchronize(b->stream));
+  // Each stage times its candidates in two rounds, the second in reverse
+  // order, and keeps each candidate's faster time (a large batch drives the
+  // GPU into its power cap while tuning; one round would favour whichever
+  // candidates ran first).
+  auto two_rounds = [](size_t n) {
+    std::vector<size_t> order;
+    for (size_t k = 0; k < n; ++k) order.push_back(k);
+    for (size_t k = n; k-- > 0;) order.push_back(k);
+    return order;
+  };
+  // stage 1: group size, default kernels
+  const std::vector<int> sizes = {32, 48, 64, 80, 96};
+  std::vector<double> size_us(sizes.size(), -1.0);
+  for (size_t k : two_rounds(sizes.size())) {
+    int rc = batch_configure(b, (size_t)sizes[k] << 20, {});
+    double us = 0.0;
+    if (!rc) rc = batch_time_sweep(b, 0, (int)b->groups.size(), &us);
+    if (rc) return rc;
+    if (size_us[k] < 0.0 || us < size_us[k]) size_us[k] = us;
+  }
+  size_t best_bytes = b->group_bytes;
+  double best_us = -1.0;
+  for (size_t k = 0; k < sizes.size(); ++k)
+    if (best_us < 0.0 || size_us[k] < best_us) {
+      best_us = size_us[k];
+      best_bytes = (size_t)sizes[k] << 20;
+    }
+  // stage 2: per group, kernel and threads per block
+  int rc = batch_configure(b, best_bytes, {});
+  if (rc) return rc;
+  std::vector<std::pair<int, int>> choice = current_choice(b);
+  for (size_t k = 0; k < choice.size(); ++k) {
+    const int c0 = b->groups[k].c0, c1 = b->groups[k].c1;
+    std::vector<std::pair<int, int>> cand;
+    for (int v : {U1V_QUAD, U1V_PAIR32, U1V_SINGLE})
+      for (int t : {64, 96, 128, 192, 256})
+        if (group_allows(b, c0, c1, v, t)) cand.push_back({v, t});
+    std::vector<double> cand_us(cand.size(), -1.0);
+    for (size_t j : two_rounds(cand.size())) {
+      std::vector<std::pair<int, int>> trial = choice;
+      trial[k] = cand[j];
+      double us = 0.0;
+      rc = batch_configure(b, best_bytes, trial);
+      if (!rc) rc = batch_time_sweep(b, (int)k, (int)k + 1, &us);
+      if (rc) return rc;
+      if (cand_us[j] < 0.0 || us < cand_us[j]) cand_us[j] = us;
+    }
+    double best_k_us = -1.0;
+    for (size_t j = 0; j < cand.size(); ++j)
+      if (best_k_us < 0.0 || cand_us[j] < best_k_us) {
+        best_k_us = cand_us[j];
+        choice[k] = cand[j];
+      }
+  }
+  rc = batch_configure(b, best_bytes, choice);
+  double tuned_us = 0.0;
+  if (!rc) rc = batch_time_sweep(b, 0, (int)b->groups.size(), &tuned_us);
+  if (rc) return rc;
+  if (tuned_us > best_us) {  // the per-group choices did not add up to a faster sweep
+    rc = batch_configure(b, best_bytes, {});
+    if (rc) return rc;
+    tuned_us = best_us;
+  }
+  u1i::dev_free(b->backup);
+  b->backup = nullptr;
+  BatchTuneRec rec{b->group_bytes, current_choice(b)};
+  std::lock_guard<std::mutex> lock(g_btune_mu);
+  g_btune[key] = rec;
+  batch_tune_save(key, rec, tuned_us);
+  return U1_OK;
+}
+
+extern "C" int u1_batch_tune(u1_batch *b, int *group_mb) {
+  u1i::NvtxRange nvtx_range("u1_batch_tune");
+  if (!b) return bfail(U1_ERR_INVALID, "u1_batch_tune: null batch");
+  U1_CUDA_TRY(cudaSetDevice(b->ctx->device));
+  int rc = batch_tune(b);
+  if (rc) {
+    if (b->backup) {  // a failed trial: put the links and pass counter back
+      cudaMemcpyAsync(b->links, b->backup, b->total_links * sizeof(float2), cudaMemcpyDeviceToDevice, b->stream);
+      const unsigned long long pass0 = b->pass;
+      cudaMemcpyAsync(b->pass_dev, &pass0, sizeof(pass0), cudaMemcpyHostToDevice, b->stream);
+      cudaStreamSynchronize(b->stream);
+      u1i::dev_free(b->backup);
+      b->backup = nullptr;
+    }
+    return rc;
+  }
+  if (group_mb) *group_mb = (int)std::min<size_t>(b->group_bytes >> 20, (size_t)INT_MAX);
+  return U1_OK;
+}
+
+extern "C" int u1_batch_configure(u1_batch *b, int group_mb, int ngroups, const int *variants, const int *threads) {
+  if (!b || ngroups < 0 || (ngroups > 0 && (!variants || !threads)))
+    return bfail(U1_ERR_INVALID, "u1_batch_configure: bad argument");
+  U1_CUDA_TRY(cudaSetDevice(b->ctx->device));
+  std::vector<std::pair<int, int>> choice;
+  for (int k = 0; k < ngroups; ++k) choice.push_back({variants[k], threads[k]});
+  const size_t bytes = group_mb > 0 ? (size_t)group_mb << 20 : b->group_bytes;
+  return batch_configure(b, bytes, choice);
+}
+
+extern "C" int u1_batch_group_info(const u1_batch *b, int group, int out[4]) {
+  if (!b || !out || group < 0 || group >= (int)b->groups.size())
+    return bfail(U1_ERR_INVALID, "u1_batch_group_info: bad argument");
+  const BatchGroup &g = b->groups[group];
+  out[0] = g.c0;
+  out[1] = g.c1;
+  out[2] = g.variant;
+  out[3] = g.threads;
   return U1_OK;
 }

@@ -228,9 +228,43 @@ __device__ __forceinline__ void fma4(float4 &acc, const float4 w, float h) {
   acc.w = fmaf(w.w, h, acc.w);
 }
 
+// The mixture transform of one active plaquette: forward, the change dy of
+// its updated link and log H'(xc); INV, the inverse transform (bisection on
+// the monotone H, as k_ncp_inverse): the change dx that undoes a forward step
+// and log H'(xs) at the solution.
+template <bool INV>
+__device__ __forceinline__ float layer_transform(float P, const float *__restrict__ pp, int K, float &logd) {
+  Mix m;
+  float g[kMaxK], gp[kMaxK], s, c;
+  if (!INV) {
+    const float xc = remainderf(P, kTwoPi);
+    mix_eval(xc, pp, K, m, g, gp, s, c);
+    logd = logf(m.Hp);
+    return m.H + pp[2 * K] - xc;
+  }
+  const float shift = pp[2 * K];
+  const float z = remainderf(P - shift, kTwoPi);
+  float lo = -3.14159265358979f, hi = 3.14159265358979f;
+  for (int it = 0; it < 40; ++it) {
+    const float mid = 0.5f * (lo + hi);
+    mix_eval(mid, pp, K, m, g, gp, s, c);
+    if (m.H < z)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  const float xs = 0.5f * (lo + hi);
+  mix_eval(xs, pp, K, m, g, gp, s, c);
+  logd = logf(m.Hp);
+  return xs - z - shift;
+}
+
 // Shared memory (floats, each part a multiple of 4): th[2 LL], P[LL], ctx[2 LL],
 // hid[H LL], w1t[18 H] ([ci*9 + k][c]), b1[H], w2t[9 H CP] ([ci*9 + k][o],
 // outputs padded to CP = round4(2K+1) with zeros), b2[CP], prm[LL/4 * CP].
+// INV: the inverse layer (the context plaquettes hold no updated link, so the
+// same parameters come out; the transform is inverted), as Coupling.inverse.
+template <bool INV>
 __global__ void __launch_bounds__(256)
     k_flow_layer_forward(const float *__restrict__ th_in, float *__restrict__ th_out, float *__restrict__ logdet,
                          int L, int mu, int off, int K, int H, const float *__restrict__ W1,
@@ -325,13 +359,9 @@ __global__ void __launch_bounds__(256)
   for (int a = tid; a < nact; a += nt) {
     int x1, x0;
     active_pos(a, L, mu, off, x1, x0);
-    const float *pp = prm + a * CP;
-    const float xc = remainderf(P[x1 * L + x0], kTwoPi);
-    Mix m;
-    float g[kMaxK], gp[kMaxK], s, c;
-    mix_eval(xc, pp, K, m, g, gp, s, c);
-    const float dy = m.H + pp[2 * K] - xc;
-    ld += (double)logf(m.Hp);
+    float lg;
+    const float dy = layer_transform<INV>(P[x1 * L + x0], prm + a * CP, K, lg);
+    ld += (double)lg;
     if (mu == 0)
       th[x1 * L + x0] += dy;
     else
@@ -351,33 +381,48 @@ __global__ void __launch_bounds__(256)
 }
 
 // ---------------------------------------------------------------------------
-// Backward of k_flow_layer_forward for one configuration per block.  The
-// forward is recomputed in shared memory (plaquettes, context, conv1
-// pre-activations, parameters); then, given gth_out (dL/dtheta_out) and
-// gld (dL/dlogdet), the adjoint runs backwards through the transform, conv2,
-// the LeakyReLU, conv1, the context and the plaquette map:
+// Backward of k_flow_layer_forward<INV> for one configuration per block, for
+// L up to 32.  The forward is recomputed (plaquettes, context, then the
+// parameters, accumulated chunk by chunk over the hidden channels); then,
+// given gth_out (dL/dtheta_out) and gld (dL/dlogdet), the adjoint runs
+// backwards through the transform, conv2, the LeakyReLU, conv1, the context
+// and the plaquette map:
 //   gth_in = gth_out + plaquette-adjoint(gP),
 //   gP = [active] d/dP of the transform + [frozen] (-sin P, cos P) . g_context.
-// Convolution adjoints are written as gathers (each output element sums over
-// the inputs that read it), so no atomics are needed.  Weight gradients (with
-// respect to the bf16-rounded weights the forward used, passed straight to
-// the FP32 master weights) go to per-block partials wpart[b][:] =
-// (gW1[c][ci][k], gB1[c], gW2[o][ci][k], gB2[o]), summed over blocks in a
-// fixed order by k_flow_wgrad_reduce.  L <= 16 (shared-memory size).
+// Only Cc hidden channels (8, or 4 when H % 8 != 0) are held in shared memory
+// at a time: their conv1 pre-activations are recomputed from the context
+// (18 multiply-adds per channel and pixel) for the parameter pass and again
+// for the adjoint pass, which for each chunk forms dL/dpre, the chunk's
+// weight gradients and its share of the context gradient.  This keeps an
+// L = 32, H = 32 layer at about 157 KB of shared memory (the whole hidden
+// layer and its gradient would take 256 KB).  Convolution adjoints are
+// gathers (each output sums over the inputs that read it), so no atomics;
+// weight gradients (with respect to the bf16-rounded weights the forward
+// used, passed straight to the FP32 master weights) go to per-block partials
+// wpart[b][:] = (gW1[c][ci][k], gB1[c], gW2[o][ci][k], gB2[o]), summed over
+// blocks in a fixed order by k_flow_wgrad_reduce.
+__device__ __forceinline__ int nbr_at(int p, int k, int L) {  // pixel at offset k (ky-major) of pixel p
+  int yy = p / L + k / 3 - 1, xx = p % L + k % 3 - 1;
+  yy = yy < 0 ? yy + L : (yy >= L ? yy - L : yy);
+  xx = xx < 0 ? xx + L : (xx >= L ? xx - L : xx);
+  return yy * L + xx;
+}
+__device__ __forceinline__ float lrelu(float v, float slope) { return v > 0.f ? v : slope * v; }
+
+template <bool INV>
 __global__ void __launch_bounds__(256)
     k_flow_layer_backward(const float *__restrict__ th_in, const float *__restrict__ gth_out,
                           const float *__restrict__ gld, float *__restrict__ gth_in, float *__restrict__ wpart, int L,
-                          int mu, int off, int K, int H, const float *__restrict__ W1, const float *__restrict__ B1,
-                          const float *__restrict__ W2, const float *__restrict__ B2, float slope) {
+                          int mu, int off, int K, int H, int Cc, const float *__restrict__ W1,
+                          const float *__restrict__ B1, const float *__restrict__ W2, const float *__restrict__ B2,
+                          float slope) {
   extern __shared__ float4 sm4[];
   float *sm = reinterpret_cast<float *>(sm4);
-  const int LL = L * L, C2 = 2 * K + 1, CP = (C2 + 3) & ~3, nact = LL / 4;
+  const int LL = L * L, C2 = 2 * K + 1, CP = (C2 + 3) & ~3, nact = LL / 4, ng = CP / 4;
   float *th = sm;                  // 2 LL
   float *P = th + 2 * LL;          // LL
   float *ctx = P + LL;             // 2 LL
-  float *pre = ctx + 2 * LL;       // H LL   conv1 pre-activations
-  float *gh = pre + H * LL;        // H LL   dL/dhidden, then dL/dpre
-  float *w1t = gh + H * LL;        // 18 H   [ci*9 + k][c]
+  float *w1t = ctx + 2 * LL;       // 18 H   [ci*9 + k][c]
   float *b1 = w1t + 18 * H;        // H
   float *w2t = b1 + H;             // 9 H CP [ci*9 + k][o]
   float *b2 = w2t + 9 * H * CP;    // CP
@@ -385,9 +430,11 @@ __global__ void __launch_bounds__(256)
   float *gprm = prm + nact * CP;   // nact CP
   float *gctx = gprm + nact * CP;  // 2 LL
   float *gP = gctx + 2 * LL;       // LL
-  int *amap = reinterpret_cast<int *>(gP + LL);  // LL: active index of a plaquette, or -1
-  int *nbt = amap + LL;                          // 9 LL: nbt[k * LL + p] = pixel at offset k of p
-  int *apos = nbt + 9 * LL;                      // nact: pixel of active plaquette a
+  float *hc = gP + LL;             // Cc LL  pre-activations of the chunk's channels
+  float *ghc = hc + Cc * LL;       // Cc LL  dL/dpre of the chunk's channels
+  float *gw1h = ghc + Cc * LL;     // 36 Cc  gW1 of the chunk, two pixel halves
+  int *amap = reinterpret_cast<int *>(gw1h + 36 * Cc);  // LL: active index of a plaquette, or -1
+  int *apos = amap + LL;                                // nact: pixel of active plaquette a
   const int nt = blockDim.x, tid = threadIdx.x, b = blockIdx.x;
   const float *src = th_in + (size_t)b * 2 * LL;
   const float *go = gth_out + (size_t)b * 2 * LL;
@@ -404,10 +451,7 @@ __global__ void __launch_bounds__(256)
   for (int t = tid; t < CP; t += nt) b2[t] = t < C2 ? bf16_round(B2[t]) : 0.f;
   for (int p = tid; p < LL; p += nt) {
     amap[p] = -1;
-    int o9[9];
-    nbr9(p / L, p % L, L, o9);
-#pragma unroll
-    for (int k = 0; k < 9; ++k) nbt[k * LL + p] = o9[k];
+    gP[p] = 0.f;
   }
   __syncthreads();
   for (int a = tid; a < nact; a += nt) {
@@ -416,7 +460,6 @@ __global__ void __launch_bounds__(256)
     amap[x1 * L + x0] = a;
     apos[a] = x1 * L + x0;
   }
-  // ---- forward recomputation
   for (int p = tid; p < LL; p += nt) {
     const int x0 = p % L, x1 = p / L;
     const int x0p = x0 + 1 == L ? 0 : x0 + 1, x1p = x1 + 1 == L ? 0 : x1 + 1;
@@ -430,49 +473,57 @@ __global__ void __launch_bounds__(256)
     ctx[p] = frozen ? cs : 0.f;
     ctx[LL + p] = frozen ? sn : 0.f;
   }
+  for (int q = tid; q < nact * CP; q += nt) prm[q] = b2[q % CP];
+  for (int t = tid; t < 2 * LL; t += nt) gctx[t] = 0.f;
   __syncthreads();
   const float4 *w1v = reinterpret_cast<const float4 *>(w1t);
-  for (int p = tid; p < LL; p += nt) {
-    float in[18];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) {
-      const int q = nbt[k * LL + p];
-      in[k] = ctx[q];
-      in[9 + k] = ctx[LL + q];
-    }
-    for (int c4 = 0; c4 < H; c4 += 4) {
-      float4 acc = make_float4(b1[c4], b1[c4 + 1], b1[c4 + 2], b1[c4 + 3]);
-#pragma unroll
-      for (int r = 0; r < 18; ++r) fma4(acc, w1v[(r * H + c4) >> 2], in[r]);
-      pre[(c4 + 0) * LL + p] = acc.x;
-      pre[(c4 + 1) * LL + p] = acc.y;
-      pre[(c4 + 2) * LL + p] = acc.z;
-      pre[(c4 + 3) * LL + p] = acc.w;
-    }
-  }
-  __syncthreads();
   const float4 *w2v = reinterpret_cast<const float4 *>(w2t);
-  const int ng = CP / 4;
-  for (int q = tid; q < nact * ng; q += nt) {
-    const int a = q / ng, og = q - a * ng;
-    const int pa = apos[a];
-    float4 acc = make_float4(b2[og * 4], b2[og * 4 + 1], b2[og * 4 + 2], b2[og * 4 + 3]);
-    for (int ci = 0; ci < H; ++ci) {
-      const float *pc = pre + ci * LL;
+  // conv1 pre-activations of channels c0 .. c0+Cc-1 into hc
+  auto conv1_chunk = [&](int c0) {
+    for (int p = tid; p < LL; p += nt) {
+      int o9[9];
+      nbr9(p / L, p % L, L, o9);
+      float in[18];
 #pragma unroll
       for (int k = 0; k < 9; ++k) {
-        const float v = pc[nbt[k * LL + pa]];
-        fma4(acc, w2v[((ci * 9 + k) * CP >> 2) + og], v > 0.f ? v : slope * v);
+        in[k] = ctx[o9[k]];
+        in[9 + k] = ctx[LL + o9[k]];
+      }
+      for (int c4 = 0; c4 < Cc; c4 += 4) {
+        const int c = c0 + c4;
+        float4 acc = make_float4(b1[c], b1[c + 1], b1[c + 2], b1[c + 3]);
+#pragma unroll
+        for (int r = 0; r < 18; ++r) fma4(acc, w1v[(r * H + c) >> 2], in[r]);
+        hc[(c4 + 0) * LL + p] = acc.x;
+        hc[(c4 + 1) * LL + p] = acc.y;
+        hc[(c4 + 2) * LL + p] = acc.z;
+        hc[(c4 + 3) * LL + p] = acc.w;
       }
     }
-    float *dst = prm + a * CP + og * 4;
-    dst[0] = acc.x;
-    dst[1] = acc.y;
-    dst[2] = acc.z;
-    dst[3] = acc.w;
+  };
+  // ---- forward recomputation: parameters, summed over the hidden channels in order
+  for (int c0 = 0; c0 < H; c0 += Cc) {
+    conv1_chunk(c0);
+    __syncthreads();
+    for (int q = tid; q < nact * ng; q += nt) {
+      const int a = q / ng, og = q - a * ng;
+      int o9[9];
+      const int pa = apos[a];
+      nbr9(pa / L, pa % L, L, o9);
+      float *dst = prm + a * CP + og * 4;
+      float4 acc = make_float4(dst[0], dst[1], dst[2], dst[3]);
+      for (int cl = 0; cl < Cc; ++cl) {
+        const float *pc = hc + cl * LL;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) fma4(acc, w2v[(((c0 + cl) * 9 + k) * CP >> 2) + og], lrelu(pc[o9[k]], slope));
+      }
+      dst[0] = acc.x;
+      dst[1] = acc.y;
+      dst[2] = acc.z;
+      dst[3] = acc.w;
+    }
+    __syncthreads();
   }
-  for (int p = tid; p < LL; p += nt) gP[p] = 0.f;
-  __syncthreads();
   // ---- transform adjoint: gprm and the active plaquettes' gP
   const float gl = gld ? gld[b] : 0.f;
   for (int a = tid; a < nact; a += nt) {
@@ -480,109 +531,129 @@ __global__ void __launch_bounds__(256)
     const int x1 = pa / L, x0 = pa - x1 * L;
     const float *pp = prm + a * CP;
     float *gpo = gprm + a * CP;
-    const float xc = remainderf(P[pa], kTwoPi);
+    const int link = mu == 0 ? pa : LL + x1 * L + (x0 + 1 == L ? 0 : x0 + 1);
+    const float gout = go[link];
     Mix m;
     float g[kMaxK], gp[kMaxK], s, c;
-    mix_eval(xc, pp, K, m, g, gp, s, c);
-    const int link = mu == 0 ? pa : LL + x1 * L + (x0 + 1 == L ? 0 : x0 + 1);
-    const float gdy = go[link];
-    float gxc;
-    mix_backward(m, g, gp, s, c, K, gdy, gl / m.Hp, gxc, gpo);
+    if (!INV) {  // dy = H(xc) + shift - xc, logd = log H'(xc)
+      const float xc = remainderf(P[pa], kTwoPi);
+      mix_eval(xc, pp, K, m, g, gp, s, c);
+      float gxc;
+      mix_backward(m, g, gp, s, c, K, gout, gl / m.Hp, gxc, gpo);
+      gpo[2 * K] = gout;
+      gP[pa] = gxc - gout;
+    } else {  // dx = xs - z - shift with H(xs) = z = P - shift (mod 2 pi), logd = log H'(xs)
+      const float shift = pp[2 * K];
+      const float z = remainderf(P[pa] - shift, kTwoPi);
+      float lo = -3.14159265358979f, hi = 3.14159265358979f;
+      for (int it = 0; it < 40; ++it) {
+        const float mid = 0.5f * (lo + hi);
+        mix_eval(mid, pp, K, m, g, gp, s, c);
+        if (m.H < z)
+          lo = mid;
+        else
+          hi = mid;
+      }
+      mix_eval(0.5f * (lo + hi), pp, K, m, g, gp, s, c);
+      // implicit differentiation at the solution, as k_ncp_inverse_backward
+      float dHp_dx = 0.f;
+      for (int k = 0; k < K; ++k) {
+        const float al = m.al[k];
+        const float den = c * c + al * al * s * s;
+        dHp_dx += m.w[k] * (-al * s * c * (al * al - 1.f)) / (den * den);
+      }
+      const float r = (gout + gl * dHp_dx / m.Hp) / m.Hp;  // dL/dz through xs
+      float unused;
+      mix_backward(m, g, gp, s, c, K, -r, gl / m.Hp, unused, gpo);
+      gpo[2 * K] = -r;
+      gP[pa] = r - gout;
+    }
     for (int k = 0; k < K; ++k)
       if (fabsf(pp[k]) > 8.f) gpo[k] = 0.f;
-    gpo[2 * K] = gdy;
     for (int o = C2; o < CP; ++o) gpo[o] = 0.f;
-    gP[pa] = gxc - gdy;  // dy = H + shift - xc
   }
   __syncthreads();
   float *wp = wpart + (size_t)b * (H * 18 + H + C2 * H * 9 + C2);
   float *gW1 = wp, *gB1 = wp + H * 18, *gW2 = gB1 + H, *gB2 = gW2 + C2 * H * 9;
   const float4 *gpv = reinterpret_cast<const float4 *>(gprm);
-  // gW2[o][ci][k] = sum_a gprm[a][o] h[ci][nbr(a, k)]: one (ci, k) per work item, all outputs
-  for (int e = tid; e < H * 9; e += nt) {
-    const int ci = e / 9, k = e - ci * 9;
-    const float *pc = pre + ci * LL;
-    const int *nk = nbt + k * LL;
-    float4 acc[5];
-#pragma unroll
-    for (int j = 0; j < 5; ++j) acc[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int a = 0; a < nact; ++a) {
-      const float v0 = pc[nk[apos[a]]];
-      const float v = v0 > 0.f ? v0 : slope * v0;
-#pragma unroll
-      for (int j = 0; j < 5; ++j)
-        if (j < ng) fma4(acc[j], gpv[a * ng + j], v);
-    }
-#pragma unroll
-    for (int j = 0; j < 5; ++j) {
-      if (j >= ng) break;
-      const float av[4] = {acc[j].x, acc[j].y, acc[j].z, acc[j].w};
-#pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        const int o = 4 * j + t;
-        if (o < C2) gW2[(size_t)o * H * 9 + e] = av[t];
-      }
-    }
-  }
   for (int o = tid; o < C2; o += nt) {
     float acc = 0.f;
     for (int a = 0; a < nact; ++a) acc += gprm[a * CP + o];
     gB2[o] = acc;
   }
-  // gh[ci][p] = sum_k sum_o W2[o][ci][k] gprm[a][o] over active a at p - (k offset); then * LeakyReLU'(pre)
-  for (int q = tid; q < H * LL; q += nt) {
-    const int ci = q / LL, p = q - ci * LL;
-    float acc = 0.f;
+  // ---- adjoint, chunk by chunk over the hidden channels
+  for (int c0 = 0; c0 < H; c0 += Cc) {
+    conv1_chunk(c0);
+    __syncthreads();
+    // dL/dpre[c][p] = LeakyReLU'(pre) * sum_k sum_o W2[o][c][k] gprm[a][o] over active a whose offset-k neighbour is p
+    for (int q = tid; q < Cc * LL; q += nt) {
+      const int cl = q / LL, p = q - cl * LL;
+      int o9[9];
+      nbr9(p / L, p % L, L, o9);
+      float acc = 0.f;
 #pragma unroll
-    for (int k = 0; k < 9; ++k) {
-      const int a = amap[nbt[(8 - k) * LL + p]];  // the pixel whose offset-k neighbour is p
-      if (a >= 0) {
-        const float4 *wv = w2v + ((ci * 9 + k) * CP >> 2);
-        for (int og = 0; og < ng; ++og) {
-          const float4 w = wv[og], gg = gpv[a * ng + og];
-          acc = fmaf(w.x, gg.x, fmaf(w.y, gg.y, fmaf(w.z, gg.z, fmaf(w.w, gg.w, acc))));
+      for (int k = 0; k < 9; ++k) {
+        const int a = amap[o9[8 - k]];
+        if (a >= 0) {
+          const float4 *wv = w2v + (((c0 + cl) * 9 + k) * CP >> 2);
+          for (int og = 0; og < ng; ++og) {
+            const float4 w = wv[og], gg = gpv[a * ng + og];
+            acc = fmaf(w.x, gg.x, fmaf(w.y, gg.y, fmaf(w.z, gg.z, fmaf(w.w, gg.w, acc))));
+          }
         }
       }
+      ghc[q] = hc[q] > 0.f ? acc : slope * acc;
     }
-    gh[q] = pre[q] > 0.f ? acc : slope * acc;  // dL/dpre
-  }
-  __syncthreads();
-  // gW1[c][ci][k] = sum_p gpre[c][p] ctx[ci][nbr(p, k)]: one (ci, k, 4 channels) per work item
-  for (int e = tid; e < 18 * (H / 4); e += nt) {
-    const int r = e % 18, c4 = 4 * (e / 18), ci = r / 9, k = r - ci * 9;
-    const float *cx = ctx + ci * LL;
-    const int *nk = nbt + k * LL;
-    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
-    for (int p = 0; p < LL; ++p) {
-      const float v = cx[nk[p]];
-      a0 = fmaf(gh[(c4 + 0) * LL + p], v, a0);
-      a1 = fmaf(gh[(c4 + 1) * LL + p], v, a1);
-      a2 = fmaf(gh[(c4 + 2) * LL + p], v, a2);
-      a3 = fmaf(gh[(c4 + 3) * LL + p], v, a3);
-    }
-    gW1[(c4 + 0) * 18 + r] = a0;
-    gW1[(c4 + 1) * 18 + r] = a1;
-    gW1[(c4 + 2) * 18 + r] = a2;
-    gW1[(c4 + 3) * 18 + r] = a3;
-  }
-  for (int c = tid; c < H; c += nt) {
-    float acc = 0.f;
-    for (int p = 0; p < LL; ++p) acc += gh[c * LL + p];
-    gB1[c] = acc;
-  }
-  // gctx[ci][p] = sum_k sum_c W1[c][ci][k] gpre[c][p - (k offset)]
-  for (int q = tid; q < 2 * LL; q += nt) {
-    const int ci = q / LL, p = q - ci * LL;
-    float acc = 0.f;
+    // gW2[o][c][k] = sum_a gprm[a][o] h[c][nbr(a, k)]: one (c, k, group of four outputs) per work item
+    for (int e = tid; e < Cc * 9 * ng; e += nt) {
+      const int cl = e / (9 * ng), rem = e - cl * 9 * ng, k = rem / ng, og = rem - k * ng;
+      const float *pc = hc + cl * LL;
+      float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int a = 0; a < nact; ++a) fma4(acc, gpv[a * ng + og], lrelu(pc[nbr_at(apos[a], k, L)], slope));
+      const float av[4] = {acc.x, acc.y, acc.z, acc.w};
 #pragma unroll
-    for (int k = 0; k < 9; ++k) {
-      const int pq = nbt[(8 - k) * LL + p];
-      const float *wr = w1t + (ci * 9 + k) * H;
-      for (int c = 0; c < H; ++c) acc = fmaf(wr[c], gh[c * LL + pq], acc);
+      for (int t = 0; t < 4; ++t) {
+        const int o = 4 * og + t;
+        if (o < C2) gW2[(size_t)o * H * 9 + (c0 + cl) * 9 + k] = av[t];
+      }
     }
-    gctx[q] = acc;
+    __syncthreads();
+    // gW1[c][ci][k] = sum_p dL/dpre[c][p] ctx[ci][nbr(p, k)]: (ci*9 + k, c, half of the pixels) per work item
+    for (int e = tid; e < 36 * Cc; e += nt) {
+      const int half = e & 1, rc = e >> 1, r = rc % 18, cl = rc / 18, ci = r / 9, k = r - ci * 9;
+      const float *cx = ctx + ci * LL;
+      const float *gc = ghc + cl * LL;
+      const int p1 = half ? LL : LL / 2;
+      float acc = 0.f;
+      for (int p = half ? LL / 2 : 0; p < p1; ++p) acc = fmaf(gc[p], cx[nbr_at(p, k, L)], acc);
+      gw1h[e] = acc;
+    }
+    for (int cl = tid; cl < Cc; cl += nt) {
+      float acc = 0.f;
+      for (int p = 0; p < LL; ++p) acc += ghc[cl * LL + p];
+      gB1[c0 + cl] = acc;
+    }
+    // gctx[ci][p] += sum_k sum_{c in chunk} W1[c][ci][k] dL/dpre[c][p - (k offset)]
+    for (int q = tid; q < 2 * LL; q += nt) {
+      const int ci = q / LL, p = q - ci * LL;
+      int o9[9];
+      nbr9(p / L, p % L, L, o9);
+      float acc = gctx[q];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        const int pq = o9[8 - k];
+        const float *wr = w1t + (ci * 9 + k) * H + c0;
+        for (int cl = 0; cl < Cc; ++cl) acc = fmaf(wr[cl], ghc[cl * LL + pq], acc);
+      }
+      gctx[q] = acc;
+    }
+    __syncthreads();
+    for (int e = tid; e < 18 * Cc; e += nt) {
+      const int r = e % 18, cl = e / 18;
+      gW1[(c0 + cl) * 18 + r] = gw1h[2 * (cl * 18 + r)] + gw1h[2 * (cl * 18 + r) + 1];
+    }
+    __syncthreads();
   }
-  __syncthreads();
   // context adjoint into gP (frozen plaquettes): ctx = (cos P, sin P)
   for (int p = tid; p < LL; p += nt) {
     const int xn = mu == 0 ? p / L : p % L;
@@ -613,10 +684,13 @@ __global__ void k_flow_wgrad_reduce(const float *__restrict__ wpart, int nb, int
   out[j] = acc;
 }
 
+int flow_chunk(int H) { return H % 8 == 0 ? 8 : 4; }
+
 size_t flow_layer_bwd_smem(int L, int K, int H) {
-  const size_t LL = (size_t)L * L, CP = (2 * K + 1 + 3) & ~3, nact = LL / 4;
-  return sizeof(float) * (2 * LL + LL + 2 * LL + 2 * H * LL + 18 * H + H + 9 * H * CP + CP + 2 * nact * CP +
-                          2 * LL + LL + LL + 9 * LL + nact);
+  const size_t LL = (size_t)L * L, CP = (2 * K + 1 + 3) & ~3, nact = LL / 4, Cc = flow_chunk(H);
+  return sizeof(float) * (2 * LL + LL + 2 * LL + 18 * H + H + 9 * H * CP + CP + 2 * nact * CP + 2 * LL + LL +
+                          2 * Cc * LL + 36 * Cc) +
+         sizeof(int) * (LL + nact);
 }
 
 size_t flow_layer_smem(int L, int K, int H) {
@@ -678,50 +752,86 @@ extern "C" int u1_ncp_inverse_backward(const float *xsol, const float *params, c
   return U1_OK;
 }
 
+namespace {
+template <bool INV>
+int flow_layer_fwd(const char *name, const float *theta_in, float *theta_out, float *logdet, int batch, int L, int mu,
+                   int off, int K, int hidden, const float *W1, const float *B1, const float *W2, const float *B2,
+                   float slope, void *stream) {
+  if (!theta_in || !theta_out || !logdet || !W1 || !B1 || !W2 || !B2)
+    return flfail(U1_ERR_INVALID, std::string(name) + ": null pointer");
+  if (theta_in == theta_out) return flfail(U1_ERR_INVALID, std::string(name) + ": in and out must not alias");
+  if (batch < 1 || L < 4 || L > 32 || L % 4 || (mu != 0 && mu != 1) || off < 0 || off > 3 || K < 1 || K > kMaxK ||
+      hidden < 4 || hidden > 32 || hidden % 4)
+    return flfail(U1_ERR_INVALID, std::string(name) +
+                                      ": bad shape (L a multiple of 4 up to 32, K <= 8, hidden a multiple of 4 up to 32)");
+  const size_t smem = flow_layer_smem(L, K, hidden);
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_flow_layer_forward<INV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return u1i::cuda_fail(e, name);
+  }
+  k_flow_layer_forward<INV><<<batch, 256, smem, (cudaStream_t)stream>>>(theta_in, theta_out, logdet, L, mu, off, K,
+                                                                         hidden, W1, B1, W2, B2, slope);
+  U1_LAUNCH_CHECK(name);
+  return U1_OK;
+}
+
+template <bool INV>
+int flow_layer_bwd(const char *name, const float *theta_in, const float *grad_theta_out, const float *grad_logdet,
+                   float *grad_theta_in, float *wgrad_partials, float *wgrad, int batch, int L, int mu, int off, int K,
+                   int hidden, const float *W1, const float *B1, const float *W2, const float *B2, float slope,
+                   void *stream) {
+  if (!theta_in || !grad_theta_out || !grad_theta_in || !wgrad_partials || !wgrad || !W1 || !B1 || !W2 || !B2)
+    return flfail(U1_ERR_INVALID, std::string(name) + ": null pointer");
+  if (batch < 1 || L < 4 || L > 32 || L % 4 || (mu != 0 && mu != 1) || off < 0 || off > 3 || K < 1 ||
+      K > kMaxK || hidden < 4 || hidden > 32 || hidden % 4)
+    return flfail(U1_ERR_INVALID, std::string(name) +
+                                      ": bad shape (L a multiple of 4 up to 32, K <= 8, hidden a multiple of 4 up to 32)");
+  const size_t smem = flow_layer_bwd_smem(L, K, hidden);
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_flow_layer_backward<INV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return u1i::cuda_fail(e, name);
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  k_flow_layer_backward<INV><<<batch, 256, smem, s>>>(theta_in, grad_theta_out, grad_logdet, grad_theta_in,
+                                                       wgrad_partials, L, mu, off, K, hidden, flow_chunk(hidden), W1,
+                                                       B1, W2, B2, slope);
+  U1_LAUNCH_CHECK(name);
+  const int nw = hidden * 18 + hidden + (2 * K + 1) * hidden * 9 + (2 * K + 1);
+  k_flow_wgrad_reduce<<<(nw + 255) / 256, 256, 0, s>>>(wgrad_partials, batch, nw, wgrad);
+  U1_LAUNCH_CHECK("k_flow_wgrad_reduce");
+  return U1_OK;
+}
+}  // namespace
+
 extern "C" int u1_flow_layer_forward(const float *theta_in, float *theta_out, float *logdet, int batch, int L,
                                      int mu, int off, int K, int hidden, const float *W1, const float *B1,
                                      const float *W2, const float *B2, float slope, void *stream) {
-  if (!theta_in || !theta_out || !logdet || !W1 || !B1 || !W2 || !B2)
-    return flfail(U1_ERR_INVALID, "u1_flow_layer_forward: null pointer");
-  if (theta_in == theta_out) return flfail(U1_ERR_INVALID, "u1_flow_layer_forward: in and out must not alias");
-  if (batch < 1 || L < 4 || L > 32 || L % 4 || (mu != 0 && mu != 1) || off < 0 || off > 3 || K < 1 || K > kMaxK ||
-      hidden < 4 || hidden > 32 || hidden % 4)
-    return flfail(U1_ERR_INVALID,
-                  "u1_flow_layer_forward: bad shape (L a multiple of 4 up to 32, K <= 8, hidden a multiple of 4 up to 32)");
-  const size_t smem = flow_layer_smem(L, K, hidden);
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k_flow_layer_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return u1i::cuda_fail(e, "u1_flow_layer_forward: shared memory");
-  }
-  k_flow_layer_forward<<<batch, 256, smem, (cudaStream_t)stream>>>(theta_in, theta_out, logdet, L, mu, off, K,
-                                                                    hidden, W1, B1, W2, B2, slope);
-  U1_LAUNCH_CHECK("k_flow_layer_forward");
-  return U1_OK;
+  return flow_layer_fwd<false>("u1_flow_layer_forward", theta_in, theta_out, logdet, batch, L, mu, off, K, hidden,
+                               W1, B1, W2, B2, slope, stream);
+}
+
+extern "C" int u1_flow_layer_inverse(const float *theta_in, float *theta_out, float *logdet, int batch, int L,
+                                     int mu, int off, int K, int hidden, const float *W1, const float *B1,
+                                     const float *W2, const float *B2, float slope, void *stream) {
+  return flow_layer_fwd<true>("u1_flow_layer_inverse", theta_in, theta_out, logdet, batch, L, mu, off, K, hidden, W1,
+                              B1, W2, B2, slope, stream);
 }
 
 extern "C" int u1_flow_layer_backward(const float *theta_in, const float *grad_theta_out, const float *grad_logdet,
                                       float *grad_theta_in, float *wgrad_partials, float *wgrad, int batch, int L,
                                       int mu, int off, int K, int hidden, const float *W1, const float *B1,
                                       const float *W2, const float *B2, float slope, void *stream) {
-  if (!theta_in || !grad_theta_out || !grad_theta_in || !wgrad_partials || !wgrad || !W1 || !B1 || !W2 || !B2)
-    return flfail(U1_ERR_INVALID, "u1_flow_layer_backward: null pointer");
-  if (batch < 1 || L < 4 || L > 16 || L % 4 || (mu != 0 && mu != 1) || off < 0 || off > 3 || K < 1 ||
-      K > kMaxK || hidden < 4 || hidden > 32 || hidden % 4)
-    return flfail(U1_ERR_INVALID,
-                  "u1_flow_layer_backward: bad shape (L a multiple of 4 up to 16, K <= 8, hidden a multiple of 4 up to 32)");
-  const size_t smem = flow_layer_bwd_smem(L, K, hidden);
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k_flow_layer_backward, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return u1i::cuda_fail(e, "u1_flow_layer_backward: shared memory");
-  }
-  cudaStream_t s = (cudaStream_t)stream;
-  k_flow_layer_backward<<<batch, 256, smem, s>>>(theta_in, grad_theta_out, grad_logdet, grad_theta_in,
-                                                  wgrad_partials, L, mu, off, K, hidden, W1, B1, W2, B2, slope);
-  U1_LAUNCH_CHECK("k_flow_layer_backward");
-  const int nw = hidden * 18 + hidden + (2 * K + 1) * hidden * 9 + (2 * K + 1);
-  k_flow_wgrad_reduce<<<(nw + 255) / 256, 256, 0, s>>>(wgrad_partials, batch, nw, wgrad);
-  U1_LAUNCH_CHECK("k_flow_wgrad_reduce");
-  return U1_OK;
+  return flow_layer_bwd<false>("u1_flow_layer_backward", theta_in, grad_theta_out, grad_logdet, grad_theta_in,
+                               wgrad_partials, wgrad, batch, L, mu, off, K, hidden, W1, B1, W2, B2, slope, stream);
+}
+
+extern "C" int u1_flow_layer_inverse_backward(const float *theta_in, const float *grad_theta_out,
+                                              const float *grad_logdet, float *grad_theta_in, float *wgrad_partials,
+                                              float *wgrad, int batch, int L, int mu, int off, int K, int hidden,
+                                              const float *W1, const float *B1, const float *W2, const float *B2,
+                                              float slope, void *stream) {
+  return flow_layer_bwd<true>("u1_flow_layer_inverse_backward", theta_in, grad_theta_out, grad_logdet, grad_theta_in,
+                              wgrad_partials, wgrad, batch, L, mu, off, K, hidden, W1, B1, W2, B2, slope, stream);
 }

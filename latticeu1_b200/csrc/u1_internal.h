@@ -1,5 +1,6 @@
 // Host-side object layout behind the C ABI (include/u1_b200.h).
 #pragma once
+#include <nvtx3/nvToolsExt.h>
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -54,6 +55,8 @@ struct u1_lattice {
   bool use_graphs = true;
   int variant = U1V_AUTO;          // update kernel variant (U1V_AUTO: tune on first update)
   int block = 256;                 // threads per block of the phase kernels (tuned with the variant)
+  int remap_block = -1;            // block size remap_sms was worked out for
+  int remap_sms = 0;               // SM-local block order of the four-site kernels (0: launch order)
   // Metropolis proposal: half-width delta (0: the reference's whole-circle
   // theta' = 2 pi u), win = delta/pi as used by the kernels, hits per link
   double delta = 0.0;
@@ -63,13 +66,36 @@ struct u1_lattice {
   // persistent sweep (U1V_WAVE): per-tile phase flags, then ticket and error word
   unsigned int *wave_state = nullptr;
   int wave_ok = -1;                // -1 unknown, 0 not usable, 1 usable
+  unsigned wave_spin_limit = 0;    // polls per neighbour wait (0: the kernel's default)
+  int wave_stall_tile = -1;        // test hook: this tile never publishes its phases (-1: none)
 };
 
 namespace u1i {
+// NVTX range around a host entry point: named ranges for nsys / ncu
+// (--nvtx --nvtx-include); without an attached tool the push and pop return
+// at once.
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange &) = delete;
+  NvtxRange &operator=(const NvtxRange &) = delete;
+};
 void set_error(const std::string &msg);
 int cuda_fail(cudaError_t e, const char *what);
 extern std::atomic<unsigned long long> g_launches;
 int ensure_scratch(u1_lattice *lat, size_t partial_doubles, size_t out_doubles);
+// Every device allocation of the library: cudaMalloc / cudaFree unless the
+// caller installed its own pair (u1_set_device_allocator).  A failed
+// allocation returns cudaErrorMemoryAllocation and leaves *p null.
+cudaError_t dev_alloc(void **p, size_t bytes);
+cudaError_t dev_free(void *p);
+template <class T>
+inline cudaError_t dev_alloc(T **p, size_t bytes) {
+  void *v = nullptr;
+  cudaError_t e = dev_alloc(&v, bytes);
+  *p = static_cast<T *>(v);
+  return e;
+}
 // Geometry from the ABI struct (Grid mapping of the reference's
 // SetupLatticeParameters); U1_ERR_INVALID on odd extents.
 int make_geom(const u1_geom *geom, u1b::GeomK &g);

@@ -24,8 +24,12 @@
 //    without ordering between them) race on the array.
 //  * The first call on a device looks up the array's device address on that
 //    device (cudaGetSymbolAddress, with the device current); make that first
-//    call before any stream capture.  The current device must own links,
-//    out and stream.
+//    call before any stream capture.  The address belongs to the device's
+//    current CUDA context: when that context changes (cudaDeviceReset, or a
+//    host framework that tears its context down and creates a new one) the
+//    next call looks the address up again.  The current device must own
+//    links, out and stream.
+#include <cuda.h>
 #include <mutex>
 #include <string>
 
@@ -48,9 +52,29 @@ constexpr size_t kScratchDoubles = (size_t)kNoAllocMaxBlocks * 6 + 32;
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
 std::mutex g_noalloc_mu;
-double *g_noalloc_addr[kNoAllocMaxDevices] = {};
+struct ScratchAddr {
+  CUcontext ctx = nullptr;  // context the address was looked up in
+  double *addr = nullptr;
+};
+ScratchAddr g_noalloc_addr[kNoAllocMaxDevices];
 
-// Device address of g_noalloc_scratch on the current device (set-up once per device).
+// The driver's cuCtxGetCurrent, reached through the runtime (no link against
+// libcuda); null if the driver does not provide it.
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+CtxGetCurrentFn ctx_get_current() {
+  static const CtxGetCurrentFn fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<CtxGetCurrentFn>(p);
+  }();
+  return fn;
+}
+
+// Device address of g_noalloc_scratch on the current device, looked up once
+// per device and again whenever the device's current context changes.
 int noalloc_scratch(double **out) {
   int dev = -1;
   U1_CUDA_TRY(cudaGetDevice(&dev));
@@ -58,14 +82,18 @@ int noalloc_scratch(double **out) {
     u1i::set_error("u1_measure_noalloc: device ordinal out of range");
     return U1_ERR_UNSUPPORTED;
   }
+  CUcontext cur = nullptr;
+  if (CtxGetCurrentFn f = ctx_get_current()) f(&cur);
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
+  ScratchAddr &c = g_noalloc_addr[dev];
+  if (!c.addr || c.ctx != cur) {
     void *p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return u1i::cuda_fail(e, "u1_measure_noalloc: cudaGetSymbolAddress");
-    g_noalloc_addr[dev] = (double *)p;
+    c.addr = (double *)p;
+    c.ctx = cur;
   }
-  *out = g_noalloc_addr[dev];
+  *out = c.addr;
   return U1_OK;
 }
 
@@ -73,6 +101,8 @@ template <int D>
 int launch_noalloc(const float2 *links, const GeomK &g, double *scratch, double *out, cudaStream_t s) {
   const MeasK m = measure_layout(g);
   const int nb = m.nb_plaq + m.nb_poly;
+  // Unreachable after the caller's V/2 check (nb_plaq <= V/2 / 256 and
+  // nb_poly <= V/8 / 256); kept so the array can never be overrun.
   if (nb > kNoAllocMaxBlocks) {
     u1i::set_error("u1_measure_noalloc: measurement needs more blocks than the fixed scratch array holds");
     return U1_ERR_INVALID;

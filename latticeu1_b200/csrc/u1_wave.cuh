@@ -39,9 +39,11 @@ struct WaveArgs {
   unsigned int *ticket;        // blocks finished (0 at launch)
   unsigned int *err;           // 1 + phase of a wait that ran out (0: none)
   unsigned long long *pass_rw; // the pass counter (same address as a.pass_dev)
+  unsigned spin_limit;         // polls per neighbour wait (>= 1)
+  int stall_tile;              // a tile that never publishes its phases (-1: none; test hook)
 };
 
-constexpr unsigned kWaveSpinLimit = 1u << 21;  // about a second of polling with the back-off
+constexpr unsigned kWaveSpinLimit = 1u << 21;  // default: about a second of polling with the back-off
 
 __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p) {
   unsigned v;
@@ -115,7 +117,7 @@ static __global__ void __launch_bounds__(256, 8) k_sweep_wave(const WaveArgs w) 
         // acquire polls (measured faster here than relaxed polls plus one fence)
         while (ld_acquire_gpu(w.flags + watch) < (unsigned)ph) {
           if (n > 16) __nanosleep(32);  // back off after a short spin
-          if (++n == kWaveSpinLimit) {
+          if (++n >= w.spin_limit) {
             atomicMax(w.err, (unsigned)ph + 1u);
             failed = 1;
             break;
@@ -138,7 +140,7 @@ static __global__ void __launch_bounds__(256, 8) k_sweep_wave(const WaveArgs w) 
     else
       wave_dispatch<D, false>(a, mu, meas, i, slot);
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && tile != w.stall_tile) {
       __threadfence();
       st_release_gpu(w.flags + tile, (unsigned)ph + 1u);
     }

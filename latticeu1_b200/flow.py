@@ -120,26 +120,32 @@ def ncp_inverse(y, params, K):
 
 class _FusedLayer(torch.autograd.Function):
     """A whole coupling layer as the library's fused kernels:
-    (theta, W1, B1, W2, B2) -> (theta_out, logdet) with u1_flow_layer_forward,
-    gradients with u1_flow_layer_backward (L <= 16)."""
+    (theta, W1, B1, W2, B2) -> (theta_out, logdet) with u1_flow_layer_forward
+    (or, inverse, u1_flow_layer_inverse), gradients with
+    u1_flow_layer_backward (u1_flow_layer_inverse_backward); L <= 32."""
 
     @staticmethod
-    def forward(ctx, th, W1, B1, W2, B2, meta):
+    def forward(ctx, th, W1, B1, W2, B2, meta, inverse=False):
         L, mu, off, K, H, slope = meta
         th = th.contiguous()
         out = torch.empty_like(th)
         ld = torch.empty(th.shape[0], device=th.device)
+        fn, name = ((lib.u1_flow_layer_inverse, "u1_flow_layer_inverse") if inverse
+                    else (lib.u1_flow_layer_forward, "u1_flow_layer_forward"))
         with torch.cuda.device(th.device):
-            check(lib.u1_flow_layer_forward(_p(th), _p(out), _p(ld), th.shape[0], L, mu, off, K, H, _p(W1), _p(B1),
-                                            _p(W2), _p(B2), C.c_float(slope), _stream(th)), "u1_flow_layer_forward")
+            check(fn(_p(th), _p(out), _p(ld), th.shape[0], L, mu, off, K, H, _p(W1), _p(B1), _p(W2), _p(B2),
+                     C.c_float(slope), _stream(th)), name)
         ctx.save_for_backward(th, W1, B1, W2, B2)
         ctx.meta = meta
+        ctx.inverse = inverse
         return out, ld
 
     @staticmethod
     def backward(ctx, g_out, g_ld):
         th, W1, B1, W2, B2 = ctx.saved_tensors
         L, mu, off, K, H, slope = ctx.meta
+        fn, name = ((lib.u1_flow_layer_inverse_backward, "u1_flow_layer_inverse_backward") if ctx.inverse
+                    else (lib.u1_flow_layer_backward, "u1_flow_layer_backward"))
         B = th.shape[0]
         C2 = 2 * K + 1
         nw = H * 18 + H + C2 * H * 9 + C2
@@ -149,9 +155,8 @@ class _FusedLayer(torch.autograd.Function):
         part = torch.empty((B, nw), device=th.device)
         wg = torch.empty(nw, device=th.device)
         with torch.cuda.device(th.device):
-            check(lib.u1_flow_layer_backward(_p(th), _p(g_out), _p(g_ld), _p(gth), _p(part), _p(wg), B, L, mu, off,
-                                             K, H, _p(W1), _p(B1), _p(W2), _p(B2), C.c_float(slope), _stream(th)),
-                  "u1_flow_layer_backward")
+            check(fn(_p(th), _p(g_out), _p(g_ld), _p(gth), _p(part), _p(wg), B, L, mu, off, K, H, _p(W1), _p(B1),
+                     _p(W2), _p(B2), C.c_float(slope), _stream(th)), name)
         o = 0
         gW1 = wg[o:o + H * 18].view_as(W1)
         o += H * 18
@@ -160,7 +165,7 @@ class _FusedLayer(torch.autograd.Function):
         gW2 = wg[o:o + C2 * H * 9].view_as(W2)
         o += C2 * H * 9
         gB2 = wg[o:o + C2]
-        return gth, gW1, gB1, gW2, gB2, None
+        return gth, gW1, gB1, gW2, gB2, None, None
 
 
 def plaquettes_no(th: torch.Tensor) -> torch.Tensor:
@@ -236,11 +241,17 @@ class Coupling(nn.Module):
         return torch.stack(parts, 1).reshape_as(th)
 
     def forward_fused(self, th: torch.Tensor):
-        """The layer as the library's fused forward/backward kernels (L <= 16
-        for gradients): bf16-rounded weights, FP32 arithmetic."""
+        """The layer as the library's fused forward/backward kernels:
+        bf16-rounded weights, FP32 arithmetic."""
         c1, c2 = self.net[0], self.net[2]
         meta = (self.L, self.mu, self.off, self.K, c1.out_channels, self.net[1].negative_slope)
         return _FusedLayer.apply(th, c1.weight, c1.bias, c2.weight, c2.bias, meta)
+
+    def inverse_fused(self, th: torch.Tensor):
+        """The inverse layer as the library's fused kernels (differentiable)."""
+        c1, c2 = self.net[0], self.net[2]
+        meta = (self.L, self.mu, self.off, self.K, c1.out_channels, self.net[1].negative_slope)
+        return _FusedLayer.apply(th, c1.weight, c1.bias, c2.weight, c2.bias, meta, True)
 
     def forward(self, th: torch.Tensor):
         B = th.shape[0]
@@ -283,7 +294,7 @@ class Flow2D(nn.Module):
 
     def sample(self, B: int, generator: torch.Generator | None = None, fused: bool = False):
         """(theta, log q(theta)) for B flow samples; fused: each layer through
-        the library's fused kernels (differentiable, L <= 16)."""
+        the library's fused kernels (differentiable)."""
         dev = self.perm.device
         th = torch.rand((B, 2, self.L, self.L), device=dev, generator=generator) * TWO_PI
         logq = torch.full((B,), self.log_prior, device=dev)
@@ -314,11 +325,12 @@ class Flow2D(nn.Module):
                 th, buf = buf, th
         return torch.remainder(th, TWO_PI), logq
 
-    def log_prob(self, th: torch.Tensor) -> torch.Tensor:
-        """log q(theta) through the inverse flow."""
+    def log_prob(self, th: torch.Tensor, fused: bool = False) -> torch.Tensor:
+        """log q(theta) through the inverse flow; fused: each inverse layer
+        through the library's fused kernels (differentiable)."""
         logq = torch.full((th.shape[0],), self.log_prior, device=th.device)
         for layer in reversed(self.layers):
-            th, ld = layer.inverse(th)
+            th, ld = layer.inverse_fused(th) if fused else layer.inverse(th)
             logq = logq - ld
         return logq
 
@@ -374,8 +386,8 @@ class Flow2D(nn.Module):
         step.graph = graph
         return step, static
 
-    def forward_kl_step(self, opt, data: torch.Tensor) -> float:
-        loss = -self.log_prob(data).mean()
+    def forward_kl_step(self, opt, data: torch.Tensor, fused: bool = False) -> float:
+        loss = -self.log_prob(data, fused=fused).mean()
         opt.zero_grad(set_to_none=True)
         loss.backward()
         opt.step()
@@ -497,7 +509,7 @@ def run_experiment(L: int = 16, beta: float = 2.0, n_layers: int = 8, K: int = 6
     from scipy.special import ive
     torch.manual_seed(seed)
     if fused is None:
-        fused = L <= 16  # the fused backward kernel covers L <= 16
+        fused = L <= 32  # the fused layer kernels (forward, inverse and their backward) cover L <= 32
     res = {"L": L, "beta": beta, "layers": n_layers, "K": K, "hidden": hidden, "batch": batch,
            "training_layers": "fused kernels" if fused else "torch/cuDNN"}
     flow = Flow2D(L, beta, n_layers, K, hidden).cuda()
@@ -512,7 +524,7 @@ def run_experiment(L: int = 16, beta: float = 2.0, n_layers: int = 8, K: int = 6
     for ep in range(warm_epochs):
         idx = torch.randperm(data.shape[0], device="cuda")
         for i in range(0, data.shape[0] - batch + 1, batch):
-            fkl.append(flow.forward_kl_step(opt, data[idx[i:i + batch]]))
+            fkl.append(flow.forward_kl_step(opt, data[idx[i:i + batch]], fused=fused))
     torch.cuda.synchronize()
     res["warm_s"] = time.perf_counter() - t0
     res["forward_kl_first_last"] = [fkl[0], fkl[-1]] if fkl else None

@@ -172,6 +172,11 @@ class Lattice:
     def set_block(self, threads: int) -> None:
         check(lib.u1_lattice_set_block(self._h, int(threads)), "u1_lattice_set_block")
 
+    def set_wave_wait(self, spin_limit: int = 0, stall_tile: int = -1) -> None:
+        """Waits of the persistent sweep (variant 4): polls per neighbour wait
+        (0: the default) and a tile that never publishes (-1: none)."""
+        check(lib.u1_lattice_set_wave_wait(self._h, int(spin_limit), int(stall_tile)), "u1_lattice_set_wave_wait")
+
     def set_metropolis(self, delta: float = 0.0, nhits: int = 1) -> None:
         """Metropolis proposal: nhits hits per link and pass, each proposing
         theta' = theta + delta (2u - 1), or theta' = 2 pi u for delta = 0
@@ -431,6 +436,32 @@ class Batch:
 
     def set_stream(self, stream_ptr: int | None) -> None:
         check(lib.u1_batch_set_stream(self._h, C.c_void_p(stream_ptr or 0)), "u1_batch_set_stream")
+
+    VARIANTS = {5: "quad", 1: "pair32", 3: "single"}
+
+    def tune(self) -> int:
+        """Tune (or apply the cached tuning of) the group size and each
+        group's kernel and block size; returns the group size in MiB."""
+        mb = C.c_int()
+        check(lib.u1_batch_tune(self._h, C.byref(mb)), "u1_batch_tune")
+        return int(mb.value)
+
+    def configure(self, group_mb: int = 0, choices: Sequence = ()) -> None:
+        """Explicit layout: group size in MiB (0: keep) and (variant, threads)
+        per group for the first len(choices) groups."""
+        n = len(choices)
+        v = (C.c_int * max(1, n))(*[int(c[0]) for c in choices])
+        t = (C.c_int * max(1, n))(*[int(c[1]) for c in choices])
+        check(lib.u1_batch_configure(self._h, int(group_mb), n, v, t), "u1_batch_configure")
+
+    def layout(self) -> list[tuple[int, int, int, int]]:
+        """Per group: (first chain, end chain, variant, threads per block)."""
+        out = []
+        for k in range(self.groups):
+            a = (C.c_int * 4)()
+            check(lib.u1_batch_group_info(self._h, k, a), "u1_batch_group_info")
+            out.append(tuple(int(x) for x in a))
+        return out
 
     def hot_start(self) -> None:
         check(lib.u1_batch_hot_start(self._h), "u1_batch_hot_start")

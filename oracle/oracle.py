@@ -26,7 +26,8 @@ _dp = C.POINTER(C.c_double)
 
 
 def build(ref: bool = True) -> None:
-    """Build the oracle (and, when the reference sources exist, oracle/_ref)."""
+    """Build the oracle (and, when the reference sources exist at
+    $U1_REFERENCE_DIR, oracle/_ref)."""
     targets = ["oracle"] + (["ref"] if ref else [])
     subprocess.run(["make", "-s", "-C", str(HERE), "-j8"] + targets, check=True)
 

@@ -1,7 +1,8 @@
 """Generate the golden fixtures in tests/golden/ from the REFERENCE's own code.
 
-Run here (where the reference sources exist and oracle/_ref/libu1ref.so is
-built by `make -C oracle`):   python tests/golden/make_golden.py
+Run where the reference sources exist and oracle/_ref/libu1ref.so is built
+(`make -C oracle ref REF=<reference source tree>`):
+    python tests/golden/make_golden.py
 
 For each geometry the fixture holds a seeded random lattice and what the
 reference's own FP64 CPU functions (reference src/update.cu:51-98,

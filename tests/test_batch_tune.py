@@ -255,3 +255,71 @@ def test_wave_measured_sweep(ctx, geom):
         assert abs(complex(got[0], got[1]) - want["plaq_ss"]) < 2e-6
         assert abs(complex(got[2], got[3]) - want["plaq_st"]) < 2e-6
         assert abs(complex(got[4], got[5]) - want["poly"]) < 2e-6
+
+
+# a batch whose groups differ: 16^4 chains (2 MiB each, four sites per
+# thread allowed), 12^3 x 8 chains (N0/2 = 6: two sites per thread at most),
+# 6^4 chains (N0/2 odd: one site per thread only); 9.4 MiB of links
+TUNE_SET = ([(4, (16, 16, 16, 16), 0.9 + 0.02 * k) for k in range(4)] + [(4, (12, 12, 12, 8), 1.0, 1.3)] * 3 +
+            [(4, (6, 6, 6, 6), 1.1)] * 3)
+
+
+def _batch_run(ctx, layout=None, tune=False):
+    b = Batch(ctx, TUNE_SET, seed=77, first_chain=3)
+    if layout is not None:
+        b.configure(*layout)
+    if tune:
+        b.tune()
+    b.hot_start()
+    for m, o, meas in ((1, 4, True), (2, 1, False), (1, 4, True)):
+        b.update(m, o, measure=meas)
+    return b, np.concatenate([b.export_angles(c) for c in range(b.n)]), b.results_raw()
+
+
+def test_batch_layouts_bit_identical(ctx):
+    """Every chain-group size and per-group kernel / block size gives the
+    same links and measurements bit for bit; choices a group's chains do not
+    allow fall back to the default."""
+    base, th0, m0 = _batch_run(ctx)
+    assert [g[2] for g in base.layout()] == [3]  # one group holding 6^4 chains: one site per thread
+    layouts = [(4, ()),  # 4 MiB groups, default kernels
+               # 1 MiB: each 16^4 chain alone, two 12^3x8 chains, then 12^3x8 + 3 x 6^4
+               (1, ((5, 64), (5, 96), (1, 256), (3, 96), (1, 192), (3, 64))),
+               # 2 MiB: the last group mixes 12^3x8 and 6^4 chains, which refuse (5, 128)
+               (2, ((5, 128), (1, 64), (3, 256), (5, 64), (5, 128))),
+               (64, ((3, 128),))]
+    for layout in layouts:
+        b, th, m = _batch_run(ctx, layout)
+        lay = b.layout()
+        if layout[0] == 1:
+            assert [(g[2], g[3]) for g in lay] == list(layout[1])
+        if layout[0] == 2:
+            assert lay[-1][2:] == (3, 256)
+        assert lay[0][0] == 0 and lay[-1][1] == b.n
+        for c0, c1, v, t in lay:  # only choices the chains allow
+            assert v in (1, 3, 5) and 32 <= t <= (128 if v == 5 else 256)
+            for c in range(c0, c1):
+                h = TUNE_SET[c][1][0] // 2
+                assert (v != 5 or h % 4 == 0) and (v != 1 or h % 2 == 0)
+        assert np.array_equal(th, th0), layout
+        assert np.array_equal(m, m0, equal_nan=True), layout
+
+
+def test_batch_tune_and_cache(ctx, monkeypatch, tmp_path):
+    """u1_batch_tune picks a group size and a per-group kernel / block size,
+    keeps the Markov chains bit for bit, and caches the result in
+    $U1_RESOURCE_PATH; a second batch of the same extents applies it."""
+    monkeypatch.setenv("U1_RESOURCE_PATH", str(tmp_path))
+    _, th0, m0 = _batch_run(ctx)
+    b, th, m = _batch_run(ctx, tune=True)
+    assert np.array_equal(th, th0) and np.array_equal(m, m0, equal_nan=True)
+    lay = b.layout()
+    f = tmp_path / "u1b200_batch_tunecache.tsv"
+    assert f.exists()
+    rows = [r.split("\t") for r in f.read_text().splitlines() if r and not r.startswith("#")]
+    assert len(rows) == 1 and int(rows[0][1]) in (32, 48, 64, 80, 96)
+    assert rows[0][2] == ",".join(f"{v}:{t}" for _, _, v, t in lay)
+    b2 = Batch(ctx, TUNE_SET, seed=5)
+    assert b2.tune() == int(rows[0][1])
+    assert b2.layout() == lay
+    assert len([r for r in f.read_text().splitlines() if r]) == 1  # applied from the cache, not re-tuned

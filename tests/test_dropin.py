@@ -6,7 +6,7 @@ compiles and links against libu1shim.so + libu1b200.so unchanged.
   compiles on the CPU; on the GPU its results equal the Python host layer's
   bit for bit (same kernels behind both);
 * the reference's unmodified u1.cpp, compiled in place by `make -C oracle
-  dropin` into oracle/_ref/u1_dropin, runs its full hard-coded workload
+  dropin REF=<reference source tree>` into oracle/_ref/u1_dropin, runs its full hard-coded workload
   (24^3 x 12, 1000 sweeps, Poly2, Poly2 multihit, MultiLevel) on the GPU and
   writes the reference's output files.
 """
@@ -113,7 +113,7 @@ def test_timing_driver_reference_vs_dropin(tmp_path):
     ref_exe = ROOT / "oracle" / "_ref" / "timing_reference"
     our_exe = ROOT / "oracle" / "_ref" / "timing_dropin"
     if not (ref_exe.exists() and our_exe.exists()):
-        pytest.skip("timing drivers not built (make -C oracle timing)")
+        pytest.skip("timing drivers not built (make -C oracle timing REF=<reference source tree>)")
     out = {}
     for name, exe in (("reference", ref_exe), ("dropin", our_exe)):
         r = subprocess.run([str(exe)], cwd=tmp_path, capture_output=True, text=True, timeout=600)
