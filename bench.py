@@ -519,7 +519,7 @@ def run_ours(args) -> None:
                             "per_chain_plaq_ss_st": per_chain},
         }
         if world == 1 and args.hbm_check and args.delta == 0.0 and args.nhits == 1:
-            hb = [hbm_resident_line(ctx, L, max(3, min(args.steps, 10)), args.warmup, flush, peak)
+            hb = [hbm_resident_line(ctx, L, max(10, min(args.steps, 20)), max(10, args.warmup), flush, peak)
                   for L in args.hbm_check]
             line["hbm_resident"] = {"lattices": hb, "note": "the same measured step on lattices beyond the "
                                                             "126 MB L2, each tuned on its first update"}
@@ -546,6 +546,9 @@ def run_multilevel(args) -> None:
     from latticeu1_b200 import Context, Lattice, Rng
     ctx = Context(0)
     lat = Lattice(ctx, 4, (24, 24, 24, 32), 0.95)
+    if args.variant:  # otherwise the tuner chooses at the first update
+        lat.set_variant(args.variant)
+        lat.set_block(args.block)
     rng = Rng(ctx, 1234)
     lat.hot_start(rng)
     for _ in range(50):
@@ -558,20 +561,29 @@ def run_multilevel(args) -> None:
     el = time.perf_counter() - t0
     sub = args.steps * n2
     t1 = time.perf_counter()
-    nsl = 0
+    sl = []
     while time.perf_counter() - t1 < el:
         lat.update(rng, METROP, OVRN)
-        c_sl = lat.poly_corr(True)
-        nsl += 1
+        sl.append(lat.poly_corr(True).real)
+    import numpy as np
+    sl = np.asarray(sl)
+    nb = 20 if len(sl) >= 40 else max(2, len(sl) // 2)
+    bins = sl[: len(sl) // nb * nb].reshape(nb, -1, sl.shape[1]).mean(axis=1)
+    loo = (bins.sum(axis=0) - bins) / (nb - 1)
+    sl_err = np.sqrt((nb - 1) / nb * ((loo - loo.mean(axis=0)) ** 2).sum(axis=0))
     line = {"metric": "multilevel level-2 sub-updates/s (24^3x32, beta=0.95)", "value": sub / el,
             "unit": "sub-updates/s", "n_gpus": 1, "steps": args.steps, "warmup": 1,
             "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "dtype": "f32+f64 accum",
             "data": "synthetic", "config": {"workload": "MultiLevel(n4=steps, k4=1, n2, k2=1, metrop=1, ovrn=4)",
                                            "lattice": "24^3x32", "beta": 0.95, "n2": n2},
             "full_config_seconds_n4_100_n2_200": el / sub * 100 * 200,
-            "C_r_multilevel": [[float(c.real), float(c.imag)] for c in c_ml[:6]],
-            "single_level_equal_time": {"configs": nsl, "C_r_last": [[float(c.real), float(c.imag)]
-                                                                     for c in c_sl[:6]]}}
+            "update_variant": Lattice.VARIANTS.get(lat.variant, str(lat.variant)), "update_block": lat.block,
+            "C_r_multilevel": [float(c.real) for c in c_ml],
+            "single_level_equal_time": {
+                "measurements": len(sl), "C_r_mean": [float(v) for v in sl.mean(axis=0)],
+                "C_r_err": [float(v) for v in sl_err],
+                "note": "Poly2(multihit) after every sweep for the multilevel call's wall time, 20-bin "
+                        "jackknife; multilevel errors over configurations: tests/multilevel_compare.py"}}
     print(json.dumps(line), flush=True)
 
 

@@ -256,7 +256,10 @@ int u1_poly_corr(u1_lattice *lat, int multihit, double *out, int out_len);
 /* Replaces MultiLevel (reference src/multilevel.cu:639-732).  Works on an
  * internal copy of the lattice (the caller's links are unchanged) and
  * advances the rng.  Requires dims == 4 and Nt % 4 == 0 (else U1_ERR_INVALID;
- * the reference exits).  out as for u1_poly_corr. */
+ * the reference exits).  out as for u1_poly_corr.  The first call allocates
+ * the work buffers (working copy, slab products and the two tensors: about
+ * 210 MB at 24^3 x 32) and they stay with the lattice until it is destroyed,
+ * as do the graphs of the last (n2-independent) sub-update shape and rng. */
 int u1_multilevel(u1_lattice *lat, u1_rng *rng, int n4, int k4, int n2, int k2,
                   int metrop, int ovrn, double *out, int out_len);
 

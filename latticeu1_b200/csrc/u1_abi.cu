@@ -52,6 +52,46 @@ static std::mutex g_alloc_mu;
 static DevAllocator g_alloc;
 static std::atomic<long long> g_live_allocs{0};
 
+cudaError_t time_graph_min(cudaGraphExec_t ex, cudaStream_t s, int warm, int reps, double *us) {
+  cudaError_t e = cudaSuccess;
+  for (int k = 0; k < warm && e == cudaSuccess; ++k) e = cudaGraphLaunch(ex, s);
+  std::vector<cudaEvent_t> ev(2 * (size_t)reps, nullptr);
+  for (size_t k = 0; k < ev.size() && e == cudaSuccess; ++k) e = cudaEventCreate(&ev[k]);
+  for (int r = 0; r < reps && e == cudaSuccess; ++r) {
+    e = cudaEventRecord(ev[2 * r], s);
+    if (e == cudaSuccess) e = cudaGraphLaunch(ex, s);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[2 * r + 1], s);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  double best = -1.0;
+  for (int r = 0; r < reps && e == cudaSuccess; ++r) {
+    float ms = 0.f;
+    e = cudaEventElapsedTime(&ms, ev[2 * r], ev[2 * r + 1]);
+    if (e == cudaSuccess && (best < 0.0 || ms < best)) best = ms;
+  }
+  for (cudaEvent_t x : ev)
+    if (x) cudaEventDestroy(x);
+  *us = 1e3 * best;
+  return e;
+}
+
+cudaError_t warm_clocks(cudaGraphExec_t ex, cudaStream_t s, double ms) {
+  double us = 0.0;
+  cudaError_t e = time_graph_min(ex, s, 0, 1, &us);
+  const int n = us > 0.0 ? (int)std::min(2000.0, 1e3 * ms / us) : 0;
+  for (int k = 0; k < n && e == cudaSuccess; ++k) e = cudaGraphLaunch(ex, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return e;
+}
+
+bool tune_verbose() {
+  static const bool v = [] {
+    const char *e = std::getenv("U1_TUNE_VERBOSE");
+    return e && e[0] == '1';
+  }();
+  return v;
+}
+
 cudaError_t dev_alloc(void **p, size_t bytes) {
   *p = nullptr;
   DevAllocator a;
@@ -255,6 +295,10 @@ static void set_coupling(u1_lattice *lat, double beta, double aniso) {
 static void drop_graphs(u1_lattice *lat) {
   for (auto &kv : lat->graphs) cudaGraphExecDestroy(kv.second);
   lat->graphs.clear();
+  if (lat->ml_g4) cudaGraphExecDestroy(lat->ml_g4);
+  if (lat->ml_g2) cudaGraphExecDestroy(lat->ml_g2);
+  lat->ml_g4 = lat->ml_g2 = nullptr;
+  lat->ml_key = std::make_tuple(-1, -1, -1, -1, (uint64_t)0, (uint64_t)0);
 }
 
 extern "C" int u1_lattice_create(u1_ctx *ctx, const u1_geom *geom, u1_lattice **out) {
@@ -305,6 +349,10 @@ extern "C" int u1_lattice_destroy(u1_lattice *lat) {
   if (lat->stage) u1i::dev_free(lat->stage);
   if (lat->backup) u1i::dev_free(lat->backup);
   if (lat->wave_state) u1i::dev_free(lat->wave_state);
+  u1i::dev_free(lat->ml_work);
+  u1i::dev_free(lat->ml_P2);
+  u1i::dev_free(lat->ml_T2);
+  u1i::dev_free(lat->ml_T4);
   if (lat->own_stream) cudaStreamDestroy(lat->own_stream);
   delete lat;
   return U1_OK;
@@ -965,9 +1013,9 @@ static bool block_valid(int threads) { return threads >= 32 && threads <= 256 &&
 // bit-identical links, so a trial never changes the Markov chain.  Each
 // trial captures its sweep as a CUDA graph, as u1_update runs it, and times
 // replays of it from a backed-up state (links and pass counter restored
-// afterwards, as the reference's preTune/postTune do), in two rounds (the
-// second in reverse order, each candidate keeping its faster time); the
-// winner is cached per (device, geometry) in
+// afterwards, as the reference's preTune/postTune do), after a clock
+// warm-up, in two rounds (the second in reverse order), each candidate scored
+// by its shortest single replay; the winner is cached per (device, geometry) in
 // memory and, when U1_RESOURCE_PATH names a directory, in
 // $U1_RESOURCE_PATH/u1b200_tunecache.tsv (the reference's tunecache.csv
 // location rule, src/tune.cpp:160-232).  U1_TUNE=0 disables tuning.
@@ -1055,46 +1103,44 @@ static int tune_update(u1_lattice *lat, u1_rng *rng, bool use_cache) {
     if (!lat->backup) U1_CUDA_TRY(u1i::dev_alloc(&lat->backup, n * sizeof(float2)));
     U1_CUDA_TRY(cudaMemcpyAsync(lat->backup, lat->links, n * sizeof(float2), cudaMemcpyDeviceToDevice, lat->stream));
     const unsigned long long pass0 = rng->pass;
-    cudaEvent_t e0, e1;
-    U1_CUDA_TRY(cudaEventCreate(&e0));
-    U1_CUDA_TRY(cudaEventCreate(&e1));
     int rc = U1_OK;
     // Two rounds over the candidates, the second in reverse order, keeping
     // each candidate's faster time: a large lattice drives the GPU into its
     // power cap during tuning, and one round would favour whichever
     // candidates ran first (measured at 64^4: the two-site kernel at 96
     // threads picked over the four-site one, 4.8 against 4.0 ms a step).
+    // Each trial scores its candidate by the shortest of 5 single replays;
+    // the first trial is preceded by about 50 ms of replays to bring the
+    // clocks up.
     std::vector<double> cand_us(cand.size(), -1.0);
     std::vector<size_t> order;
     for (size_t k = 0; k < cand.size(); ++k) order.push_back(k);
     for (size_t k = cand.size(); k-- > 0;) order.push_back(k);
+    bool warmed = false;
     for (size_t ci : order) {
       const auto &vt = cand[ci];
       lat->variant = vt.first;
       lat->block = vt.second;
       cudaGraphExec_t ex = nullptr;
       rc = capture_graph(lat, [&]() { return issue_sweep(lat, lat->links, rng, 1, 4, 0); }, &ex);
-      auto replay = [&]() -> int {
-        const cudaError_t er = cudaGraphLaunch(ex, lat->stream);
-        return er == cudaSuccess ? U1_OK : u1i::cuda_fail(er, "cudaGraphLaunch");
-      };
-      for (int k = 0; k < 2 && !rc; ++k) rc = replay();  // warm-up
-      if (!rc) {
-        const cudaError_t er = cudaEventRecord(e0, lat->stream);
-        if (er != cudaSuccess) rc = u1i::cuda_fail(er, "cudaEventRecord");
+      double us = 0.0;
+      if (!rc && !warmed) {
+        const cudaError_t er = u1i::warm_clocks(ex, lat->stream, 50.0);
+        if (er != cudaSuccess) rc = u1i::cuda_fail(er, "tuning warm-up");
+        warmed = true;
       }
-      for (int k = 0; k < 5 && !rc; ++k) rc = replay();
-      cudaEventRecord(e1, lat->stream);
-      cudaError_t e = cudaEventSynchronize(e1);
-      if (!rc && e != cudaSuccess) rc = u1i::cuda_fail(e, "tuning sweep");
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, e0, e1);
+      if (!rc) {
+        const cudaError_t er = u1i::time_graph_min(ex, lat->stream, 2, 5, &us);
+        if (er != cudaSuccess) rc = u1i::cuda_fail(er, "tuning sweep");
+      }
       cudaMemcpyAsync(lat->links, lat->backup, n * sizeof(float2), cudaMemcpyDeviceToDevice, lat->stream);
       cudaMemcpyAsync(rng->pass_dev, &pass0, sizeof(pass0), cudaMemcpyHostToDevice, lat->stream);
       cudaStreamSynchronize(lat->stream);
       if (ex) cudaGraphExecDestroy(ex);
       if (rc) break;
-      const double us = 1e3 * ms / 5.0;
+      if (u1i::tune_verbose())
+        std::fprintf(stderr, "u1_tune %s: variant %d, %d threads: %.1f us per sweep\n", key.c_str(), vt.first,
+                     vt.second, us);
       if (cand_us[ci] < 0.0 || us < cand_us[ci]) cand_us[ci] = us;
     }
     for (size_t k = 0; k < cand.size() && !rc; ++k)
@@ -1102,8 +1148,6 @@ static int tune_update(u1_lattice *lat, u1_rng *rng, bool use_cache) {
         best_us = cand_us[k];
         best = cand[k];
       }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     if (rc) {
       lat->variant = U1V_AUTO;
       lat->block = 256;
@@ -1414,25 +1458,33 @@ extern "C" int u1_multilevel(u1_lattice *lat, u1_rng *rng, int n4, int k4, int n
   U1_CUDA_TRY(cudaSetDevice(lat->ctx->device));
   const size_t size = (size_t)g.Vs * R * g.tdir;
   const int nl2 = g.N[g.tdir] / 2, nl4 = g.N[g.tdir] / 4;
-  float2 *work = nullptr;
-  double2 *P2 = nullptr, *T2 = nullptr, *T4 = nullptr;
   int rc = U1_OK;
-  auto cleanup = [&]() {
-    cudaStreamSynchronize(lat->stream);
-    if (work) u1i::dev_free(work);
-    if (P2) u1i::dev_free(P2);
-    if (T2) u1i::dev_free(T2);
-    if (T4) u1i::dev_free(T4);
-  };
-  cudaError_t e = u1i::dev_alloc(&work, (size_t)g.V * g.dims * sizeof(float2));
-  if (e == cudaSuccess) e = u1i::dev_alloc(&P2, (size_t)g.Vs * nl2 * sizeof(double2));
-  if (e == cudaSuccess) e = u1i::dev_alloc(&T2, size * nl2 * sizeof(double2));
-  if (e == cudaSuccess) e = u1i::dev_alloc(&T4, size * nl4 * sizeof(double2));
-  if (e != cudaSuccess) {
-    cleanup();
-    u1i::set_error(std::string("u1_multilevel: allocation failed: ") + cudaGetErrorString(e));
-    return U1_ERR_NOMEM;
+  auto cleanup = [&]() { cudaStreamSynchronize(lat->stream); };
+  // The work buffers (the links' working copy, slab products, T2, T4: about
+  // 210 MB at 24^3 x 32) are allocated by the first call and kept with the
+  // lattice, so later calls neither allocate nor synchronise the device.
+  if (!lat->ml_work) {
+    float2 *work = nullptr;
+    double2 *P2 = nullptr, *T2 = nullptr, *T4 = nullptr;
+    cudaError_t e = u1i::dev_alloc(&work, (size_t)g.V * g.dims * sizeof(float2));
+    if (e == cudaSuccess) e = u1i::dev_alloc(&P2, (size_t)g.Vs * nl2 * sizeof(double2));
+    if (e == cudaSuccess) e = u1i::dev_alloc(&T2, size * nl2 * sizeof(double2));
+    if (e == cudaSuccess) e = u1i::dev_alloc(&T4, size * nl4 * sizeof(double2));
+    if (e != cudaSuccess) {
+      u1i::dev_free(work);
+      u1i::dev_free(P2);
+      u1i::dev_free(T2);
+      u1i::dev_free(T4);
+      u1i::set_error(std::string("u1_multilevel: allocation failed: ") + cudaGetErrorString(e));
+      return U1_ERR_NOMEM;
+    }
+    lat->ml_work = work;
+    lat->ml_P2 = P2;
+    lat->ml_T2 = T2;
+    lat->ml_T4 = T4;
   }
+  float2 *const work = lat->ml_work;
+  double2 *const P2 = lat->ml_P2, *const T2 = lat->ml_T2, *const T4 = lat->ml_T4;
   const int nb_s = u1i::blocks_for(g.Vs, kRedThreads);
   const MlDims md{g.N[0], g.N[1], g.N[2], g.Vs, R, nl2, nl4};
   rc = u1i::ensure_scratch(lat, (size_t)nb_s * 2 * R, (size_t)2 * R);
@@ -1465,19 +1517,26 @@ extern "C" int u1_multilevel(u1_lattice *lat, u1_rng *rng, int n4, int k4, int n
   };
   const unsigned long long per_sweep = 2ull * g.dims * (metrop + ovrn) + (ovrn == 0 ? 1 : 0);
   const bool graphed = lat->use_graphs && !rng->replay_dev;
-  cudaGraphExec_t g4 = nullptr, g2 = nullptr;
+  // the graphs of the last (k4, k2, metrop, ovrn, rng) are kept with the lattice
+  const auto key = std::make_tuple(k4, k2, metrop, ovrn, rng->id, rng->seed ^ ((uint64_t)rng->chain << 48));
   auto body = [&]() -> int {
     U1_CUDA_TRY(cudaMemcpyAsync(work, lat->links, (size_t)g.V * g.dims * sizeof(float2),
                                 cudaMemcpyDeviceToDevice, lat->stream));
     U1_CUDA_TRY(cudaMemsetAsync(T4, 0, size * nl4 * sizeof(double2), lat->stream));
-    if (graphed) {
+    if (graphed && (!lat->ml_g2 || lat->ml_key != key)) {
+      if (lat->ml_g4) cudaGraphExecDestroy(lat->ml_g4);
+      if (lat->ml_g2) cudaGraphExecDestroy(lat->ml_g2);
+      lat->ml_g4 = lat->ml_g2 = nullptr;
+      lat->ml_key = std::make_tuple(-1, -1, -1, -1, (uint64_t)0, (uint64_t)0);
       if (k4 > 0) {
-        int r = capture_graph(lat, level4, &g4);
+        int r = capture_graph(lat, level4, &lat->ml_g4);
         if (r) return r;
       }
-      int r = capture_graph(lat, level2, &g2);
+      int r = capture_graph(lat, level2, &lat->ml_g2);
       if (r) return r;
+      lat->ml_key = key;
     }
+    cudaGraphExec_t g4 = lat->ml_g4, g2 = lat->ml_g2;
     for (int i = 0; i < n4; ++i) {
       if (graphed) {
         if (k4 > 0) {
@@ -1522,8 +1581,6 @@ extern "C" int u1_multilevel(u1_lattice *lat, u1_rng *rng, int n4, int k4, int n
   }
   rc = body();
   cleanup();
-  if (g4) cudaGraphExecDestroy(g4);
-  if (g2) cudaGraphExecDestroy(g2);
   if (rc) return rc;
   memcpy(out, lat->h_out, (size_t)2 * R * sizeof(double));
   return U1_OK;

@@ -16,6 +16,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <array>
+#include <cstdio>
 #include <cstring>
 #include <fstream>
 #include <map>
@@ -715,8 +716,9 @@ extern "C" int u1_batch_get_pass(const u1_batch *b, uint64_t *pass) {
 // update kernel (four, two or one site per thread) and threads per block.
 // Every choice gives the same links bit for bit, so trials never change the
 // Markov chains; each trial captures its sweep (1 Metropolis + 4 OR) as a
-// CUDA graph, as u1_batch_update runs it, and times 5 replays after 2
-// warm-up replays from a backed-up state (links and pass counter restored).
+// CUDA graph, as u1_batch_update runs it, and scores it by the shortest of 5
+// single replays after 2 warm-up replays (the first trial after about 50 ms
+// of clock warm-up), from a backed-up state (links and pass counter restored).
 // Stage 1 times whole sweeps for each group size with the default kernels;
 // stage 2 times each group's own sweep for each (kernel, threads) it
 // allows; the per-group choice is kept only if the whole sweep is faster.
@@ -795,9 +797,10 @@ std::vector<std::pair<int, int>> current_choice(const u1_batch *b) {
 }  // namespace
 
 // Microseconds per sweep (1 Metropolis + 4 OR) of groups [g0, g1) in the
-// current layout: a captured graph, 2 warm-up and 5 timed replays; the
-// links and the pass counter are restored from the backup afterwards.
-static int batch_time_sweep(u1_batch *b, int g0, int g1, double *us) {
+// current layout: a captured graph, 2 warm-up replays (after warm_ms of
+// clock warm-up), the shortest of 5 single timed replays; the links and the
+// pass counter are restored from the backup afterwards.
+static int batch_time_sweep(u1_batch *b, int g0, int g1, double *us, double warm_ms = 0.0) {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t ex = nullptr;
   U1_CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
@@ -813,27 +816,19 @@ static int batch_time_sweep(u1_batch *b, int g0, int g1, double *us) {
   e = cudaGraphInstantiate(&ex, graph, 0);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) return cuda_fail(e, "u1_batch_tune: instantiate");
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  e = cudaEventCreate(&e0);
-  if (e == cudaSuccess) e = cudaEventCreate(&e1);
-  for (int k = 0; k < 2 && e == cudaSuccess; ++k) e = cudaGraphLaunch(ex, b->stream);
-  if (e == cudaSuccess) e = cudaEventRecord(e0, b->stream);
-  for (int k = 0; k < 5 && e == cudaSuccess; ++k) e = cudaGraphLaunch(ex, b->stream);
-  if (e == cudaSuccess) e = cudaEventRecord(e1, b->stream);
-  if (e == cudaSuccess) e = cudaEventSynchronize(e1);
-  float ms = 0.f;
-  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+  if (warm_ms > 0.0) e = u1i::warm_clocks(ex, b->stream, warm_ms);
+  if (e == cudaSuccess) e = u1i::time_graph_min(ex, b->stream, 2, 5, us);
   const unsigned long long pass0 = b->pass;
   cudaError_t r1 = cudaMemcpyAsync(b->links, b->backup, b->total_links * sizeof(float2), cudaMemcpyDeviceToDevice,
                                    b->stream);
   cudaError_t r2 = cudaMemcpyAsync(b->pass_dev, &pass0, sizeof(pass0), cudaMemcpyHostToDevice, b->stream);
   cudaError_t r3 = cudaStreamSynchronize(b->stream);
-  if (e0) cudaEventDestroy(e0);
-  if (e1) cudaEventDestroy(e1);
   cudaGraphExecDestroy(ex);
   if (e == cudaSuccess) e = r1 != cudaSuccess ? r1 : r2 != cudaSuccess ? r2 : r3;
   if (e != cudaSuccess) return cuda_fail(e, "u1_batch_tune: trial");
-  *us = 1e3 * ms / 5.0;
+  if (u1i::tune_verbose())
+    std::fprintf(stderr, "u1_batch_tune: groups %d..%d of %d (%zu MiB groups): %.1f us per sweep\n", g0, g1 - 1,
+                 (int)b->groups.size(), b->group_bytes >> 20, *us);
   return U1_OK;
 }
 
@@ -862,10 +857,12 @@ static int batch_tune(u1_batch *b) {
   // stage 1: group size, default kernels
   const std::vector<int> sizes = {32, 48, 64, 80, 96};
   std::vector<double> size_us(sizes.size(), -1.0);
+  bool warmed = false;
   for (size_t k : two_rounds(sizes.size())) {
     int rc = batch_configure(b, (size_t)sizes[k] << 20, {});
     double us = 0.0;
-    if (!rc) rc = batch_time_sweep(b, 0, (int)b->groups.size(), &us);
+    if (!rc) rc = batch_time_sweep(b, 0, (int)b->groups.size(), &us, warmed ? 0.0 : 50.0);
+    warmed = true;
     if (rc) return rc;
     if (size_us[k] < 0.0 || us < size_us[k]) size_us[k] = us;
   }

@@ -22,6 +22,10 @@
 namespace {
 
 constexpr int kMaxK = 8;
+// Threads per block of the fused layer kernels (one configuration per block):
+// their shared memory (up to about 200 KB at L = 32) allows one block per SM,
+// so the block itself must bring enough warps to hide shared-memory latency.
+constexpr int kFlowThreads = 512;
 constexpr float kTwoPi = 6.28318530717958647692f;
 
 int flfail(int code, const std::string &msg) {
@@ -265,7 +269,7 @@ __device__ __forceinline__ float layer_transform(float P, const float *__restric
 // INV: the inverse layer (the context plaquettes hold no updated link, so the
 // same parameters come out; the transform is inverted), as Coupling.inverse.
 template <bool INV>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kFlowThreads)
     k_flow_layer_forward(const float *__restrict__ th_in, float *__restrict__ th_out, float *__restrict__ logdet,
                          int L, int mu, int off, int K, int H, const float *__restrict__ W1,
                          const float *__restrict__ B1, const float *__restrict__ W2, const float *__restrict__ B2,
@@ -401,16 +405,15 @@ __global__ void __launch_bounds__(256)
 // used, passed straight to the FP32 master weights) go to per-block partials
 // wpart[b][:] = (gW1[c][ci][k], gB1[c], gW2[o][ci][k], gB2[o]), summed over
 // blocks in a fixed order by k_flow_wgrad_reduce.
-__device__ __forceinline__ int nbr_at(int p, int k, int L) {  // pixel at offset k (ky-major) of pixel p
-  int yy = p / L + k / 3 - 1, xx = p % L + k % 3 - 1;
-  yy = yy < 0 ? yy + L : (yy >= L ? yy - L : yy);
-  xx = xx < 0 ? xx + L : (xx >= L ? xx - L : xx);
-  return yy * L + xx;
-}
 __device__ __forceinline__ float lrelu(float v, float slope) { return v > 0.f ? v : slope * v; }
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
 
 template <bool INV>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kFlowThreads)
     k_flow_layer_backward(const float *__restrict__ th_in, const float *__restrict__ gth_out,
                           const float *__restrict__ gld, float *__restrict__ gth_in, float *__restrict__ wpart, int L,
                           int mu, int off, int K, int H, int Cc, const float *__restrict__ W1,
@@ -427,14 +430,14 @@ __global__ void __launch_bounds__(256)
   float *w2t = b1 + H;             // 9 H CP [ci*9 + k][o]
   float *b2 = w2t + 9 * H * CP;    // CP
   float *prm = b2 + CP;            // nact CP
-  float *gprm = prm + nact * CP;   // nact CP
-  float *gctx = gprm + nact * CP;  // 2 LL
+  float *gprmT = prm + nact * CP;  // CP nact  dL/dparams, parameter-major ([o][a]: conflict-free across a)
+  float *gctx = gprmT + nact * CP; // 2 LL
   float *gP = gctx + 2 * LL;       // LL
   float *hc = gP + LL;             // Cc LL  pre-activations of the chunk's channels
   float *ghc = hc + Cc * LL;       // Cc LL  dL/dpre of the chunk's channels
-  float *gw1h = ghc + Cc * LL;     // 36 Cc  gW1 of the chunk, two pixel halves
-  int *amap = reinterpret_cast<int *>(gw1h + 36 * Cc);  // LL: active index of a plaquette, or -1
-  int *apos = amap + LL;                                // nact: pixel of active plaquette a
+  int *amap = reinterpret_cast<int *>(ghc + Cc * LL);  // LL: active index of a plaquette, or -1
+  int *apos = amap + LL;                                     // nact: pixel of active plaquette a
+  int *nbt = apos + nact;                                    // 9 LL: nbt[k * LL + p] = pixel at offset k of p
   const int nt = blockDim.x, tid = threadIdx.x, b = blockIdx.x;
   const float *src = th_in + (size_t)b * 2 * LL;
   const float *go = gth_out + (size_t)b * 2 * LL;
@@ -452,6 +455,10 @@ __global__ void __launch_bounds__(256)
   for (int p = tid; p < LL; p += nt) {
     amap[p] = -1;
     gP[p] = 0.f;
+    int o9[9];
+    nbr9(p / L, p % L, L, o9);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) nbt[k * LL + p] = o9[k];
   }
   __syncthreads();
   for (int a = tid; a < nact; a += nt) {
@@ -481,13 +488,12 @@ __global__ void __launch_bounds__(256)
   // conv1 pre-activations of channels c0 .. c0+Cc-1 into hc
   auto conv1_chunk = [&](int c0) {
     for (int p = tid; p < LL; p += nt) {
-      int o9[9];
-      nbr9(p / L, p % L, L, o9);
       float in[18];
 #pragma unroll
       for (int k = 0; k < 9; ++k) {
-        in[k] = ctx[o9[k]];
-        in[9 + k] = ctx[LL + o9[k]];
+        const int q = nbt[k * LL + p];
+        in[k] = ctx[q];
+        in[9 + k] = ctx[LL + q];
       }
       for (int c4 = 0; c4 < Cc; c4 += 4) {
         const int c = c0 + c4;
@@ -507,15 +513,14 @@ __global__ void __launch_bounds__(256)
     __syncthreads();
     for (int q = tid; q < nact * ng; q += nt) {
       const int a = q / ng, og = q - a * ng;
-      int o9[9];
       const int pa = apos[a];
-      nbr9(pa / L, pa % L, L, o9);
       float *dst = prm + a * CP + og * 4;
       float4 acc = make_float4(dst[0], dst[1], dst[2], dst[3]);
       for (int cl = 0; cl < Cc; ++cl) {
         const float *pc = hc + cl * LL;
 #pragma unroll
-        for (int k = 0; k < 9; ++k) fma4(acc, w2v[(((c0 + cl) * 9 + k) * CP >> 2) + og], lrelu(pc[o9[k]], slope));
+        for (int k = 0; k < 9; ++k)
+          fma4(acc, w2v[(((c0 + cl) * 9 + k) * CP >> 2) + og], lrelu(pc[nbt[k * LL + pa]], slope));
       }
       dst[0] = acc.x;
       dst[1] = acc.y;
@@ -530,7 +535,7 @@ __global__ void __launch_bounds__(256)
     const int pa = apos[a];
     const int x1 = pa / L, x0 = pa - x1 * L;
     const float *pp = prm + a * CP;
-    float *gpo = gprm + a * CP;
+    float gpo[2 * kMaxK + 1];
     const int link = mu == 0 ? pa : LL + x1 * L + (x0 + 1 == L ? 0 : x0 + 1);
     const float gout = go[link];
     Mix m;
@@ -570,15 +575,14 @@ __global__ void __launch_bounds__(256)
     }
     for (int k = 0; k < K; ++k)
       if (fabsf(pp[k]) > 8.f) gpo[k] = 0.f;
-    for (int o = C2; o < CP; ++o) gpo[o] = 0.f;
+    for (int o = 0; o < C2; ++o) gprmT[o * nact + a] = gpo[o];
   }
   __syncthreads();
   float *wp = wpart + (size_t)b * (H * 18 + H + C2 * H * 9 + C2);
   float *gW1 = wp, *gB1 = wp + H * 18, *gW2 = gB1 + H, *gB2 = gW2 + C2 * H * 9;
-  const float4 *gpv = reinterpret_cast<const float4 *>(gprm);
   for (int o = tid; o < C2; o += nt) {
     float acc = 0.f;
-    for (int a = 0; a < nact; ++a) acc += gprm[a * CP + o];
+    for (int a = 0; a < nact; ++a) acc += gprmT[o * nact + a];
     gB2[o] = acc;
   }
   // ---- adjoint, chunk by chunk over the hidden channels
@@ -588,69 +592,87 @@ __global__ void __launch_bounds__(256)
     // dL/dpre[c][p] = LeakyReLU'(pre) * sum_k sum_o W2[o][c][k] gprm[a][o] over active a whose offset-k neighbour is p
     for (int q = tid; q < Cc * LL; q += nt) {
       const int cl = q / LL, p = q - cl * LL;
-      int o9[9];
-      nbr9(p / L, p % L, L, o9);
       float acc = 0.f;
 #pragma unroll
       for (int k = 0; k < 9; ++k) {
-        const int a = amap[o9[8 - k]];
+        const int a = amap[nbt[(8 - k) * LL + p]];
         if (a >= 0) {
-          const float4 *wv = w2v + (((c0 + cl) * 9 + k) * CP >> 2);
-          for (int og = 0; og < ng; ++og) {
-            const float4 w = wv[og], gg = gpv[a * ng + og];
-            acc = fmaf(w.x, gg.x, fmaf(w.y, gg.y, fmaf(w.z, gg.z, fmaf(w.w, gg.w, acc))));
-          }
+          const float *wr = w2t + ((c0 + cl) * 9 + k) * CP;
+          for (int o = 0; o < C2; ++o) acc = fmaf(wr[o], gprmT[o * nact + a], acc);
         }
       }
       ghc[q] = hc[q] > 0.f ? acc : slope * acc;
     }
-    // gW2[o][c][k] = sum_a gprm[a][o] h[c][nbr(a, k)]: one (c, k, group of four outputs) per work item
-    for (int e = tid; e < Cc * 9 * ng; e += nt) {
-      const int cl = e / (9 * ng), rem = e - cl * 9 * ng, k = rem / ng, og = rem - k * ng;
+    __syncthreads();
+    // Weight gradients of the chunk as warp reductions: lanes split the sum
+    // (active plaquettes or pixels), each lane keeps several independent
+    // accumulators, and a fixed xor-shuffle tree adds the lanes (the same
+    // order every run).
+    const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
+    // gW2[o][c][k] = sum_a gprm[a][o] h[c][nbr(a, k)]: unit = (c, k, eight outputs)
+    for (int u = warp; u < Cc * 9 * (CP / 8 + (CP % 8 ? 1 : 0)); u += nwarps) {
+      const int n8 = CP / 8 + (CP % 8 ? 1 : 0);
+      const int ck = u / n8, o0 = 8 * (u - ck * n8), cl = ck / 9, k = ck - cl * 9;
       const float *pc = hc + cl * LL;
-      float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-      for (int a = 0; a < nact; ++a) fma4(acc, gpv[a * ng + og], lrelu(pc[nbr_at(apos[a], k, L)], slope));
-      const float av[4] = {acc.x, acc.y, acc.z, acc.w};
+      const int *nk = nbt + k * LL;
+      float acc[8];
 #pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        const int o = 4 * og + t;
-        if (o < C2) gW2[(size_t)o * H * 9 + (c0 + cl) * 9 + k] = av[t];
+      for (int j = 0; j < 8; ++j) acc[j] = 0.f;
+      for (int a = lane; a < nact; a += 32) {
+        const float v = lrelu(pc[nk[apos[a]]], slope);
+        const float *gg = gprmT + o0 * nact + a;
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+          if (o0 + j < C2) acc[j] = fmaf(gg[j * nact], v, acc[j]);
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc[j] = warp_sum(acc[j]);
+      if (lane < 8 && o0 + lane < C2) {
+        float v = acc[0];
+#pragma unroll
+        for (int j = 1; j < 8; ++j)
+          if (lane == j) v = acc[j];
+        gW2[(size_t)(o0 + lane) * H * 9 + (c0 + cl) * 9 + k] = v;
       }
     }
-    __syncthreads();
-    // gW1[c][ci][k] = sum_p dL/dpre[c][p] ctx[ci][nbr(p, k)]: (ci*9 + k, c, half of the pixels) per work item
-    for (int e = tid; e < 36 * Cc; e += nt) {
-      const int half = e & 1, rc = e >> 1, r = rc % 18, cl = rc / 18, ci = r / 9, k = r - ci * 9;
-      const float *cx = ctx + ci * LL;
+    // gW1[c][ci][k] = sum_p dL/dpre[c][p] ctx[ci][nbr(p, k)] and gB1[c] = sum_p dL/dpre[c][p]:
+    // unit = (c, ci), nine offsets per lane
+    for (int u = warp; u < Cc * 2; u += nwarps) {
+      const int cl = u >> 1, ci = u & 1;
       const float *gc = ghc + cl * LL;
-      const int p1 = half ? LL : LL / 2;
-      float acc = 0.f;
-      for (int p = half ? LL / 2 : 0; p < p1; ++p) acc = fmaf(gc[p], cx[nbr_at(p, k, L)], acc);
-      gw1h[e] = acc;
-    }
-    for (int cl = tid; cl < Cc; cl += nt) {
-      float acc = 0.f;
-      for (int p = 0; p < LL; ++p) acc += ghc[cl * LL + p];
-      gB1[c0 + cl] = acc;
+      const float *cx = ctx + ci * LL;
+      float acc[9], accb = 0.f;
+#pragma unroll
+      for (int k = 0; k < 9; ++k) acc[k] = 0.f;
+      for (int p = lane; p < LL; p += 32) {
+        const float gv = gc[p];
+        accb += gv;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) acc[k] = fmaf(gv, cx[nbt[k * LL + p]], acc[k]);
+      }
+#pragma unroll
+      for (int k = 0; k < 9; ++k) acc[k] = warp_sum(acc[k]);
+      accb = warp_sum(accb);
+      if (lane < 9) {
+        float v = acc[0];
+#pragma unroll
+        for (int k = 1; k < 9; ++k)
+          if (lane == k) v = acc[k];
+        gW1[(c0 + cl) * 18 + ci * 9 + lane] = v;
+      }
+      if (ci == 0 && lane == 0) gB1[c0 + cl] = accb;
     }
     // gctx[ci][p] += sum_k sum_{c in chunk} W1[c][ci][k] dL/dpre[c][p - (k offset)]
     for (int q = tid; q < 2 * LL; q += nt) {
       const int ci = q / LL, p = q - ci * LL;
-      int o9[9];
-      nbr9(p / L, p % L, L, o9);
       float acc = gctx[q];
 #pragma unroll
       for (int k = 0; k < 9; ++k) {
-        const int pq = o9[8 - k];
+        const int pq = nbt[(8 - k) * LL + p];
         const float *wr = w1t + (ci * 9 + k) * H + c0;
         for (int cl = 0; cl < Cc; ++cl) acc = fmaf(wr[cl], ghc[cl * LL + pq], acc);
       }
       gctx[q] = acc;
-    }
-    __syncthreads();
-    for (int e = tid; e < 18 * Cc; e += nt) {
-      const int r = e % 18, cl = e / 18;
-      gW1[(c0 + cl) * 18 + r] = gw1h[2 * (cl * 18 + r)] + gw1h[2 * (cl * 18 + r) + 1];
     }
     __syncthreads();
   }
@@ -689,8 +711,8 @@ int flow_chunk(int H) { return H % 8 == 0 ? 8 : 4; }
 size_t flow_layer_bwd_smem(int L, int K, int H) {
   const size_t LL = (size_t)L * L, CP = (2 * K + 1 + 3) & ~3, nact = LL / 4, Cc = flow_chunk(H);
   return sizeof(float) * (2 * LL + LL + 2 * LL + 18 * H + H + 9 * H * CP + CP + 2 * nact * CP + 2 * LL + LL +
-                          2 * Cc * LL + 36 * Cc) +
-         sizeof(int) * (LL + nact);
+                          2 * Cc * LL) +
+         sizeof(int) * (LL + nact + 9 * LL);
 }
 
 size_t flow_layer_smem(int L, int K, int H) {
@@ -770,7 +792,7 @@ int flow_layer_fwd(const char *name, const float *theta_in, float *theta_out, fl
                                          (int)smem);
     if (e != cudaSuccess) return u1i::cuda_fail(e, name);
   }
-  k_flow_layer_forward<INV><<<batch, 256, smem, (cudaStream_t)stream>>>(theta_in, theta_out, logdet, L, mu, off, K,
+  k_flow_layer_forward<INV><<<batch, kFlowThreads, smem, (cudaStream_t)stream>>>(theta_in, theta_out, logdet, L, mu, off, K,
                                                                          hidden, W1, B1, W2, B2, slope);
   U1_LAUNCH_CHECK(name);
   return U1_OK;
@@ -794,7 +816,7 @@ int flow_layer_bwd(const char *name, const float *theta_in, const float *grad_th
     if (e != cudaSuccess) return u1i::cuda_fail(e, name);
   }
   cudaStream_t s = (cudaStream_t)stream;
-  k_flow_layer_backward<INV><<<batch, 256, smem, s>>>(theta_in, grad_theta_out, grad_logdet, grad_theta_in,
+  k_flow_layer_backward<INV><<<batch, kFlowThreads, smem, s>>>(theta_in, grad_theta_out, grad_logdet, grad_theta_in,
                                                        wgrad_partials, L, mu, off, K, hidden, flow_chunk(hidden), W1,
                                                        B1, W2, B2, slope);
   U1_LAUNCH_CHECK(name);

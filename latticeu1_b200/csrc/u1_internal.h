@@ -66,6 +66,13 @@ struct u1_lattice {
   // persistent sweep (U1V_WAVE): per-tile phase flags, then ticket and error word
   unsigned int *wave_state = nullptr;
   int wave_ok = -1;                // -1 unknown, 0 not usable, 1 usable
+  // multilevel (u1_multilevel): work copy of the links, level-2 slab products,
+  // T2 and T4, kept from the first call until the lattice is destroyed, and
+  // the level-4 / level-2 graphs of the last (k4, k2, metrop, ovrn, rng) used
+  float2 *ml_work = nullptr;
+  double2 *ml_P2 = nullptr, *ml_T2 = nullptr, *ml_T4 = nullptr;
+  std::tuple<int, int, int, int, uint64_t, uint64_t> ml_key{-1, -1, -1, -1, 0, 0};
+  cudaGraphExec_t ml_g4 = nullptr, ml_g2 = nullptr;
   unsigned wave_spin_limit = 0;    // polls per neighbour wait (0: the kernel's default)
   int wave_stall_tile = -1;        // test hook: this tile never publishes its phases (-1: none)
 };
@@ -84,6 +91,16 @@ void set_error(const std::string &msg);
 int cuda_fail(cudaError_t e, const char *what);
 extern std::atomic<unsigned long long> g_launches;
 int ensure_scratch(u1_lattice *lat, size_t partial_doubles, size_t out_doubles);
+// Tuning trials: the shortest of `reps` individually timed replays of graph
+// `ex` on stream `s` after `warm` untimed ones, in microseconds.  The
+// shortest replay is insensitive to clock ramps and power-cap drift that an
+// average over back-to-back replays picks up.
+cudaError_t time_graph_min(cudaGraphExec_t ex, cudaStream_t s, int warm, int reps, double *us);
+// Replay `ex` for at least `ms` milliseconds of device time (clock warm-up
+// before the first trial of a tuning run).
+cudaError_t warm_clocks(cudaGraphExec_t ex, cudaStream_t s, double ms);
+// U1_TUNE_VERBOSE=1: tuners print every trial to stderr.
+bool tune_verbose();
 // Every device allocation of the library: cudaMalloc / cudaFree unless the
 // caller installed its own pair (u1_set_device_allocator).  A failed
 // allocation returns cudaErrorMemoryAllocation and leaves *p null.

@@ -84,7 +84,7 @@ def table(res: dict) -> str:
     for r in range(len(res["C_ml"])):
         em, es = res["err_ml"][r], res["err_sl"][r]
         lines.append(f"| {r + 1} | {res['C_ml'][r]:.4e} | {em:.2e} | {res['C_sl'][r]:.4e} | {es:.2e} | "
-                     f"{es / em:.1f} |")
+                     f"{es / em:.3g} |")
     return "\n".join(lines)
 
 

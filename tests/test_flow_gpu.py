@@ -215,7 +215,80 @@ def test_fused_sampler_consistent_with_inverse():
     assert (lq2 - logq).abs().max().item() < 0.5
 
 
-@pytest.mark.parametrize("L,layer", [(8, 0), (8, 3), (16, 4), (16, 7)])
+def _layer_ref_fp32_inverse(c, th):
+    """The inverse coupling layer in plain torch FP32 with bf16-rounded
+    weights and the library's elementwise inverse transform (its analytic
+    backward is checked against float64 in test_ncp_inverse_and_backward)."""
+    import torch.nn.functional as Fn
+    from latticeu1_b200.flow import ncp_inverse, plaquettes_no
+    r = lambda t: t + (t.detach().to(torch.bfloat16).float() - t.detach())
+    torch.backends.cudnn.allow_tf32 = False
+    B = th.shape[0]
+    P = plaquettes_no(th)
+    ctx = torch.stack([torch.cos(P), torch.sin(P)], 1) * c.frozen
+    h = Fn.conv2d(Fn.pad(ctx, (1, 1, 1, 1), mode="circular"), r(c.net[0].weight), r(c.net[0].bias))
+    h = Fn.leaky_relu(h, c.net[1].negative_slope)
+    prm = Fn.conv2d(Fn.pad(h, (1, 1, 1, 1), mode="circular"), r(c.net[2].weight), r(c.net[2].bias))
+    prm = prm.reshape(B, 2 * c.K + 1, -1)[:, :, c.act_idx].permute(0, 2, 1).reshape(-1, 2 * c.K + 1)
+    Pa = P.reshape(B, -1)[:, c.act_idx].reshape(-1)
+    dx, logd = ncp_inverse(Pa, prm, c.K)
+    return c._apply_delta(th, dx), logd.reshape(B, -1).sum(1)
+
+
+def _random_coupling(L, layer, seed):
+    torch.manual_seed(seed)
+    c = Coupling(L, layer % 2, (layer // 2) % 4, K=6, hidden=32).cuda()
+    with torch.no_grad():
+        for m in c.net:
+            if isinstance(m, torch.nn.Conv2d):
+                m.weight.normal_(0, 0.2)
+                m.bias.normal_(0, 0.2)
+    return c
+
+
+@pytest.mark.parametrize("L,layer", [(8, 1), (16, 6), (32, 3)])
+def test_fused_inverse_layer(L, layer):
+    """u1_flow_layer_inverse undoes u1_flow_layer_forward, returns the same
+    log-det, and equals the torch inverse layer (FP32, bf16-rounded weights)."""
+    c = _random_coupling(L, layer, 30 + layer)
+    th = torch.rand(16, 2, L, L, device="cuda") * TWO_PI
+    with torch.no_grad():
+        fw, ld_f = c.forward_fused(th)
+        back, ld_i = c.inverse_fused(fw)
+        want, want_ld = _layer_ref_fp32_inverse(c, fw)
+    d = torch.remainder(back - th + math.pi, TWO_PI) - math.pi
+    assert d.abs().max().item() < 5e-4
+    assert (ld_i - ld_f).abs().max().item() < 5e-3
+    d = torch.remainder(back - want + math.pi, TWO_PI) - math.pi
+    assert d.abs().max().item() < 2e-4
+    assert (ld_i - want_ld).abs().max().item() < 2e-3
+
+
+@pytest.mark.parametrize("L,layer", [(8, 2), (32, 5)])
+def test_fused_inverse_backward_matches_autograd(L, layer):
+    """Gradients of the fused inverse layer equal torch autograd through the
+    FP32 inverse reference layer."""
+    c = _random_coupling(L, layer, 40 + layer)
+    B = 8
+    th0 = torch.rand(B, 2, L, L, device="cuda") * TWO_PI
+    R = torch.randn(B, 2, L, L, device="cuda")
+    r = torch.randn(B, device="cuda")
+
+    def run(fn):
+        c.zero_grad(set_to_none=True)
+        th = th0.clone().requires_grad_(True)
+        out, ld = fn(th)
+        ((out * R).sum() + (ld * r).sum()).backward()
+        return th.grad.clone(), [p.grad.clone() for p in c.parameters()]
+
+    g_f, w_f = run(c.inverse_fused)
+    g_r, w_r = run(lambda t: _layer_ref_fp32_inverse(c, t))
+    assert torch.allclose(g_f, g_r, atol=3e-3, rtol=3e-3)
+    for a, b in zip(w_f, w_r):
+        assert torch.allclose(a, b, atol=5e-3 * max(1.0, b.abs().max().item()), rtol=3e-3)
+
+
+@pytest.mark.parametrize("L,layer", [(8, 0), (8, 3), (16, 4), (16, 7), (32, 1), (32, 6)])
 def test_fused_layer_backward_matches_autograd(L, layer):
     """Gradients of the fused layer (theta and all weights) equal torch autograd
     through the FP32 reference layer with the same bf16-rounded weights."""
