@@ -253,17 +253,20 @@ def analyse(out: Path, k: int, oracle_dir: str | None = None) -> dict | None:
     ref = observables(np.load(out / f"ref_{k}.npy")[therm:])
     res["ours"], res["ref"] = summarize(ours), summarize(ref)
     res["pull_ref"] = pulls(res["ours"], res["ref"])
-    odir = Path(oracle_dir) if oracle_dir else out
-    if (odir / f"oracle_{k}.npy").exists():
-        ometa = json.load(open(odir / f"oracle_{k}.json"))
+    floor = {o: res["ours"][o]["tau_int"] for o in OBS}
+    # the short oracle arm started from our thermalised configuration (`gpu`)
+    # and the independent oracle chain with its own thermalisation (`oracle-chain`)
+    for tag, d in (("oracle", out), ("oracle_chain", Path(oracle_dir) if oracle_dir else None)):
+        if d is None or not (d / f"oracle_{k}.npy").exists():
+            continue
+        ometa = json.load(open(d / f"oracle_{k}.json"))
+        if (tag == "oracle") == bool(ometa.get("independent")):
+            continue
         drop = 0 if ometa.get("independent") else meta["oracle_drop"]
-        orc = observables(np.load(odir / f"oracle_{k}.npy")[drop:])
-        res["oracle"] = summarize(orc, nbins=10, tau_floor={o: res["ours"][o]["tau_int"] for o in OBS})
-        res["pull_oracle"] = pulls(res["ours"], res["oracle"])
-        res["oracle_meta"] = ometa
-        # the oracle chain starts from our thermalised configuration: its
-        # first sweeps show whether that configuration is in equilibrium
-        res["oracle_first"] = observables(np.load(odir / f"oracle_{k}.npy")[:5]).tolist()
+        orc = observables(np.load(d / f"oracle_{k}.npy")[drop:])
+        res[tag] = summarize(orc, nbins=10, tau_floor=floor)
+        res["pull_" + tag] = pulls(res["ours"], res[tag])
+        res[tag + "_meta"] = ometa
     return res
 
 
@@ -277,7 +280,8 @@ def _report(args) -> None:
     print("| configuration | arm | sweeps used | " + " | ".join(OBS) + " | tau_int (P_SS, P_ST, |L|) |")
     print("|---|---|---|" + "---|" * len(OBS) + "---|")
     for r in rows:
-        for arm, label in (("ours", "ours"), ("ref", "reference CUDA"), ("oracle", "FP64 oracle")):
+        for arm, label in (("ours", "ours"), ("ref", "reference CUDA"), ("oracle", "FP64 oracle (from ours)"),
+                           ("oracle_chain", "FP64 oracle (own chain)")):
             if arm not in r:
                 continue
             s = r[arm]
@@ -291,7 +295,8 @@ def _report(args) -> None:
     print("|---|---|" + "---|" * len(OBS))
     allp = []
     for r in rows:
-        for key, label in (("pull_ref", "reference CUDA"), ("pull_oracle", "FP64 oracle")):
+        for key, label in (("pull_ref", "reference CUDA"), ("pull_oracle", "FP64 oracle (from ours)"),
+                           ("pull_oracle_chain", "FP64 oracle (own chain)")):
             if key in r:
                 allp += list(r[key].values())
                 print(f"| {r['config']['name']} | {label} | " + " | ".join(f"{r[key][o]:+.2f}" for o in OBS) + " |")
