@@ -687,23 +687,28 @@ static int launch_phase(const UpdArgs &a, cudaStream_t s, bool met, int src, int
 // lattice, so a plane and its neighbour planes are loaded many waves apart
 // and miss in L2 (measured at 64^4: 1.5x the algorithmic DRAM reads, L2 hit
 // rate 22 %).  U1_REMAP=0 in the environment keeps the launch order always.
+// Whether a four-site phase at the lattice's block size runs as a single
+// wave (the SM-local block order then applies); cached per block size.
+static void quad_layout(u1_lattice *lat) {
+  if (lat->remap_block == lat->block) return;
+  const int sms = lat->ctx->prop.multiProcessorCount;
+  const int threads = std::min(lat->block, 128);
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_update_quad<4, 0, false, SRC_PHILOX>, threads, 0) !=
+      cudaSuccess)
+    per_sm = 0;
+  const long long blocks = ((long long)lat->g.Vh / 4 + threads - 1) / threads;
+  lat->remap_sms = (per_sm > 0 && blocks <= (long long)per_sm * sms) ? sms : 0;
+  lat->remap_block = lat->block;
+}
+
 static int sm_remap(u1_lattice *lat) {
   static const bool off = [] {
     const char *r = std::getenv("U1_REMAP");
     return r && r[0] == '0';
   }();
-  if (off) return 0;
-  if (lat->remap_block != lat->block) {
-    const int sms = lat->ctx->prop.multiProcessorCount;
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_update_quad<4, 0, false, SRC_PHILOX>, lat->block,
-                                                      0) != cudaSuccess)
-      per_sm = 0;
-    const long long blocks = ((long long)lat->g.Vh / 4 + lat->block - 1) / lat->block;
-    lat->remap_sms = (per_sm > 0 && blocks <= (long long)per_sm * sms) ? sms : 0;
-    lat->remap_block = lat->block;
-  }
-  return lat->remap_sms;
+  quad_layout(lat);
+  return off ? 0 : lat->remap_sms;
 }
 
 // The proposal settings of `lat` into the kernel arguments.

@@ -323,3 +323,32 @@ def test_batch_tune_and_cache(ctx, monkeypatch, tmp_path):
     assert b2.tune() == int(rows[0][1])
     assert b2.layout() == lay
     assert len([r for r in f.read_text().splitlines() if r]) == 1  # applied from the cache, not re-tuned
+
+
+def test_quad_multi_wave_bit_identical(ctx):
+    """A four-site phase larger than one wave (40^4: 2500 blocks of 128
+    threads, launch order) gives the two-site kernel's links bit for bit.
+    The measured sweep's sums are
+    bit-identical between block sizes of the four-site kernel; against the
+    two-site kernel they agree to rounding (its per-thread partial sums hold
+    two sites instead of four)."""
+    import torch
+    N = (40, 40, 40, 40)
+    res = []
+    for variant, block in ((5, 128), (5, 64), (1, 256)):
+        lat = Lattice(ctx, 4, N, 1.0)
+        lat.set_variant(variant)
+        lat.set_block(block)
+        rng = Rng(ctx, 404)
+        lat.hot_start(rng)
+        lat.update(rng, 1, 4)
+        out = torch.zeros(6, dtype=torch.float64, device="cuda")
+        lat.update_measure(rng, 2, 1, out.data_ptr())
+        torch.cuda.synchronize()
+        res.append((lat.export_angles(), out.cpu().numpy(), rng.state))
+        lat.close()
+    for th, m, st in res[1:]:
+        assert np.array_equal(th, res[0][0])
+        assert st == res[0][2]
+    assert np.array_equal(res[1][1], res[0][1])
+    assert np.abs(res[2][1] - res[0][1]).max() < 1e-9
