@@ -444,6 +444,26 @@ int u1_flow_layer_inverse_backward(const float *theta_in, const float *grad_thet
 /* Number of kernels this library has launched in the calling process. */
 int u1_kernel_launch_count(uint64_t *out);
 
+/* Checked build (libu1b200_check.so, compiled with -DU1_BOUNDS_CHECK; a test
+ * build: the reference has none, its kernels run unchecked).  Every link
+ * access of the update kernels (single-lattice, batched, measuring and
+ * persistent phases) is checked against the (direction, parity) half it
+ * addresses and its alignment; a violating access is counted and skipped,
+ * never performed.  After every phase a kernel counts the links that were
+ * written and also read by another thread, or written twice, in that phase
+ * (checkerboard races; not for the persistent variant 4, whose phases
+ * overlap within one launch).
+ * u1_check_report: out[0] violations, out[1] races, out[2] phases checked,
+ * out[3] links accessed (summed over the phases), out[4..6] index, half size
+ * and kind (0 read, 1 own read, 2 write) of the first violation (-1: none),
+ * out[7] a raced link's buffer offset (-1: none); synchronises the device;
+ * reset != 0 clears the counters.  u1_check_selftest runs the checks on a
+ * 16-link slab with two refused accesses and two races planted in the marks
+ * (never dereferenced) and reports as u1_check_report.  In the normal build
+ * both return U1_ERR_UNSUPPORTED. */
+int u1_check_report(u1_ctx *ctx, int64_t out[8], int reset);
+int u1_check_selftest(u1_ctx *ctx, int64_t out[8]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,15 +1,19 @@
 """ctypes binding of the C ABI declared in include/u1_b200.h.
 
 The shared library is latticeu1_b200/lib/libu1b200.so, built in-tree by
-latticeu1_b200/build.py.  There is no fallback: if the library is missing
-or cannot be loaded, importing this module raises.
+latticeu1_b200/build.py.  With U1_CHECKED=1 in the environment the checked
+build libu1b200_check.so (bounds and race checks on every link access of the
+update kernels; a test build) is loaded instead.  There is no fallback: if
+the library is missing or cannot be loaded, importing this module raises.
 """
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
-LIB_PATH = Path(__file__).resolve().parent / "lib" / "libu1b200.so"
+CHECKED = os.environ.get("U1_CHECKED", "0") not in ("", "0")
+LIB_PATH = Path(__file__).resolve().parent / "lib" / ("libu1b200_check.so" if CHECKED else "libu1b200.so")
 
 U1_OK = 0
 U1_ERR_INVALID = -1
@@ -123,6 +127,8 @@ SIGNATURES = {
     "u1_set_device_allocator": [DEV_ALLOC_FN, DEV_FREE_FN, _vp],
     "u1_device_allocations": [C.POINTER(C.c_int64)],
     "u1_lattice_set_wave_wait": [_vp, C.c_uint, _i],
+    "u1_check_report": [_vp, C.POINTER(C.c_int64), _i],
+    "u1_check_selftest": [_vp, C.POINTER(C.c_int64)],
     "u1_last_error": [],
     "u1_version": [],
 }
@@ -165,3 +171,24 @@ def launch_count() -> int:
     v = C.c_uint64(0)
     check(lib.u1_kernel_launch_count(C.byref(v)), "u1_kernel_launch_count")
     return int(v.value)
+
+
+def check_report(ctx, reset: bool = False) -> dict:
+    """Counters of the checked build (U1_CHECKED=1): bounds violations,
+    races, phases checked, links accessed and the first violation."""
+    out = (C.c_int64 * 8)()
+    check(lib.u1_check_report(ctx, out, 1 if reset else 0), "u1_check_report")
+    return _check_dict(out)
+
+
+def check_selftest(ctx) -> dict:
+    """The checked build's checks on a planted 16-link case (u1_check_selftest)."""
+    out = (C.c_int64 * 8)()
+    check(lib.u1_check_selftest(ctx, out), "u1_check_selftest")
+    return _check_dict(out)
+
+
+def _check_dict(out) -> dict:
+    keys = ("bad", "races", "phases", "marked", "first_bad_idx", "first_bad_half", "first_bad_kind",
+            "first_race_link")
+    return {k: int(v) for k, v in zip(keys, out)}

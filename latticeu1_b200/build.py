@@ -2,7 +2,8 @@
 
 `python latticeu1_b200/build.py` compiles latticeu1_b200/csrc/*.cu with nvcc
 into latticeu1_b200/lib/libu1b200.so (in-tree, so it travels with the
-repository snapshot).  No JIT cache is used.
+repository snapshot); `--checked` also builds the checked test library
+libu1b200_check.so (-DU1_BOUNDS_CHECK).  No JIT cache is used.
 """
 from __future__ import annotations
 
@@ -10,6 +11,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -38,37 +40,61 @@ def _stale(target: Path, deps: list[Path]) -> bool:
     return any(d.stat().st_mtime > t for d in deps)
 
 
-def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> Path:
-    """Compile every CUDA source into one shared library; returns its path."""
-    LIBDIR.mkdir(exist_ok=True)
+def _deps() -> list[Path]:
     deps = sources() + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + [ROOT / "include" / "u1_b200.h"]
-    deps += sorted((PKG / "shim").rglob("*.cpp")) + sorted((PKG / "shim").rglob("*.h"))
-    if not force and not _stale(LIB, deps):
-        return LIB
-    objdir = LIBDIR / "obj"
-    objdir.mkdir(exist_ok=True)
+    return deps + sorted((PKG / "shim").rglob("*.cpp")) + sorted((PKG / "shim").rglob("*.h"))
+
+
+def _compile_lib(target: Path, objdir: Path, defines: list[str], verbose: bool) -> None:
+    """Every CUDA source (compiled in parallel) linked into `target`."""
+    objdir.mkdir(parents=True, exist_ok=True)
     # -fmad=false: no compiler-chosen multiply-add contraction, so the
     # one-site, two-site and fused-measurement update kernels round every
     # link update identically (FMAs are written out where wanted).
     flags = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC",
                     "-I" + str(ROOT / "include"), "-I" + str(CSRC),
-                    "--expt-relaxed-constexpr"] + (extra or [])
-    objs = []
+                    "--expt-relaxed-constexpr"] + defines
+    cmds, objs = [], []
     for src in sources():
         obj = objdir / (src.stem + ".o")
-        cmd = [nvcc()] + flags + ["-c", str(src), "-o", str(obj)]
+        cmds.append([nvcc()] + flags + ["-c", str(src), "-o", str(obj)])
+        objs.append(str(obj))
+
+    def run(cmd: list[str]) -> None:
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-        objs.append(str(obj))
-    tmp = LIB.with_suffix(".so.tmp")
-    cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", str(tmp)] + objs
-    if verbose:
-        print(" ".join(cmd), flush=True)
-    subprocess.run(cmd, check=True)
-    os.replace(tmp, LIB)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as pool:
+        for f in [pool.submit(run, c) for c in cmds]:
+            f.result()
+    tmp = target.with_suffix(".so.tmp")
+    run([nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", str(tmp)] + objs)
+    os.replace(tmp, target)
+
+
+def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> Path:
+    """Compile every CUDA source into one shared library; returns its path."""
+    LIBDIR.mkdir(exist_ok=True)
+    if not force and not _stale(LIB, _deps()):
+        return LIB
+    _compile_lib(LIB, LIBDIR / "obj", list(extra or []), verbose)
     build_shim(verbose=verbose)
     return LIB
+
+
+CHECK_LIB = LIBDIR / "libu1b200_check.so"
+
+
+def build_checked(force: bool = False, verbose: bool = False) -> Path:
+    """The checked build (-DU1_BOUNDS_CHECK): the same sources with bounds and
+    race checks on every link access of the update kernels, loaded instead of
+    libu1b200.so when U1_CHECKED=1 (test infrastructure)."""
+    LIBDIR.mkdir(exist_ok=True)
+    if not force and not _stale(CHECK_LIB, _deps()):
+        return CHECK_LIB
+    _compile_lib(CHECK_LIB, LIBDIR / "obj_check", ["-DU1_BOUNDS_CHECK"], verbose)
+    return CHECK_LIB
 
 
 SHIM = PKG / "shim"
@@ -93,3 +119,5 @@ def build_shim(verbose: bool = False) -> Path:
 if __name__ == "__main__":
     force = "--force" in sys.argv
     print(build(force=force, verbose=True))
+    if "--checked" in sys.argv:
+        print(build_checked(force=force, verbose=True))

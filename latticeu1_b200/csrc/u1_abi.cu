@@ -227,6 +227,10 @@ extern "C" int u1_ctx_create(int device, u1_ctx **out) {
 
 extern "C" int u1_ctx_destroy(u1_ctx *ctx) {
   if (!ctx) return U1_OK;
+  if (ctx->chk) {
+    cudaSetDevice(ctx->device);
+    u1i::dev_free(ctx->chk);
+  }
   delete ctx;
   return U1_OK;
 }
@@ -326,6 +330,13 @@ extern "C" int u1_lattice_create(u1_ctx *ctx, const u1_geom *geom, u1_lattice **
     u1i::set_error(std::string("u1_lattice_create: link allocation: ") + cudaGetErrorString(e));
     return U1_ERR_NOMEM;
   }
+#ifdef U1_BOUNDS_CHECK
+  lat->shadow = u1i::chk_shadow(nl);
+  if (!lat->shadow || !u1i::chk_state(ctx)) {
+    u1_lattice_destroy(lat);
+    return fail(U1_ERR_NOMEM, "u1_lattice_create: no device memory for the access checks");
+  }
+#endif
   rc = u1_cold_start(lat);
   if (rc) {
     u1_lattice_destroy(lat);
@@ -353,6 +364,7 @@ extern "C" int u1_lattice_destroy(u1_lattice *lat) {
   u1i::dev_free(lat->ml_P2);
   u1i::dev_free(lat->ml_T2);
   u1i::dev_free(lat->ml_T4);
+  u1i::dev_free(lat->shadow);
   if (lat->own_stream) cudaStreamDestroy(lat->own_stream);
   delete lat;
   return U1_OK;
@@ -767,6 +779,13 @@ static int launch_wave(u1_lattice *lat, float2 *links, u1_rng *rng, int metrop, 
   w.pass_rw = rng->pass_dev;
   w.spin_limit = lat->wave_spin_limit ? lat->wave_spin_limit : kWaveSpinLimit;
   w.stall_tile = lat->wave_stall_tile;
+#ifdef U1_BOUNDS_CHECK
+  // bounds checks only: the persistent sweep's phases overlap within the
+  // launch, so there is no phase end for the race marks
+  w.a.chk = lat->ctx->chk;
+  w.a.shadow = nullptr;
+  w.a.chk_base = links;
+#endif
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)tiles);
   cfg.blockDim = dim3((unsigned)wave_threads(lat->g));
@@ -925,6 +944,11 @@ static int issue_sweep(u1_lattice *lat, float2 *links, u1_rng *rng, int metrop, 
   a.replay_base = rng->replay_base;
   a.ml = ml;
   set_proposal(a, lat);
+#ifdef U1_BOUNDS_CHECK
+  a.chk = lat->ctx->chk;
+  a.shadow = lat->shadow;
+  a.chk_base = links;
+#endif
   // with a freeze period the SM-local order would hand whole frozen slabs to
   // some SMs and none to others (measured 4 % slower multilevel): keep the launch order
   a.sms = ml ? 0 : sm_remap(lat);
@@ -936,14 +960,20 @@ static int issue_sweep(u1_lattice *lat, float2 *links, u1_rng *rng, int metrop, 
   int phase = 0;
   auto launch = [&](bool met) -> int {
     ++phase;
+    int rc;
     // the last pass is phases total-2D+1 .. total; its parity-1 half with mu >= 1 measures
     if (meas_partials && phase > total - 2 * D && a.p == 1 && a.mu >= 1)
-      return D == 2 ? launch_meas_phase<2>(a, lat->stream, met, src == SRC_WINDOW, var == U1V_QUAD, meas_partials)
-           : D == 3 ? launch_meas_phase<3>(a, lat->stream, met, src == SRC_WINDOW, var == U1V_QUAD, meas_partials)
-                    : launch_meas_phase<4>(a, lat->stream, met, src == SRC_WINDOW, var == U1V_QUAD, meas_partials);
-    return D == 2 ? launch_phase<2>(a, lat->stream, met, src, var, lat->block)
+      rc = D == 2 ? launch_meas_phase<2>(a, lat->stream, met, src == SRC_WINDOW, var == U1V_QUAD, meas_partials)
+         : D == 3 ? launch_meas_phase<3>(a, lat->stream, met, src == SRC_WINDOW, var == U1V_QUAD, meas_partials)
+                  : launch_meas_phase<4>(a, lat->stream, met, src == SRC_WINDOW, var == U1V_QUAD, meas_partials);
+    else
+      rc = D == 2 ? launch_phase<2>(a, lat->stream, met, src, var, lat->block)
          : D == 3 ? launch_phase<3>(a, lat->stream, met, src, var, lat->block)
                   : launch_phase<4>(a, lat->stream, met, src, var, lat->block);
+#ifdef U1_BOUNDS_CHECK
+    if (rc == U1_OK) rc = u1i::chk_phase_end(lat->stream, a.shadow, (size_t)D * lat->g.V, a.chk);
+#endif
+    return rc;
   };
   for (int m = 0; m < metrop; ++m)
     for (int p = 0; p < 2; ++p)
@@ -1330,13 +1360,23 @@ extern "C" int u1_update_phase(u1_lattice *lat, u1_rng *rng, int metropolis, int
   a.replay_base = rng->replay_base;
   set_proposal(a, lat);
   a.sms = sm_remap(lat);
+#ifdef U1_BOUNDS_CHECK
+  a.chk = lat->ctx->chk;
+  a.shadow = lat->shadow;
+  a.chk_base = lat->links;
+#endif
   const int src = metropolis_src(lat, rng);
   const int var = sweep_variant(lat, src, 0);
+  int rc;
   switch (lat->g.dims) {
-    case 2: return launch_phase<2>(a, lat->stream, met, src, var, lat->block);
-    case 3: return launch_phase<3>(a, lat->stream, met, src, var, lat->block);
-    default: return launch_phase<4>(a, lat->stream, met, src, var, lat->block);
+    case 2: rc = launch_phase<2>(a, lat->stream, met, src, var, lat->block); break;
+    case 3: rc = launch_phase<3>(a, lat->stream, met, src, var, lat->block); break;
+    default: rc = launch_phase<4>(a, lat->stream, met, src, var, lat->block); break;
   }
+#ifdef U1_BOUNDS_CHECK
+  if (rc == U1_OK) rc = u1i::chk_phase_end(lat->stream, a.shadow, (size_t)lat->g.dims * lat->g.V, a.chk);
+#endif
+  return rc;
 }
 
 // ---------------------------------------------------------------- measurements

@@ -53,6 +53,11 @@ struct BatchPhase {
   const unsigned long long *pass_dev;
   unsigned long long *bump_ptr;
   unsigned int bump_by;
+#ifdef U1_BOUNDS_CHECK
+  ChkState *chk;           // checked build: counters, per-link marks of the batch's links
+  unsigned *shadow;
+  const float2 *chk_base;
+#endif
 };
 
 __device__ __forceinline__ void stage_chain(const BatchChain *__restrict__ chains, int c, BatchChain &sch) {
@@ -80,6 +85,11 @@ __device__ __forceinline__ UpdArgs batch_args(const BatchChain &sch, const Batch
   a.hit = ph.hit;
   a.bump_ptr = ph.bump_ptr;
   a.bump_by = ph.bump_by;
+#ifdef U1_BOUNDS_CHECK
+  a.chk = ph.chk;
+  a.shadow = ph.shadow;
+  a.chk_base = ph.chk_base;
+#endif
   return a;
 }
 
@@ -102,19 +112,7 @@ __global__ void __launch_bounds__(256, 8)
   const int blk = (int)blockIdx.x + ph.block_base;
   const int cidx = __ldg(block_chain + blk);
   stage_chain(chains, cidx, sch);
-  UpdArgs a{};
-  a.lat = sch.links;
-  a.g = sch.g;
-  a.c = sch.c;
-  a.p = ph.p;
-  a.mu = MU;
-  a.key0 = ph.key0;
-  a.key1 = ph.key1;
-  a.chain = sch.chain;
-  a.pass_dev = ph.pass_dev;
-  a.hit = ph.hit;
-  a.bump_ptr = ph.bump_ptr;
-  a.bump_by = ph.bump_by;
+  const UpdArgs a = batch_args(sch, ph, MU);
   const int local = blk - sch.first_upd;
   if (PAIR)
     update_pair_body<D, MU, MET, SRC_PHILOX>(a, 2 * (local * blockDim.x + threadIdx.x));
@@ -206,6 +204,7 @@ struct u1_batch {
   size_t group_bytes = 64ull << 20;       // group size limit the groups were cut with
   bool quad_enabled = true;               // four-site kernels allowed (U1_BATCH_QUAD=0: no)
   float2 *backup = nullptr;               // link backup while tuning
+  unsigned *shadow = nullptr;              // checked build: per-link access marks (total_links words)
 };
 
 using u1i::cuda_fail;
@@ -320,6 +319,7 @@ extern "C" int u1_batch_destroy(u1_batch *b) {
   u1i::dev_free(b->partials);
   u1i::dev_free(b->d_out);
   u1i::dev_free(b->pass_dev);
+  u1i::dev_free(b->shadow);
   if (b->h_out) cudaFreeHost(b->h_out);
   if (b->own_stream) cudaStreamDestroy(b->own_stream);
   delete b;
@@ -409,6 +409,13 @@ extern "C" int u1_batch_create(u1_ctx *ctx, int nchains, const u1_geom *geoms, u
     u1i::set_error(std::string("u1_batch_create: ") + cudaGetErrorString(e));
     return U1_ERR_NOMEM;
   }
+#ifdef U1_BOUNDS_CHECK
+  b->shadow = u1i::chk_shadow(b->total_links);
+  if (!b->shadow || !u1i::chk_state(ctx)) {
+    u1_batch_destroy(b);
+    return bfail(U1_ERR_NOMEM, "u1_batch_create: no device memory for the access checks");
+  }
+#endif
   for (int c = 0; c < nchains; ++c) b->h_chains[c].links = b->links + offsets[c];
   e = cudaMemcpy(b->d_tab_site, tab_site.data(), sizeof(int) * tab_site.size(), cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
@@ -561,6 +568,11 @@ static int batch_issue_sweep(u1_batch *b, int metrop, int ovrn, bool measure, in
   ph.key0 = (uint32_t)b->seed;
   ph.key1 = (uint32_t)(b->seed >> 32);
   ph.pass_dev = b->pass_dev;
+#ifdef U1_BOUNDS_CHECK
+  ph.chk = b->ctx->chk;
+  ph.shadow = b->shadow;
+  ph.chk_base = b->links;
+#endif
   const int D = b->dims;
   const int ngroups = g1 < 0 ? (int)b->groups.size() : g1;
   // Each chain group runs the whole sweep before the next starts.  Every
@@ -569,9 +581,13 @@ static int batch_issue_sweep(u1_batch *b, int metrop, int ovrn, bool measure, in
   bool bumped = (metrop == 0);
   for (int grp = g0; grp < ngroups; ++grp) {
     auto run = [&](int mu, bool met) {
-      return D == 2 ? batch_phase<2>(b, ph, mu, met, grp)
-           : D == 3 ? batch_phase<3>(b, ph, mu, met, grp)
-                    : batch_phase<4>(b, ph, mu, met, grp);
+      int rc = D == 2 ? batch_phase<2>(b, ph, mu, met, grp)
+             : D == 3 ? batch_phase<3>(b, ph, mu, met, grp)
+                      : batch_phase<4>(b, ph, mu, met, grp);
+#ifdef U1_BOUNDS_CHECK
+      if (rc == U1_OK) rc = u1i::chk_phase_end(b->stream, ph.shadow, b->total_links, ph.chk);
+#endif
+      return rc;
     };
     for (int m = 0; m < metrop; ++m)
       for (int p = 0; p < 2; ++p)

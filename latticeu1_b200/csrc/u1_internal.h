@@ -11,10 +11,15 @@
 #include "u1_b200.h"
 #include "u1_geom.cuh"
 
+namespace u1b {
+struct ChkState;
+}
+
 struct u1_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaDeviceProp prop{};
+  u1b::ChkState *chk = nullptr;     // checked build: access-check counters (device)
 };
 
 struct u1_rng {
@@ -75,6 +80,7 @@ struct u1_lattice {
   cudaGraphExec_t ml_g4 = nullptr, ml_g2 = nullptr;
   unsigned wave_spin_limit = 0;    // polls per neighbour wait (0: the kernel's default)
   int wave_stall_tile = -1;        // test hook: this tile never publishes its phases (-1: none)
+  unsigned *shadow = nullptr;      // checked build: per-link access marks (V*dims words)
 };
 
 namespace u1i {
@@ -113,6 +119,13 @@ inline cudaError_t dev_alloc(T **p, size_t bytes) {
   *p = static_cast<T *>(v);
   return e;
 }
+// Checked build (-DU1_BOUNDS_CHECK): counters of the context (allocated on
+// first use) and a zeroed shadow of n words; elsewhere both return null.
+u1b::ChkState *chk_state(u1_ctx *ctx);
+unsigned *chk_shadow(size_t n);
+// Checked build: the race check and reset of the shadow after one phase on
+// stream s (no-op when shadow is null or in the normal build).
+int chk_phase_end(cudaStream_t s, unsigned *shadow, size_t n, u1b::ChkState *st);
 // Geometry from the ABI struct (Grid mapping of the reference's
 // SetupLatticeParameters); U1_ERR_INVALID on odd extents.
 int make_geom(const u1_geom *geom, u1b::GeomK &g);

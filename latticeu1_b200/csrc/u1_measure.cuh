@@ -181,14 +181,14 @@ __device__ __forceinline__ void plaq_sites_pair(const float2 *__restrict__ lat, 
     const int q = 1 - p;
     Pair2 U[D];
 #pragma unroll
-    for (int mu = 0; mu < D; ++mu) U[mu] = ld_vec2(lat + mu * g.V + p * g.Vh, i);
+    for (int mu = 0; mu < D; ++mu) U[mu] = ld_vec2(lat + mu * g.V + p * g.Vh, i, no_chk());
 #pragma unroll
     for (int mu = 0; mu < D - 1; ++mu) {
 #pragma unroll
       for (int nu = mu + 1; nu < D; ++nu) {
         const float2 *Lq_nu = lat + nu * g.V + q * g.Vh;
-        const Pair2 a = (mu == 0) ? ld_two(Lq_nu, i + fwd[0], i + 1 + f0b) : ld_vec2(Lq_nu, i + fwd[mu]);
-        const Pair2 b = ld_vec2(lat + mu * g.V + q * g.Vh, i + fwd[nu]);  // U_mu(x+nu), nu >= 1
+        const Pair2 a = (mu == 0) ? ld_two(Lq_nu, i + fwd[0], i + 1 + f0b, no_chk()) : ld_vec2(Lq_nu, i + fwd[mu], no_chk());
+        const Pair2 b = ld_vec2(lat + mu * g.V + q * g.Vh, i + fwd[nu], no_chk());  // U_mu(x+nu), nu >= 1
         plaq_accum(U[mu].s0, a.s0, b.s0, U[nu].s0, nu == D - 1, vs);
         plaq_accum(U[mu].s1, a.s1, b.s1, U[nu].s1, nu == D - 1, vs);
       }

@@ -107,7 +107,101 @@ struct UpdArgs {
   float win;                           // SRC_WINDOW: proposal half-width / pi (0: whole circle)
   int nhits;                           // SRC_WINDOW: Metropolis hits per link and pass
   int sms;                             // k_update_quad: > 0 remaps the block order over this many SMs
+#ifdef U1_BOUNDS_CHECK
+  struct ChkState *chk;                // checked build: violation counters (see Chk below)
+  unsigned *shadow;                    // checked build: per-link marks of this phase (nullptr: no race marks)
+  const float2 *chk_base;              // checked build: the link buffer the shadow mirrors
+#endif
 };
+
+// ---------------------------------------------------------------------------
+// Checked build (-DU1_BOUNDS_CHECK, libu1b200_check.so; test infrastructure,
+// never the product path).  Every link access of the update bodies passes
+// chk(): the index must lie inside the (direction, parity) half it addresses
+// (0 <= idx and idx + W <= V/2 for W consecutive links) and a vector access
+// must be aligned to its width.  A violation is counted in ChkState (the
+// first one recorded) and the access is skipped (a load returns zeros), so
+// the kernel never touches memory outside its half of the lattice.  With a
+// shadow array (one word per link of the buffer) every access is also marked:
+// bit 0 for a read of a link the thread does not own, +2 for a write.
+// k_chk_phase_end runs after every phase: a link written and also read by
+// another thread, or written twice, within one phase is a checkerboard race;
+// it counts them and clears the marks.  In the normal build Chk is empty and
+// every check folds to `true`.
+struct ChkState {
+  unsigned long long bad;        // bounds or alignment violations
+  unsigned long long races;      // links written and read (or written twice) within one phase
+  unsigned long long phases;     // phases checked by k_chk_phase_end
+  unsigned long long marked;     // links accessed, summed over the checked phases
+  long long first_bad_idx;       // index, half size and kind of the first violation
+  long long first_bad_half;
+  long long first_race_link;     // buffer offset of a raced link
+  int first_bad_kind;
+  int pad;
+};
+
+struct Chk {
+#ifdef U1_BOUNDS_CHECK
+  ChkState *st;
+  unsigned *shadow;
+  const float2 *base;
+  int Vh;
+#endif
+};
+
+enum : int { CHK_READ = 0, CHK_OWN = 1, CHK_WRITE = 2 };  // another thread's link / the thread's own / a store
+
+__device__ __forceinline__ Chk make_chk(const UpdArgs &a) {
+#ifdef U1_BOUNDS_CHECK
+  return Chk{a.chk, a.shadow, a.chk_base, a.g.Vh};
+#else
+  (void)a;
+  return Chk{};
+#endif
+}
+
+// Callers outside the update bodies (the standalone measurement) are not checked.
+__device__ __forceinline__ Chk no_chk() { return Chk{}; }
+
+// Whether W consecutive links at slab[idx] may be accessed (always true in
+// the normal build); marks them in the checked build.
+template <int W, int KIND>
+__device__ __forceinline__ bool chk(const Chk &c, const float2 *slab, int idx) {
+#ifdef U1_BOUNDS_CHECK
+  if (c.st == nullptr) return true;  // an unchecked caller (no_chk)
+  const bool ok = idx >= 0 && idx + W <= c.Vh && ((uintptr_t)(slab + idx) & (uintptr_t)(W * 8 - 1)) == 0;
+  if (!ok) {
+    if (atomicAdd(&c.st->bad, 1ull) == 0ull) {
+      c.st->first_bad_idx = idx;
+      c.st->first_bad_half = c.Vh;
+      c.st->first_bad_kind = KIND;
+    }
+    return false;
+  }
+  if (c.shadow != nullptr && KIND != CHK_OWN) {
+    unsigned *m = c.shadow + ((slab + idx) - c.base);
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      if (KIND == CHK_READ)
+        atomicOr(m + k, 1u);
+      else
+        atomicAdd(m + k, 2u);
+    }
+  }
+  return true;
+#else
+  (void)c;
+  (void)slab;
+  (void)idx;
+  return true;
+#endif
+}
+
+// One link through the read-only path, checked.
+__device__ __forceinline__ float2 ld1(const float2 *slab, int idx, const Chk &ck) {
+  if (!chk<1, CHK_READ>(ck, slab, idx)) return make_float2(0.f, 0.f);
+  return __ldg(slab + idx);
+}
 
 // Work item of launch-order block b of G when the blocks of a single wave
 // are handed to S SMs round-robin: the blocks that share SM s (b = s, s+S,
@@ -136,7 +230,7 @@ enum : int {
 // the last pass, see update_pair_body); the staple itself is unchanged.
 template <int D, int MU, bool MEAS = false>
 __device__ __forceinline__ float2 staple_steps(const float2 *__restrict__ lat, const GeomK &g, const CoupK &c,
-                                               int i, int p, const int fwd[4], const int bwd[4],
+                                               int i, int p, const int fwd[4], const int bwd[4], const Chk &ck,
                                                float2 *mA = nullptr, float2 *mD = nullptr) {
   const int q = 1 - p;
   const float2 *Lq_mu = lat + MU * g.V + q * g.Vh;
@@ -148,13 +242,13 @@ __device__ __forceinline__ float2 staple_steps(const float2 *__restrict__ lat, c
     const float2 *Lp_nu = lat + nu * g.V + p * g.Vh;
     const float2 *Lq_nu = lat + nu * g.V + q * g.Vh;
     // upper: U_nu(x+mu) conj(U_mu(x+nu)) conj(U_nu(x))
-    const float2 a = __ldg(Lq_nu + i_xm);
-    const float2 b = __ldg(Lq_mu + i + fwd[nu]);
-    const float2 cc = __ldg(Lp_nu + i);
+    const float2 a = ld1(Lq_nu, i_xm, ck);
+    const float2 b = ld1(Lq_mu, i + fwd[nu], ck);
+    const float2 cc = ld1(Lp_nu, i, ck);
     // lower: conj(U_nu(x+mu-nu)) conj(U_mu(x-nu)) U_nu(x-nu)
-    const float2 d = __ldg(Lp_nu + i_xm + bwd[nu]);
-    const float2 e = __ldg(Lq_mu + i + bwd[nu]);
-    const float2 f = __ldg(Lq_nu + i + bwd[nu]);
+    const float2 d = ld1(Lp_nu, i_xm + bwd[nu], ck);
+    const float2 e = ld1(Lq_mu, i + bwd[nu], ck);
+    const float2 f = ld1(Lq_nu, i + bwd[nu], ck);
     const float2 up = cmulc(cmulc(a, b), cc), lo = cmul(cconjmul(d, e), f);
     const float2 sum = cadd(up, lo);
     if (MU == D - 1 || nu == D - 1)
@@ -273,11 +367,13 @@ __device__ __forceinline__ void update_single_body(const UpdArgs a, int i, float
   if (!MEAS && MU != 3 && a.ml > 0 && (x[D - 1] & (a.ml - 1)) == 0) return;
   int fwd[4], bwd[4];
   eo_steps<D>(a.g, x, k, fwd, bwd);
-  float2 *own = a.lat + MU * a.g.V + a.p * a.g.Vh + i;
+  const Chk ck = make_chk(a);
+  float2 *own_slab = a.lat + MU * a.g.V + a.p * a.g.Vh;
   float2 mA = make_float2(0.f, 0.f), mD = mA;
-  const float2 S = staple_steps<D, MU, MEAS>(a.lat, a.g, a.c, i, a.p, fwd, bwd, &mA, &mD);
-  const float2 N = update_one<D, MU, MET, SRC>(a, i, S, *own);
-  *own = N;
+  const float2 S = staple_steps<D, MU, MEAS>(a.lat, a.g, a.c, i, a.p, fwd, bwd, ck, &mA, &mD);
+  const float2 U = chk<1, CHK_OWN>(ck, own_slab, i) ? own_slab[i] : make_float2(0.f, 0.f);
+  const float2 N = update_one<D, MU, MET, SRC>(a, i, S, U);
+  if (chk<1, CHK_WRITE>(ck, own_slab, i)) own_slab[i] = N;
   pdl_release_dependents();
   if (MEAS) *meas = make_float2(2.f * MU - cre_mul(mA, N), cim_mul(mD, N));
 }
@@ -298,14 +394,20 @@ struct Pair2 {
 // for the persistent sweep kernel that reads links other blocks wrote earlier
 // in the same launch (ordered by its acquire fences).
 template <bool COH = false>
-__device__ __forceinline__ Pair2 ld_vec2(const float2 *base, int idx) {
+__device__ __forceinline__ Pair2 ld_vec2(const float2 *base, int idx, const Chk &ck) {
+  if (!chk<2, CHK_READ>(ck, base, idx)) return Pair2{make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
   const float4 *p = reinterpret_cast<const float4 *>(base + idx);
   const float4 t = COH ? __ldca(p) : __ldg(p);
   return Pair2{make_float2(t.x, t.y), make_float2(t.z, t.w)};
 }
 template <bool COH = false>
-__device__ __forceinline__ Pair2 ld_two(const float2 *base, int i0, int i1) {
-  return COH ? Pair2{__ldca(base + i0), __ldca(base + i1)} : Pair2{__ldg(base + i0), __ldg(base + i1)};
+__device__ __forceinline__ float2 ld_one(const float2 *base, int idx, const Chk &ck) {
+  if (!chk<1, CHK_READ>(ck, base, idx)) return make_float2(0.f, 0.f);
+  return COH ? __ldca(base + idx) : __ldg(base + idx);
+}
+template <bool COH = false>
+__device__ __forceinline__ Pair2 ld_two(const float2 *base, int i0, int i1, const Chk &ck) {
+  return Pair2{ld_one<COH>(base, i0, ck), ld_one<COH>(base, i1, ck)};
 }
 
 // upper + lower staple contributions of one nu for both sites
@@ -338,6 +440,7 @@ __device__ __forceinline__ void update_pair_body(const UpdArgs a, int i, float2 
   const int V = a.g.V, Vh = a.g.Vh;
   const float2 *lat = a.lat;
   const float2 *Lq_mu = lat + MU * V + q * Vh;
+  const Chk ck = make_chk(a);
   float2 ss0 = make_float2(0.f, 0.f), ss1 = ss0, st0 = ss0, st1 = ss0;
   float2 mA0 = ss0, mA1 = ss0, mD0 = ss0, mD1 = ss0;  // measurement sums (MEAS), see update_single_body
 #pragma unroll
@@ -346,25 +449,25 @@ __device__ __forceinline__ void update_pair_body(const UpdArgs a, int i, float2 
     const float2 *Lp_nu = lat + nu * V + a.p * Vh;
     const float2 *Lq_nu = lat + nu * V + q * Vh;
     Pair2 A, B, C, Dd, E, F;
-    C = ld_vec2<COH>(Lp_nu, i);
+    C = ld_vec2<COH>(Lp_nu, i, ck);
     if (MU == 0) {  // nu != 0: steps along nu shared, along x0 per site
-      A = ld_two<COH>(Lq_nu, i + f0a, i + 1 + f0b);
-      B = ld_vec2<COH>(Lq_mu, i + fwd[nu]);
-      Dd = ld_two<COH>(Lp_nu, i + f0a + bwd[nu], i + 1 + f0b + bwd[nu]);
-      E = ld_vec2<COH>(Lq_mu, i + bwd[nu]);
-      F = ld_vec2<COH>(Lq_nu, i + bwd[nu]);
+      A = ld_two<COH>(Lq_nu, i + f0a, i + 1 + f0b, ck);
+      B = ld_vec2<COH>(Lq_mu, i + fwd[nu], ck);
+      Dd = ld_two<COH>(Lp_nu, i + f0a + bwd[nu], i + 1 + f0b + bwd[nu], ck);
+      E = ld_vec2<COH>(Lq_mu, i + bwd[nu], ck);
+      F = ld_vec2<COH>(Lq_nu, i + bwd[nu], ck);
     } else if (nu == 0) {  // MU != 0
-      A = ld_vec2<COH>(Lq_nu, i + fwd[MU]);
-      B = ld_two<COH>(Lq_mu, i + f0a, i + 1 + f0b);
-      Dd = ld_two<COH>(Lp_nu, i + fwd[MU] + b0a, i + 1 + fwd[MU] + b0b);
-      E = ld_two<COH>(Lq_mu, i + b0a, i + 1 + b0b);
-      F = ld_two<COH>(Lq_nu, i + b0a, i + 1 + b0b);
+      A = ld_vec2<COH>(Lq_nu, i + fwd[MU], ck);
+      B = ld_two<COH>(Lq_mu, i + f0a, i + 1 + f0b, ck);
+      Dd = ld_two<COH>(Lp_nu, i + fwd[MU] + b0a, i + 1 + fwd[MU] + b0b, ck);
+      E = ld_two<COH>(Lq_mu, i + b0a, i + 1 + b0b, ck);
+      F = ld_two<COH>(Lq_nu, i + b0a, i + 1 + b0b, ck);
     } else {  // MU != 0, nu != 0: every step even, all loads 128-bit
-      A = ld_vec2<COH>(Lq_nu, i + fwd[MU]);
-      B = ld_vec2<COH>(Lq_mu, i + fwd[nu]);
-      Dd = ld_vec2<COH>(Lp_nu, i + fwd[MU] + bwd[nu]);
-      E = ld_vec2<COH>(Lq_mu, i + bwd[nu]);
-      F = ld_vec2<COH>(Lq_nu, i + bwd[nu]);
+      A = ld_vec2<COH>(Lq_nu, i + fwd[MU], ck);
+      B = ld_vec2<COH>(Lq_mu, i + fwd[nu], ck);
+      Dd = ld_vec2<COH>(Lp_nu, i + fwd[MU] + bwd[nu], ck);
+      E = ld_vec2<COH>(Lq_mu, i + bwd[nu], ck);
+      F = ld_vec2<COH>(Lq_nu, i + bwd[nu], ck);
     }
     if (MEAS && nu < MU) {
       // the same operations as staple_term2, with the upper and lower terms kept
@@ -390,8 +493,9 @@ __device__ __forceinline__ void update_pair_body(const UpdArgs a, int i, float2 
   }
   const float2 S0 = cweigh(ss0, a.c.w_ss, st0, a.c.w_st);
   const float2 S1 = cweigh(ss1, a.c.w_ss, st1, a.c.w_st);
-  float4 *own = reinterpret_cast<float4 *>(a.lat + MU * V + a.p * Vh + i);
-  const float4 U = *own;
+  float2 *own_slab = a.lat + MU * V + a.p * Vh;
+  float4 *own = reinterpret_cast<float4 *>(own_slab + i);
+  const float4 U = chk<2, CHK_OWN>(ck, own_slab, i) ? *own : make_float4(0.f, 0.f, 0.f, 0.f);
   // sites i, i+1 (i even, V/2 even) share one Philox block
   Philox4 blk;
   if (MET && SRC != SRC_REPLAY)
@@ -399,7 +503,7 @@ __device__ __forceinline__ void update_pair_body(const UpdArgs a, int i, float2 
                               a.key0, a.key1);
   const float2 N0 = update_one<D, MU, MET, SRC>(a, i, S0, make_float2(U.x, U.y), &blk);
   const float2 N1 = update_one<D, MU, MET, SRC>(a, i + 1, S1, make_float2(U.z, U.w), &blk);
-  *own = make_float4(N0.x, N0.y, N1.x, N1.y);
+  if (chk<2, CHK_WRITE>(ck, own_slab, i)) *own = make_float4(N0.x, N0.y, N1.x, N1.y);
   pdl_release_dependents();
   if (MEAS) {
     // for MU = D-1 every nu < MU term is in st: mA = st
@@ -423,8 +527,13 @@ struct Quad2 {
 // Four consecutive links from a 32-byte aligned address (idx % 4 == 0).
 // Non-coherent (read-only path): a phase kernel never reads what it writes.
 // volatile + "memory" keep the load after the grid-dependency wait.
-__device__ __forceinline__ Quad2 ld_quad(const float2 *base, int idx) {
+__device__ __forceinline__ Quad2 ld_quad(const float2 *base, int idx, const Chk &ck) {
   Quad2 q;
+  if (!chk<4, CHK_READ>(ck, base, idx)) {
+#pragma unroll
+    for (int s = 0; s < 4; ++s) q.s[s] = make_float2(0.f, 0.f);
+    return q;
+  }
   asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
                : "=f"(q.s[0].x), "=f"(q.s[0].y), "=f"(q.s[1].x), "=f"(q.s[1].y), "=f"(q.s[2].x), "=f"(q.s[2].y),
                  "=f"(q.s[3].x), "=f"(q.s[3].y)
@@ -433,8 +542,14 @@ __device__ __forceinline__ Quad2 ld_quad(const float2 *base, int idx) {
   return q;
 }
 // The same through the coherent path (the thread's own links, stored later).
-__device__ __forceinline__ Quad2 ld_quad_own(const float2 *p) {
+__device__ __forceinline__ Quad2 ld_quad_own(const float2 *slab, int idx, const Chk &ck) {
   Quad2 q;
+  if (!chk<4, CHK_OWN>(ck, slab, idx)) {
+#pragma unroll
+    for (int s = 0; s < 4; ++s) q.s[s] = make_float2(0.f, 0.f);
+    return q;
+  }
+  const float2 *p = slab + idx;
   asm volatile("ld.global.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
                : "=f"(q.s[0].x), "=f"(q.s[0].y), "=f"(q.s[1].x), "=f"(q.s[1].y), "=f"(q.s[2].x), "=f"(q.s[2].y),
                  "=f"(q.s[3].x), "=f"(q.s[3].y)
@@ -442,16 +557,18 @@ __device__ __forceinline__ Quad2 ld_quad_own(const float2 *p) {
                : "memory");
   return q;
 }
-__device__ __forceinline__ void st_quad(float2 *p, const float2 n[4]) {
+__device__ __forceinline__ void st_quad(float2 *slab, int idx, const float2 n[4], const Chk &ck) {
+  if (!chk<4, CHK_WRITE>(ck, slab, idx)) return;
+  float2 *p = slab + idx;
   asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "f"(n[0].x), "f"(n[0].y), "f"(n[1].x),
                "f"(n[1].y), "f"(n[2].x), "f"(n[2].y), "f"(n[3].x), "f"(n[3].y)
                : "memory");
 }
 // Per-site links at base + i + s + sh[s], s = 0..3.
-__device__ __forceinline__ Quad2 ld_shifted(const float2 *base, int i, const int sh[4]) {
+__device__ __forceinline__ Quad2 ld_shifted(const float2 *base, int i, const int sh[4], const Chk &ck) {
   Quad2 q;
 #pragma unroll
-  for (int s = 0; s < 4; ++s) q.s[s] = __ldg(base + i + s + sh[s]);
+  for (int s = 0; s < 4; ++s) q.s[s] = ld1(base, i + s + sh[s], ck);
   return q;
 }
 
@@ -482,6 +599,7 @@ __device__ __forceinline__ void update_quad_body(const UpdArgs a, int i, float2 
   const int V = a.g.V, Vh = a.g.Vh;
   const float2 *lat = a.lat;
   const float2 *Lq_mu = lat + MU * V + q * Vh;
+  const Chk ck = make_chk(a);
   float2 ss[4], st[4], mA[4], mD[4];  // mA, mD: measurement sums (MEAS), see update_single_body
 #pragma unroll
   for (int s = 0; s < 4; ++s) ss[s] = st[s] = mA[s] = mD[s] = make_float2(0.f, 0.f);
@@ -491,25 +609,25 @@ __device__ __forceinline__ void update_quad_body(const UpdArgs a, int i, float2 
     const float2 *Lp_nu = lat + nu * V + a.p * Vh;
     const float2 *Lq_nu = lat + nu * V + q * Vh;
     Quad2 A, B, C, Dd, E, F;
-    C = ld_quad(Lp_nu, i);
+    C = ld_quad(Lp_nu, i, ck);
     if (MU == 0) {  // nu != 0: steps along nu shared, along x0 per site
-      A = ld_shifted(Lq_nu, i, f0);
-      B = ld_quad(Lq_mu, i + fwd[nu]);
-      Dd = ld_shifted(Lp_nu, i + bwd[nu], f0);
-      E = ld_quad(Lq_mu, i + bwd[nu]);
-      F = ld_quad(Lq_nu, i + bwd[nu]);
+      A = ld_shifted(Lq_nu, i, f0, ck);
+      B = ld_quad(Lq_mu, i + fwd[nu], ck);
+      Dd = ld_shifted(Lp_nu, i + bwd[nu], f0, ck);
+      E = ld_quad(Lq_mu, i + bwd[nu], ck);
+      F = ld_quad(Lq_nu, i + bwd[nu], ck);
     } else if (nu == 0) {  // MU != 0
-      A = ld_quad(Lq_nu, i + fwd[MU]);
-      B = ld_shifted(Lq_mu, i, f0);
-      Dd = ld_shifted(Lp_nu, i + fwd[MU], b0);
-      E = ld_shifted(Lq_mu, i, b0);
-      F = ld_shifted(Lq_nu, i, b0);
+      A = ld_quad(Lq_nu, i + fwd[MU], ck);
+      B = ld_shifted(Lq_mu, i, f0, ck);
+      Dd = ld_shifted(Lp_nu, i + fwd[MU], b0, ck);
+      E = ld_shifted(Lq_mu, i, b0, ck);
+      F = ld_shifted(Lq_nu, i, b0, ck);
     } else {  // MU != 0, nu != 0: every load 256-bit
-      A = ld_quad(Lq_nu, i + fwd[MU]);
-      B = ld_quad(Lq_mu, i + fwd[nu]);
-      Dd = ld_quad(Lp_nu, i + fwd[MU] + bwd[nu]);
-      E = ld_quad(Lq_mu, i + bwd[nu]);
-      F = ld_quad(Lq_nu, i + bwd[nu]);
+      A = ld_quad(Lq_nu, i + fwd[MU], ck);
+      B = ld_quad(Lq_mu, i + fwd[nu], ck);
+      Dd = ld_quad(Lp_nu, i + fwd[MU] + bwd[nu], ck);
+      E = ld_quad(Lq_mu, i + bwd[nu], ck);
+      F = ld_quad(Lq_nu, i + bwd[nu], ck);
     }
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
@@ -525,8 +643,8 @@ __device__ __forceinline__ void update_quad_body(const UpdArgs a, int i, float2 
       }
     }
   }
-  float2 *own = a.lat + MU * V + a.p * Vh + i;
-  const Quad2 U = ld_quad_own(own);
+  float2 *own_slab = a.lat + MU * V + a.p * Vh;
+  const Quad2 U = ld_quad_own(own_slab, i, ck);
   // sites i, i+1 and i+2, i+3 share one Philox block each
   Philox4 blk0, blk1;
   if (MET && SRC != SRC_REPLAY) {
@@ -539,7 +657,7 @@ __device__ __forceinline__ void update_quad_body(const UpdArgs a, int i, float2 
   for (int s = 0; s < 4; ++s)
     N[s] = update_one<D, MU, MET, SRC>(a, i + s, cweigh(ss[s], a.c.w_ss, st[s], a.c.w_st), U.s[s],
                                        s < 2 ? &blk0 : &blk1);
-  st_quad(own, N);
+  st_quad(own_slab, i, N, ck);
   pdl_release_dependents();
   if (MEAS) {
     float re = 8.f * MU, im = 0.f;
