@@ -40,6 +40,7 @@ DIMS = 4
 METRIC = "link-updates/s at 32^4 (1 Metropolis + 4 OR per sweep)"
 UNIT = "link-updates/s"
 CLOCK_WINDOW_S = 1.5
+HBM_WARM_S = 0.5  # minimum warm-up of each lattice beyond L2
 E2E_CHAINS = 3  # chains in flight in the end-to-end leg
 
 
@@ -279,11 +280,14 @@ def run_reference(args) -> None:
 
 
 # ------------------------------------------------------------------ our arm
-def hbm_resident_line(ctx, L: int, steps: int, warmup: int, flush, peak: float) -> dict:
+def hbm_resident_line(ctx, L: int, steps: int, warmup: int, flush, peak: float, gpu: str) -> dict:
     """The measured step (1 Metropolis + 4 OR + measurement) on an L^4
     lattice larger than L2, tuned as the headline lattice: device time per
     step (CUDA events, L2 flushed between steps), link-updates/s and the
-    update kernel's algorithmic bandwidth against the measured HBM peak."""
+    update kernel's algorithmic bandwidth against the measured HBM peak.
+    Warm-up runs for at least HBM_WARM_S of steps (clock ramp after the
+    lighter work before it); the clocks are sampled over the timed steps and
+    CLOCK_WINDOW_S more of the same step."""
     import torch
 
     from latticeu1_b200 import Lattice, Rng
@@ -295,16 +299,29 @@ def hbm_resident_line(ctx, L: int, steps: int, warmup: int, flush, peak: float) 
     obs = torch.zeros(6, dtype=torch.float64, device="cuda")
     with torch.cuda.stream(stream):
         lat.hot_start(rng)
-        for _ in range(warmup):
+        t0, n = time.perf_counter(), 0
+        while n < warmup or time.perf_counter() - t0 < HBM_WARM_S:
             flush.zero_()
             lat.update_measure(rng, METROP, OVRN, obs.data_ptr())
+            n += 1
+            if n % 20 == 0:
+                stream.synchronize()
         ev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(steps)]
+        clocks = ClockSampler(gpu)
+        clocks.start()
         for k in range(steps):
             flush.zero_()
             ev[k][0].record(stream)
             lat.update_measure(rng, METROP, OVRN, obs.data_ptr())
             ev[k][1].record(stream)
         torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        while time.perf_counter() - t1 < CLOCK_WINDOW_S:
+            for _ in range(10):
+                flush.zero_()
+                lat.update_measure(rng, METROP, OVRN, obs.data_ptr())
+            stream.synchronize()
+        clk = clocks.stop()
     ms = sum(e[0].elapsed_time(e[1]) for e in ev) / steps
     launches = 2 * DIMS * (METROP + OVRN)
     alg = algorithmic_bytes_per_link_update(DIMS) * volume(N) // 2
@@ -312,10 +329,36 @@ def hbm_resident_line(ctx, L: int, steps: int, warmup: int, flush, peak: float) 
     line = {"lattice": geom_name(N), "link_bytes": lat.nlinks * 8, "ms_per_step": ms,
             "value": link_updates_per_step(N) / (ms * 1e-3), "unit": UNIT, "achieved_gbs": achieved,
             "frac": achieved / peak, "update_variant": Lattice.VARIANTS.get(lat.variant, str(lat.variant)),
-            "update_block": lat.block, "steps": steps}
+            "update_block": lat.block, "steps": steps, "warmup_steps": n, "clocks": clk}
     lat.close()
     rng.close()
     return line
+
+
+def pcie_both_gbs(nbytes: int, reps: int = 10) -> float:
+    """Pinned host <-> device copy bandwidth per direction with both
+    directions busy at once (one H2D and one D2H of `nbytes` on two streams),
+    in GB/s: the ceiling of the end-to-end leg, which moves one
+    configuration each way per step."""
+    import torch
+    n = nbytes // 8
+    h = [torch.empty(n, dtype=torch.float64, pin_memory=True) for _ in range(2)]
+    d = [torch.empty(n, dtype=torch.float64, device="cuda") for _ in range(2)]
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def both():
+        with torch.cuda.stream(s1):
+            d[0].copy_(h[0], non_blocking=True)
+        with torch.cuda.stream(s2):
+            h[1].copy_(d[1], non_blocking=True)
+
+    both()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        both()
+    torch.cuda.synchronize()
+    return nbytes * reps / (time.perf_counter() - t0) / 1e9
 
 
 def e2e_rate(ctx, lat, rng, stream, N, beta, aniso, args, rank, world):
@@ -470,6 +513,7 @@ def run_ours(args) -> None:
     else:
         e2e_value, e2e_steps, e2e_obs_ok = e2e_rate(ctx, lat, rng, stream, N, beta, aniso, args, rank, world)
     bytes_cfg = lat.nlinks * 8
+    pcie_gbs = None if e2e_value is None else pcie_both_gbs(bytes_cfg)
 
     ob = obs[args.warmup:].cpu().numpy()
     per_chain = replicas.gather_observables([float(ob[:, 0].mean()), float(ob[:, 2].mean())])
@@ -503,6 +547,11 @@ def run_ours(args) -> None:
             "e2e": None if e2e_value is None else {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_cfg,
                     "d2h_bytes_per_step": bytes_cfg + 48, "steps": e2e_steps, "chains_in_flight": E2E_CHAINS,
                     "observables_finite": e2e_obs_ok,
+                    # each step moves one configuration each way: at most one step per
+                    # bytes_cfg / (per-direction bandwidth with both directions busy)
+                    "roofline": {"bound": "pcie", "pcie_gbs_per_direction": pcie_gbs,
+                                 "bound_value": world * lu * pcie_gbs * 1e9 / bytes_cfg,
+                                 "frac": e2e_value / (world * lu * pcie_gbs * 1e9 / bytes_cfg)},
                     "path": "per step, one of three chains (own stream, own pinned host FP64 configuration): "
                             "u1_lattice_import_angles_async + u1_update_measure + D2H of the 6 observables + "
                             "u1_lattice_export_angles_async; host wall clock from a synchronised start to "
@@ -519,7 +568,8 @@ def run_ours(args) -> None:
                             "per_chain_plaq_ss_st": per_chain},
         }
         if world == 1 and args.hbm_check and args.delta == 0.0 and args.nhits == 1:
-            hb = [hbm_resident_line(ctx, L, max(10, min(args.steps, 20)), max(10, args.warmup), flush, peak)
+            gpu_id = ("GPU-" + uuid) if uuid and not uuid.startswith("GPU-") else (uuid or str(local))
+            hb = [hbm_resident_line(ctx, L, max(10, min(args.steps, 20)), max(10, args.warmup), flush, peak, gpu_id)
                   for L in args.hbm_check]
             line["hbm_resident"] = {"lattices": hb, "note": "the same measured step on lattices beyond the "
                                                             "126 MB L2, each tuned on its first update"}
