@@ -12,8 +12,9 @@ phase-dependency check.
   passes; an odd extent, which u1_geom_validate refuses, is shown to break
   the decomposition.
 * checked build (GPU, child process with U1_CHECKED=1): every update
-  variant, the batched kernels, the measuring phases, windowed Metropolis
-  and multilevel sub-updates run with bounds, alignment and race checks on
+  variant, the batched kernels, the measuring phases, windowed Metropolis,
+  multilevel sub-updates and full-size four-site phases (32^4 in one wave,
+  40^4 in several) run with bounds, alignment and race checks on
   every link access; no violation and no race may occur, the phase count
   must match the phases launched, and the links and measurements must be
   bit-identical to the normal build's.  The checker itself is exercised by
@@ -183,6 +184,21 @@ def run_workload(out: Path) -> dict:
             res[f"links_{gi}_{v}"] = lat.export_angles()
             lat.close()
             rng.close()
+    # full-size four-site phases: 32^4 (one wave, SM-local block order) and
+    # 40^4 (several waves, launch order)
+    for L in (32, 40):
+        lat = Lattice(ctx, 4, (L,) * 4, 1.0)
+        lat.set_variant(5)
+        lat.set_block(128)
+        rng = Rng(ctx, 11)
+        lat.hot_start(rng)
+        lat.update_measure(rng, 1, 4, meas.data_ptr())
+        phases["lattice"] += 2 * 4 * 5
+        torch.cuda.synchronize()
+        res[f"meas_{L}"] = meas.cpu().numpy().copy()
+        res[f"links_{L}"] = lat.export_angles()
+        lat.close()
+        rng.close()
     report = {"lattice": None}
     if _lib.CHECKED:
         report["lattice"] = _lib.check_report(ctx.handle, reset=True)
