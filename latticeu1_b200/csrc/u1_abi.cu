@@ -693,12 +693,6 @@ static int launch_phase(const UpdArgs &a, cudaStream_t s, bool met, int src, int
   return fail(U1_ERR_INVALID, "k_update: direction out of range");
 }
 
-// SM count for the block-order remap of the four-site phase kernels
-// (sm_local_block) when a phase's grid runs as a single wave, else 0 (launch
-// order).  Over several waves the remap hands each SM a distant slice of the
-// lattice, so a plane and its neighbour planes are loaded many waves apart
-// and miss in L2 (measured at 64^4: 1.5x the algorithmic DRAM reads, L2 hit
-// rate 22 %).  U1_REMAP=0 in the environment keeps the launch order always.
 // Whether a four-site phase at the lattice's block size runs as a single
 // wave (the SM-local block order then applies); cached per block size.
 static void quad_layout(u1_lattice *lat) {
@@ -714,6 +708,25 @@ static void quad_layout(u1_lattice *lat) {
   lat->remap_block = lat->block;
 }
 
+// Whether consecutive phases alternate their block order (rev_block): for a
+// lattice whose links exceed half the L2, each phase then starts on the
+// links the previous one left in L2.  U1_ALTERNATE=0 in the environment keeps
+// the launch order.
+static bool alternate_order(const u1_lattice *lat) {
+  static const bool off = [] {
+    const char *r = std::getenv("U1_ALTERNATE");
+    return r && r[0] == '0';
+  }();
+  const size_t bytes = (size_t)lat->g.V * lat->g.dims * sizeof(float2);
+  return !off && 2 * bytes > (size_t)lat->ctx->prop.l2CacheSize;
+}
+
+// SM count for the block-order remap of the four-site phase kernels
+// (sm_local_block) when a phase's grid runs as a single wave, else 0 (launch
+// order).  Over several waves the remap hands each SM a distant slice of the
+// lattice, so a plane and its neighbour planes are loaded many waves apart
+// and miss in L2 (measured at 64^4: 1.5x the algorithmic DRAM reads, L2 hit
+// rate 22 %).  U1_REMAP=0 in the environment keeps the launch order always.
 static int sm_remap(u1_lattice *lat) {
   static const bool off = [] {
     const char *r = std::getenv("U1_REMAP");
@@ -952,6 +965,7 @@ static int issue_sweep(u1_lattice *lat, float2 *links, u1_rng *rng, int metrop, 
   // with a freeze period the SM-local order would hand whole frozen slabs to
   // some SMs and none to others (measured 4 % slower multilevel): keep the launch order
   a.sms = ml ? 0 : sm_remap(lat);
+  const bool alternate = a.sms == 0 && alternate_order(lat);
   const int src = metropolis_src(lat, rng);
   const int var = sweep_variant(lat, src, ml);
   if (var == U1V_WAVE) return launch_wave(lat, links, rng, metrop, ovrn, meas_partials);
@@ -960,6 +974,7 @@ static int issue_sweep(u1_lattice *lat, float2 *links, u1_rng *rng, int metrop, 
   int phase = 0;
   auto launch = [&](bool met) -> int {
     ++phase;
+    a.rev = (alternate && (phase & 1) == 0) ? 1 : 0;  // every second phase runs its blocks backwards
     int rc;
     // the last pass is phases total-2D+1 .. total; its parity-1 half with mu >= 1 measures
     if (meas_partials && phase > total - 2 * D && a.p == 1 && a.mu >= 1)

@@ -21,33 +21,36 @@ template <int D, int MU, bool MET, int SRC = SRC_PHILOX>
 static __global__ void __launch_bounds__(256, 8) k_update_pair_meas(const UpdArgs a, double *partials) {
   __shared__ double smem[kRedWarps * 2];
   float2 m = make_float2(0.f, 0.f);
-  update_pair_body<D, MU, MET, SRC, true>(a, 2 * (blockIdx.x * blockDim.x + threadIdx.x), &m);
+  const int b = rev_block(a, (int)blockIdx.x, (int)gridDim.x);
+  update_pair_body<D, MU, MET, SRC, true>(a, 2 * (b * (int)blockDim.x + (int)threadIdx.x), &m);
   double v[2] = {(double)m.x, (double)m.y};
   block_sum<2>(v, smem);
-  if (threadIdx.x < 2) partials[2 * blockIdx.x + threadIdx.x] = v[0];
+  if (threadIdx.x < 2) partials[2 * b + threadIdx.x] = v[0];  // slot of the work item: any block order sums alike
 }
 
 template <int D, int MU, bool MET, int SRC = SRC_PHILOX>
 static __global__ void __launch_bounds__(256) k_update_meas(const UpdArgs a, double *partials) {
   __shared__ double smem[kRedWarps * 2];
   float2 m = make_float2(0.f, 0.f);
-  update_single_body<D, MU, MET, SRC, true>(a, blockIdx.x * blockDim.x + threadIdx.x, &m);
+  const int b = rev_block(a, (int)blockIdx.x, (int)gridDim.x);
+  update_single_body<D, MU, MET, SRC, true>(a, b * (int)blockDim.x + (int)threadIdx.x, &m);
   double v[2] = {(double)m.x, (double)m.y};
   block_sum<2>(v, smem);
-  if (threadIdx.x < 2) partials[2 * blockIdx.x + threadIdx.x] = v[0];
+  if (threadIdx.x < 2) partials[2 * b + threadIdx.x] = v[0];  // slot of the work item: any block order sums alike
 }
 
-// Four sites per thread, 128 threads (512 sites) per block: the same blocks
-// and partial slots as k_update_pair_meas.
+// Four sites per thread, 128 threads (512 sites) per block: the same work
+// items and partial slots as k_update_pair_meas.
 template <int D, int MU, bool MET, int SRC = SRC_PHILOX>
 static __global__ void __launch_bounds__(128, 7) k_update_quad_meas(const UpdArgs a, double *partials) {
   __shared__ double smem[kRedWarps * 2];
   float2 m = make_float2(0.f, 0.f);
-  const int b = sm_local_block((int)blockIdx.x, (int)gridDim.x, a.sms);
+  const int b = a.rev ? rev_block(a, (int)blockIdx.x, (int)gridDim.x)
+                      : sm_local_block((int)blockIdx.x, (int)gridDim.x, a.sms);
   update_quad_body<D, MU, MET, SRC, true>(a, 4 * (b * (int)blockDim.x + (int)threadIdx.x), &m);
   double v[2] = {(double)m.x, (double)m.y};
   block_sum<2>(v, smem);
-  if (threadIdx.x < 2) partials[2 * blockIdx.x + threadIdx.x] = v[0];
+  if (threadIdx.x < 2) partials[2 * b + threadIdx.x] = v[0];  // slot of the work item: any block order sums alike
 }
 
 // Blocks of one measuring phase (pair kernels when N0/2 is even).

@@ -110,6 +110,7 @@ struct UpdArgs {
   float win;                           // SRC_WINDOW: proposal half-width / pi (0: whole circle)
   int nhits;                           // SRC_WINDOW: Metropolis hits per link and pass
   int sms;                             // k_update_quad: > 0 remaps the block order over this many SMs
+  int rev;                             // != 0: blocks take their work in reverse launch order (see rev_block)
 #ifdef U1_BOUNDS_CHECK
   struct ChkState *chk;                // checked build: violation counters (see Chk below)
   unsigned *shadow;                    // checked build: per-link marks of this phase (nullptr: no race marks)
@@ -218,6 +219,14 @@ __device__ __forceinline__ int sm_local_block(int b, int G, int S) {
   const int s = b % S, r = b / S;
   return s * q + min(s, rem) + r;
 }
+
+// Work item of block b of G in a phase with a.rev set: the last one first.
+// A lattice larger than L2 streams every link through it in each phase;
+// consecutive phases read 7 of the same 8 (direction, parity) halves, so
+// when they alternate direction each phase starts on the links the previous
+// one left in L2 instead of on the ones it evicted first.  The links are
+// the same in any block order.
+__device__ __forceinline__ int rev_block(const UpdArgs &a, int b, int G) { return a.rev ? G - 1 - b : b; }
 
 // Where a Metropolis kernel takes its proposals from.
 enum : int {
@@ -677,7 +686,8 @@ __device__ __forceinline__ void update_quad_body(const UpdArgs a, int i, float2 
 // of 72, so 7 CTAs fit an SM (a 32^4 phase, 1024 CTAs, is then a single wave).
 template <int D, int MU, bool MET, int SRC>
 __global__ void __launch_bounds__(128, 7) k_update_quad(const UpdArgs a) {
-  const int b = sm_local_block((int)blockIdx.x, (int)gridDim.x, a.sms);
+  const int b = a.rev ? rev_block(a, (int)blockIdx.x, (int)gridDim.x)
+                      : sm_local_block((int)blockIdx.x, (int)gridDim.x, a.sms);
   update_quad_body<D, MU, MET, SRC>(a, 4 * (b * (int)blockDim.x + (int)threadIdx.x));
 }
 
@@ -685,19 +695,22 @@ __global__ void __launch_bounds__(128, 7) k_update_quad(const UpdArgs a) {
 // threads fit an SM (a 32^4 phase is then a single wave).
 template <int D, int MU, bool MET, int SRC>
 __global__ void __launch_bounds__(256, 8) k_update_pair(const UpdArgs a) {
-  update_pair_body<D, MU, MET, SRC>(a, 2 * (blockIdx.x * blockDim.x + threadIdx.x));
+  const int b = rev_block(a, (int)blockIdx.x, (int)gridDim.x);
+  update_pair_body<D, MU, MET, SRC>(a, 2 * (b * (int)blockDim.x + (int)threadIdx.x));
 }
 
 // The same with no register cap (fewer CTAs per SM, no spills).
 template <int D, int MU, bool MET, int SRC>
 __global__ void __launch_bounds__(256) k_update_pair_free(const UpdArgs a) {
-  update_pair_body<D, MU, MET, SRC>(a, 2 * (blockIdx.x * blockDim.x + threadIdx.x));
+  const int b = rev_block(a, (int)blockIdx.x, (int)gridDim.x);
+  update_pair_body<D, MU, MET, SRC>(a, 2 * (b * (int)blockDim.x + (int)threadIdx.x));
 }
 
 // One site per thread (any geometry, N0/2 odd included).
 template <int D, int MU, bool MET, int SRC>
 __global__ void __launch_bounds__(256) k_update(const UpdArgs a) {
-  update_single_body<D, MU, MET, SRC>(a, blockIdx.x * blockDim.x + threadIdx.x);
+  const int b = rev_block(a, (int)blockIdx.x, (int)gridDim.x);
+  update_single_body<D, MU, MET, SRC>(a, b * (int)blockDim.x + (int)threadIdx.x);
 }
 
 // Hot start (reference src/update.cu:30-48): every link gets
