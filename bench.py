@@ -148,16 +148,24 @@ KERNEL_OF_VARIANT = {1: "k_update_pair", 2: "k_update_pair_free", 3: "k_update",
                      5: "k_update_quad"}
 
 
-def ncu_batch_traffic_per_link_sweep():
+def ncu_batch_traffic_per_link_sweep(group_mb: int, lanes: int) -> tuple[float | None, str]:
     """DRAM bytes per link and sweep of the grouped batch from the committed
-    ncu summary, if any."""
+    ncu summary, and a note; None when there is no summary or it was measured
+    on another layout (group size, lanes)."""
     p = ROOT / "profiles" / "k_batch_update_512chains.md"
     if not p.exists():
-        return None
+        return None, "no committed ncu summary"
+    fields = {}
     for line in p.read_text().splitlines():
-        if line.startswith("dram_bytes_per_link_sweep:"):
-            return float(line.split(":", 1)[1].split()[0])
-    return None
+        if ":" in line and line.split(":", 1)[0] in ("dram_bytes_per_link_sweep", "layout_group_mb", "layout_lanes"):
+            k, v = line.split(":", 1)
+            fields[k] = float(v.split()[0])
+    if "dram_bytes_per_link_sweep" not in fields:
+        return None, "no committed ncu summary"
+    if (fields.get("layout_group_mb"), fields.get("layout_lanes", 1.0)) != (float(group_mb), float(lanes)):
+        return None, (f"the committed ncu summary was made with {fields.get('layout_group_mb'):.0f} MiB groups on "
+                      f"{fields.get('layout_lanes', 1.0):.0f} lane(s); this run uses {group_mb} MiB on {lanes}")
+    return fields["dram_bytes_per_link_sweep"], "ncu, profiles/k_batch_update_512chains.md"
 
 
 # Sources the update kernels compile from: a committed ncu figure counts only
@@ -698,7 +706,7 @@ def run_batched(args) -> None:
     alg_bytes = algorithmic_bytes_per_link_update(DIMS) * links // (2 * DIMS)
     achieved = alg_bytes / avg_launch_s / 1e9
     peak, peak_kind = measured_peak()
-    per_link = ncu_batch_traffic_per_link_sweep()
+    per_link, traffic_note = ncu_batch_traffic_per_link_sweep(group_mb, b.lanes)
     traffic = per_link * links / phases if per_link is not None else None
 
     # comparator: the same chains one at a time through the single-lattice API
@@ -742,10 +750,11 @@ def run_batched(args) -> None:
                    "l2": "flushed between timed steps (512 MiB device write)"},
         "roofline": {"bound": "hbm", "kernel": "k_batch_update (one (parity,mu) phase over all chains)",
                      "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes,
+                     "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_note,
+                     "algorithmic_bytes_per_launch": alg_bytes,
                      "avg_launch_us": avg_launch_s * 1e6},
         "update_only_ms_per_step": upd_ms / args.steps,
-        "tuned": {"group_mb": group_mb, "groups": len(layout), "seconds": t_tune,
+        "tuned": {"group_mb": group_mb, "lanes": b.lanes, "groups": len(layout), "seconds": t_tune,
                   "kernels": {f"{Batch.VARIANTS.get(v, v)}@{t}": sum(1 for g in layout if (g[2], g[3]) == (v, t))
                               for v, t in sorted({(g[2], g[3]) for g in layout})}},
         "gpu_launches": int(launches),

@@ -283,13 +283,14 @@ int u1_batch_info(const u1_batch *b, int64_t out[4]);
 /* Number of chain groups a sweep runs one after another (consecutive chains
  * whose links fit comfortably in L2, so that each group's sweep after its
  * first phase is served from L2).  The result is the same as one group.
- * The untuned group size is U1_BATCH_GROUP_MB MiB (default 64; 0: one
+ * The untuned group size is U1_BATCH_GROUP_MB MiB (default 32; 0: one
  * group), read at u1_batch_create. */
 int u1_batch_groups(const u1_batch *b, int *groups);
 /* Autotuner of the batch (replaces the reference's per-kernel block-size
  * search, src/tune.cpp:306-416, for many chains per launch): the group size
- * (32 ... 96 MiB of links) and, per group, the update kernel (four, two or
- * one site per thread) and threads per block, timed as graph-replayed sweeps
+ * (32 ... 96 MiB of links) and the lanes (below), then, per group, the update
+ * kernel (four, two or one site per thread) and threads per block, timed as
+ * graph-replayed sweeps
  * from a backed-up state (links and pass counter restored).  Every choice
  * gives the same links bit for bit.  Cached per (device, dims, chain
  * extents) in memory and in $U1_RESOURCE_PATH/u1b200_batch_tunecache.tsv;
@@ -306,6 +307,14 @@ int u1_batch_tune(u1_batch *b, int *group_mb);
 int u1_batch_configure(u1_batch *b, int group_mb, int ngroups, const int *variants, const int *threads);
 /* Group `group`: out = {first chain, end chain, variant, threads per block}. */
 int u1_batch_group_info(const u1_batch *b, int group, int out[4]);
+/* Lanes of a sweep (no counterpart in the reference): 1 sweeps the groups
+ * one after another on the batch's stream; 2 (the default, U1_BATCH_LANES=1
+ * at u1_batch_create for one) alternates them between that stream and a
+ * second one forked from and joined back into it within the sweep, so one
+ * group's phase boundaries overlap another group's phases.  The links are
+ * the same either way; the tuner picks the count. */
+int u1_batch_set_lanes(u1_batch *b, int lanes);
+int u1_batch_get_lanes(const u1_batch *b, int *lanes);
 /* Hot start of every chain (as u1_hot_start); advances the pass counter by 1. */
 int u1_batch_hot_start(u1_batch *b);
 /* One sweep of every chain: metrop Metropolis then ovrn overrelaxation

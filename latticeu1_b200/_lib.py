@@ -95,6 +95,8 @@ SIGNATURES = {
     "u1_batch_tune": [_vp, C.POINTER(_i)],
     "u1_batch_configure": [_vp, _i, _i, C.POINTER(_i), C.POINTER(_i)],
     "u1_batch_group_info": [_vp, _i, C.POINTER(_i)],
+    "u1_batch_set_lanes": [_vp, _i],
+    "u1_batch_get_lanes": [_vp, C.POINTER(_i)],
     "u1_batch_hot_start": [_vp],
     "u1_batch_update": [_vp, _i, _i, _i],
     "u1_batch_measure": [_vp, _dp],

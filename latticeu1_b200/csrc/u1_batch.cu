@@ -201,7 +201,14 @@ struct u1_batch {
   // links are served from L2; each group runs its own kernel variant and
   // block size (u1_batch_tune).
   std::vector<BatchGroup> groups;
-  size_t group_bytes = 64ull << 20;       // group size limit the groups were cut with
+  size_t group_bytes = 32ull << 20;       // group size limit the groups were cut with
+  // Lanes: with 2, consecutive groups alternate between the batch's stream
+  // and a second one inside each sweep, so one group's phase boundaries
+  // (drain, launch, refill) overlap another group's phases.  Groups are
+  // independent chains: the links are the same with one lane or two.
+  int lanes = 2;
+  cudaStream_t lane_stream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool quad_enabled = true;               // four-site kernels allowed (U1_BATCH_QUAD=0: no)
   float2 *backup = nullptr;               // link backup while tuning
   unsigned *shadow = nullptr;              // checked build: per-link access marks (total_links words)
@@ -320,6 +327,9 @@ extern "C" int u1_batch_destroy(u1_batch *b) {
   u1i::dev_free(b->d_out);
   u1i::dev_free(b->pass_dev);
   u1i::dev_free(b->shadow);
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+  if (b->ev_join) cudaEventDestroy(b->ev_join);
+  if (b->lane_stream) cudaStreamDestroy(b->lane_stream);
   if (b->h_out) cudaFreeHost(b->h_out);
   if (b->own_stream) cudaStreamDestroy(b->own_stream);
   delete b;
@@ -384,17 +394,22 @@ extern "C" int u1_batch_create(u1_ctx *ctx, int nchains, const u1_geom *geoms, u
   b->total_links = off;
   b->nb_site = (int)tab_site.size();
   b->nb_meas = (int)tab_meas.size();
-  // groups of at most U1_BATCH_GROUP_MB (default 64) MiB of links; a single
+  // groups of at most U1_BATCH_GROUP_MB (default 32) MiB of links; a single
   // chain may exceed it; 0 puts every chain in one group
   if (const char *env = std::getenv("U1_BATCH_GROUP_MB")) {
     const long long mb = std::atoll(env);
     b->group_bytes = mb > 0 ? (size_t)mb << 20 : SIZE_MAX;
   }
+  // U1_BATCH_LANES=1 sweeps the groups one after another on one stream
+  if (const char *env = std::getenv("U1_BATCH_LANES")) b->lanes = std::atoi(env) == 1 ? 1 : 2;
   // U1_BATCH_QUAD=0 keeps every group on the two-site (or one-site) kernel
   const char *qenv = std::getenv("U1_BATCH_QUAD");
   b->quad_enabled = !(qenv && qenv[0] == '0');
   cudaError_t e = cudaStreamCreate(&b->own_stream);
   b->stream = ctx->stream ? ctx->stream : b->own_stream;
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->lane_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming);
   if (e == cudaSuccess) e = u1i::dev_alloc(&b->links, b->total_links * sizeof(float2));
   if (e == cudaSuccess) e = u1i::dev_alloc(&b->d_chains, sizeof(BatchChain) * nchains);
   if (e == cudaSuccess) e = u1i::dev_alloc(&b->d_tab_site, sizeof(int) * tab_site.size());
@@ -481,13 +496,13 @@ extern "C" int u1_batch_hot_start(u1_batch *b) {
 }
 
 template <int D, int MU, bool MET>
-static int batch_launch_quad(u1_batch *b, BatchPhase ph, int group) {
+static int batch_launch_quad(u1_batch *b, BatchPhase ph, int group, cudaStream_t s) {
   const BatchGroup &gr = b->groups[group];
   ph.block_base = gr.first_block;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)gr.nblocks);
   cfg.blockDim = dim3((unsigned)gr.threads);
-  cfg.stream = b->stream;
+  cfg.stream = s;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[0].val.programmaticStreamSerializationAllowed = 1;
@@ -501,13 +516,13 @@ static int batch_launch_quad(u1_batch *b, BatchPhase ph, int group) {
 }
 
 template <int D, int MU, bool MET, bool PAIR>
-static int batch_launch(u1_batch *b, BatchPhase ph, int group) {
+static int batch_launch(u1_batch *b, BatchPhase ph, int group, cudaStream_t s) {
   const BatchGroup &gr = b->groups[group];
   ph.block_base = gr.first_block;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)gr.nblocks);
   cfg.blockDim = dim3((unsigned)gr.threads);
-  cfg.stream = b->stream;
+  cfg.stream = s;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[0].val.programmaticStreamSerializationAllowed = 1;
@@ -521,25 +536,25 @@ static int batch_launch(u1_batch *b, BatchPhase ph, int group) {
 }
 
 template <int D, int MU>
-static int batch_launch_mu(u1_batch *b, const BatchPhase &ph, bool met, int group) {
+static int batch_launch_mu(u1_batch *b, const BatchPhase &ph, bool met, int group, cudaStream_t s) {
   const int v = b->groups[group].variant;
   if (v == U1V_QUAD)
-    return met ? batch_launch_quad<D, MU, true>(b, ph, group) : batch_launch_quad<D, MU, false>(b, ph, group);
+    return met ? batch_launch_quad<D, MU, true>(b, ph, group, s) : batch_launch_quad<D, MU, false>(b, ph, group, s);
   if (v == U1V_PAIR32)
-    return met ? batch_launch<D, MU, true, true>(b, ph, group) : batch_launch<D, MU, false, true>(b, ph, group);
-  return met ? batch_launch<D, MU, true, false>(b, ph, group) : batch_launch<D, MU, false, false>(b, ph, group);
+    return met ? batch_launch<D, MU, true, true>(b, ph, group, s) : batch_launch<D, MU, false, true>(b, ph, group, s);
+  return met ? batch_launch<D, MU, true, false>(b, ph, group, s) : batch_launch<D, MU, false, false>(b, ph, group, s);
 }
 
 template <int D>
-static int batch_phase(u1_batch *b, const BatchPhase &ph, int mu, bool met, int group) {
+static int batch_phase(u1_batch *b, const BatchPhase &ph, int mu, bool met, int group, cudaStream_t s) {
   switch (mu) {
-    case 0: return batch_launch_mu<D, 0>(b, ph, met, group);
-    case 1: return batch_launch_mu<D, 1>(b, ph, met, group);
+    case 0: return batch_launch_mu<D, 0>(b, ph, met, group, s);
+    case 1: return batch_launch_mu<D, 1>(b, ph, met, group, s);
     case 2:
-      if constexpr (D > 2) return batch_launch_mu<D, 2>(b, ph, met, group);
+      if constexpr (D > 2) return batch_launch_mu<D, 2>(b, ph, met, group, s);
       break;
     case 3:
-      if constexpr (D > 3) return batch_launch_mu<D, 3>(b, ph, met, group);
+      if constexpr (D > 3) return batch_launch_mu<D, 3>(b, ph, met, group, s);
       break;
   }
   return bfail(U1_ERR_INVALID, "batch phase: direction out of range");
@@ -562,6 +577,9 @@ static int batch_measure_issue(u1_batch *b) {
   }
 }
 
+// Whether a sweep of groups [g0, g1) runs on two lanes.
+static bool two_lanes(const u1_batch *b, int g0, int g1) { return b->lanes == 2 && g1 - g0 > 1; }
+
 // The sweep of groups [g0, g1) (all groups by default).
 static int batch_issue_sweep(u1_batch *b, int metrop, int ovrn, bool measure, int g0 = 0, int g1 = -1) {
   BatchPhase ph{};
@@ -575,17 +593,33 @@ static int batch_issue_sweep(u1_batch *b, int metrop, int ovrn, bool measure, in
 #endif
   const int D = b->dims;
   const int ngroups = g1 < 0 ? (int)b->groups.size() : g1;
-  // Each chain group runs the whole sweep before the next starts.  Every
-  // group's Metropolis phases read the same pass counter; the first
-  // overrelaxation kernel of the last group (after all of them) bumps it.
-  bool bumped = (metrop == 0);
+  // Each chain group runs the whole sweep before its lane's next group
+  // starts.  Every group's Metropolis phases read the same pass counter.  On
+  // one lane the first overrelaxation kernel of the last group (after all of
+  // them) bumps it; on two lanes (groups alternate between the batch's
+  // stream and the second lane, forked from and joined back into the batch's
+  // stream) a kernel after the join does.
+  const bool lanes2 = two_lanes(b, g0, ngroups);
+  bool bumped = (metrop == 0) || lanes2;
+  if (lanes2) {
+    U1_CUDA_TRY(cudaEventRecord(b->ev_fork, b->stream));
+    U1_CUDA_TRY(cudaStreamWaitEvent(b->lane_stream, b->ev_fork, 0));
+  }
   for (int grp = g0; grp < ngroups; ++grp) {
-    auto run = [&](int mu, bool met) {
-      int rc = D == 2 ? batch_phase<2>(b, ph, mu, met, grp)
-             : D == 3 ? batch_phase<3>(b, ph, mu, met, grp)
-                      : batch_phase<4>(b, ph, mu, met, grp);
+    const cudaStream_t s = (lanes2 && ((grp - g0) & 1)) ? b->lane_stream : b->stream;
 #ifdef U1_BOUNDS_CHECK
-      if (rc == U1_OK) rc = u1i::chk_phase_end(b->stream, ph.shadow, b->total_links, ph.chk);
+    // the group's own links (its chains are consecutive): the other lane's
+    // group marks its links concurrently
+    const BatchChain &first = b->h_chains[b->groups[grp].c0], &last = b->h_chains[b->groups[grp].c1 - 1];
+    const size_t g_off = (size_t)(first.links - b->links);
+    const size_t g_len = (size_t)(last.links - first.links) + (size_t)last.g.V * last.g.dims;
+#endif
+    auto run = [&](int mu, bool met) {
+      int rc = D == 2 ? batch_phase<2>(b, ph, mu, met, grp, s)
+             : D == 3 ? batch_phase<3>(b, ph, mu, met, grp, s)
+                      : batch_phase<4>(b, ph, mu, met, grp, s);
+#ifdef U1_BOUNDS_CHECK
+      if (rc == U1_OK) rc = u1i::chk_phase_end(s, ph.shadow + g_off, g_len, ph.chk);
 #endif
       return rc;
     };
@@ -611,7 +645,11 @@ static int batch_issue_sweep(u1_batch *b, int metrop, int ovrn, bool measure, in
           if (rc) return rc;
         }
   }
-  if (!bumped) {  // no overrelaxation kernel carried the pass-counter bump
+  if (lanes2) {
+    U1_CUDA_TRY(cudaEventRecord(b->ev_join, b->lane_stream));
+    U1_CUDA_TRY(cudaStreamWaitEvent(b->stream, b->ev_join, 0));
+  }
+  if (!bumped || (lanes2 && metrop > 0)) {  // no overrelaxation kernel carried the pass-counter bump
     k_pass_add<<<1, 1, 0, b->stream>>>(b->pass_dev, (unsigned long long)metrop);
     U1_LAUNCH_CHECK("k_pass_add");
   }
@@ -646,8 +684,9 @@ extern "C" int u1_batch_update(u1_batch *b, int metrop, int ovrn, int measure) {
     it = b->graphs.emplace(key, ex).first;
   }
   U1_CUDA_TRY(cudaGraphLaunch(it->second, b->stream));
+  const bool pass_kernel = metrop > 0 && (ovrn == 0 || two_lanes(b, 0, (int)b->groups.size()));
   u1i::g_launches += (unsigned long long)(2 * b->dims * (metrop + ovrn) * b->groups.size() + (measure ? 2 : 0) +
-                                          (ovrn == 0 && metrop > 0 ? 1 : 0));
+                                          (pass_kernel ? 1 : 0));
   b->pass += (uint64_t)metrop;
   return U1_OK;
 }
@@ -745,6 +784,7 @@ namespace {
 struct BatchTuneRec {
   size_t group_bytes;
   std::vector<std::pair<int, int>> choice;
+  int lanes = 1;
 };
 std::mutex g_btune_mu;
 bool g_btune_loaded = false;
@@ -769,6 +809,7 @@ std::string batch_tune_key(const u1_batch *b) {
 }
 
 // key <tab> group MiB <tab> variant:threads,... <tab> microseconds per sweep
+// <tab> lanes (absent in older files: one lane)
 void batch_tune_load_locked() {
   if (g_btune_loaded) return;
   g_btune_loaded = true;
@@ -779,10 +820,11 @@ void batch_tune_load_locked() {
   while (std::getline(in, line)) {
     if (line.empty() || line[0] == '#') continue;
     std::istringstream ls(line);
-    std::string key, mb, list;
+    std::string key, mb, list, us, lanes;
     if (!std::getline(ls, key, '\t') || !std::getline(ls, mb, '\t') || !std::getline(ls, list, '\t')) continue;
     BatchTuneRec rec;
     rec.group_bytes = (size_t)std::atoll(mb.c_str()) << 20;
+    if (std::getline(ls, us, '\t') && std::getline(ls, lanes, '\t')) rec.lanes = std::atoi(lanes.c_str()) == 2 ? 2 : 1;
     std::istringstream li(list);
     std::string item;
     while (std::getline(li, item, ',')) {
@@ -802,7 +844,7 @@ void batch_tune_save(const std::string &key, const BatchTuneRec &rec, double us)
   out << key << '\t' << (rec.group_bytes >> 20) << '\t';
   for (size_t k = 0; k < rec.choice.size(); ++k)
     out << (k ? "," : "") << rec.choice[k].first << ':' << rec.choice[k].second;
-  out << '\t' << us << '\n';
+  out << '\t' << us << '\t' << rec.lanes << '\n';
 }
 
 std::vector<std::pair<int, int>> current_choice(const u1_batch *b) {
@@ -843,8 +885,9 @@ static int batch_time_sweep(u1_batch *b, int g0, int g1, double *us, double warm
   if (e == cudaSuccess) e = r1 != cudaSuccess ? r1 : r2 != cudaSuccess ? r2 : r3;
   if (e != cudaSuccess) return cuda_fail(e, "u1_batch_tune: trial");
   if (u1i::tune_verbose())
-    std::fprintf(stderr, "u1_batch_tune: groups %d..%d of %d (%zu MiB groups): %.1f us per sweep\n", g0, g1 - 1,
-                 (int)b->groups.size(), b->group_bytes >> 20, *us);
+    std::fprintf(stderr, "u1_batch_tune: groups %d..%d of %d (%zu MiB groups, %d lane%s): %.1f us per sweep\n", g0,
+                 g1 - 1, (int)b->groups.size(), b->group_bytes >> 20, two_lanes(b, g0, g1) ? 2 : 1,
+                 two_lanes(b, g0, g1) ? "s" : "", *us);
   return U1_OK;
 }
 
@@ -854,7 +897,10 @@ static int batch_tune(u1_batch *b) {
     std::lock_guard<std::mutex> lock(g_btune_mu);
     batch_tune_load_locked();
     auto it = g_btune.find(key);
-    if (it != g_btune.end()) return batch_configure(b, it->second.group_bytes, it->second.choice);
+    if (it != g_btune.end()) {
+      b->lanes = it->second.lanes;
+      return batch_configure(b, it->second.group_bytes, it->second.choice);
+    }
   }
   if (!b->backup) U1_CUDA_TRY(u1i::dev_alloc(&b->backup, b->total_links * sizeof(float2)));
   U1_CUDA_TRY(cudaMemcpyAsync(b->backup, b->links, b->total_links * sizeof(float2), cudaMemcpyDeviceToDevice,
@@ -870,12 +916,15 @@ static int batch_tune(u1_batch *b) {
     for (size_t k = n; k-- > 0;) order.push_back(k);
     return order;
   };
-  // stage 1: group size, default kernels
-  const std::vector<int> sizes = {32, 48, 64, 80, 96};
+  // stage 1: group size and lanes, default kernels
+  std::vector<std::pair<int, int>> sizes;  // (MiB, lanes)
+  for (int lanes : {1, 2})
+    for (int mb : {32, 48, 64, 80, 96}) sizes.push_back({mb, lanes});
   std::vector<double> size_us(sizes.size(), -1.0);
   bool warmed = false;
   for (size_t k : two_rounds(sizes.size())) {
-    int rc = batch_configure(b, (size_t)sizes[k] << 20, {});
+    b->lanes = sizes[k].second;
+    int rc = batch_configure(b, (size_t)sizes[k].first << 20, {});
     double us = 0.0;
     if (!rc) rc = batch_time_sweep(b, 0, (int)b->groups.size(), &us, warmed ? 0.0 : 50.0);
     warmed = true;
@@ -883,12 +932,15 @@ static int batch_tune(u1_batch *b) {
     if (size_us[k] < 0.0 || us < size_us[k]) size_us[k] = us;
   }
   size_t best_bytes = b->group_bytes;
+  int best_lanes = b->lanes;
   double best_us = -1.0;
   for (size_t k = 0; k < sizes.size(); ++k)
     if (best_us < 0.0 || size_us[k] < best_us) {
       best_us = size_us[k];
-      best_bytes = (size_t)sizes[k] << 20;
+      best_bytes = (size_t)sizes[k].first << 20;
+      best_lanes = sizes[k].second;
     }
+  b->lanes = best_lanes;
   // stage 2: per group, kernel and threads per block
   int rc = batch_configure(b, best_bytes, {});
   if (rc) return rc;
@@ -927,7 +979,7 @@ static int batch_tune(u1_batch *b) {
   }
   u1i::dev_free(b->backup);
   b->backup = nullptr;
-  BatchTuneRec rec{b->group_bytes, current_choice(b)};
+  BatchTuneRec rec{b->group_bytes, current_choice(b), b->lanes};
   std::lock_guard<std::mutex> lock(g_btune_mu);
   g_btune[key] = rec;
   batch_tune_save(key, rec, tuned_us);
@@ -938,8 +990,10 @@ extern "C" int u1_batch_tune(u1_batch *b, int *group_mb) {
   u1i::NvtxRange nvtx_range("u1_batch_tune");
   if (!b) return bfail(U1_ERR_INVALID, "u1_batch_tune: null batch");
   U1_CUDA_TRY(cudaSetDevice(b->ctx->device));
+  const int lanes0 = b->lanes;
   int rc = batch_tune(b);
   if (rc) {
+    b->lanes = lanes0;
     if (b->backup) {  // a failed trial: put the links and pass counter back
       cudaMemcpyAsync(b->links, b->backup, b->total_links * sizeof(float2), cudaMemcpyDeviceToDevice, b->stream);
       const unsigned long long pass0 = b->pass;
@@ -962,6 +1016,23 @@ extern "C" int u1_batch_configure(u1_batch *b, int group_mb, int ngroups, const 
   for (int k = 0; k < ngroups; ++k) choice.push_back({variants[k], threads[k]});
   const size_t bytes = group_mb > 0 ? (size_t)group_mb << 20 : b->group_bytes;
   return batch_configure(b, bytes, choice);
+}
+
+extern "C" int u1_batch_set_lanes(u1_batch *b, int lanes) {
+  if (!b || (lanes != 1 && lanes != 2)) return bfail(U1_ERR_INVALID, "u1_batch_set_lanes: lanes must be 1 or 2");
+  U1_CUDA_TRY(cudaSetDevice(b->ctx->device));
+  if (lanes == b->lanes) return U1_OK;
+  U1_CUDA_TRY(cudaStreamSynchronize(b->stream));
+  for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);  // captured with the other lane count
+  b->graphs.clear();
+  b->lanes = lanes;
+  return U1_OK;
+}
+
+extern "C" int u1_batch_get_lanes(const u1_batch *b, int *lanes) {
+  if (!b || !lanes) return bfail(U1_ERR_INVALID, "u1_batch_get_lanes: null argument");
+  *lanes = b->lanes;
+  return U1_OK;
 }
 
 extern "C" int u1_batch_group_info(const u1_batch *b, int group, int out[4]) {

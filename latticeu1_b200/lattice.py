@@ -437,6 +437,16 @@ class Batch:
     def set_stream(self, stream_ptr: int | None) -> None:
         check(lib.u1_batch_set_stream(self._h, C.c_void_p(stream_ptr or 0)), "u1_batch_set_stream")
 
+    @property
+    def lanes(self) -> int:
+        """Streams a sweep spreads its chain groups over (1 or 2)."""
+        v = C.c_int()
+        check(lib.u1_batch_get_lanes(self._h, C.byref(v)), "u1_batch_get_lanes")
+        return int(v.value)
+
+    def set_lanes(self, lanes: int) -> None:
+        check(lib.u1_batch_set_lanes(self._h, int(lanes)), "u1_batch_set_lanes")
+
     VARIANTS = {5: "quad", 1: "pair32", 3: "single"}
 
     def tune(self) -> int:

@@ -138,7 +138,7 @@ def test_auto_variant_tunes_on_first_update(ctx, monkeypatch, tmp_path):
 
 
 BATCH_SETS = {
-    "4d-groups": [(4, (24, 24, 24, 24), 0.9 + 0.05 * k) for k in range(8)],  # 85 MB of links: two groups
+    "4d-groups": [(4, (24, 24, 24, 24), 0.9 + 0.05 * k) for k in range(8)],  # 85 MB: three groups, two lanes
     "4d-mixed": [(4, (8, 8, 8, 8), 1.0), (4, (12, 8, 4, 8), 0.85, 1.2), (4, (8, 4, 4, 16), 1.15)],
     "4d-odd-row": [(4, (6, 6, 4, 4), 1.0), (4, (8, 8, 8, 8), 0.9)],
     "3d": [(3, (8, 8, 0, 8), 1.2), (3, (16, 12, 0, 8), 1.6, 0.9)],
@@ -152,7 +152,7 @@ def test_batch_matches_single_lattices(ctx, name):
     seed, first = 2024, 17
     b = Batch(ctx, geoms, seed=seed, first_chain=first)
     if name == "4d-groups":
-        assert b.groups == 2
+        assert b.groups == 3 and b.lanes == 2
     b.hot_start()
     plan = ((1, 4, False), (2, 0, False), (1, 2, True))
     for m, o, meas in plan:
@@ -264,8 +264,10 @@ TUNE_SET = ([(4, (16, 16, 16, 16), 0.9 + 0.02 * k) for k in range(4)] + [(4, (12
             [(4, (6, 6, 6, 6), 1.1)] * 3)
 
 
-def _batch_run(ctx, layout=None, tune=False):
+def _batch_run(ctx, layout=None, tune=False, lanes=None):
     b = Batch(ctx, TUNE_SET, seed=77, first_chain=3)
+    if lanes is not None:
+        b.set_lanes(lanes)
     if layout is not None:
         b.configure(*layout)
     if tune:
@@ -277,9 +279,9 @@ def _batch_run(ctx, layout=None, tune=False):
 
 
 def test_batch_layouts_bit_identical(ctx):
-    """Every chain-group size and per-group kernel / block size gives the
-    same links and measurements bit for bit; choices a group's chains do not
-    allow fall back to the default."""
+    """Every chain-group size, per-group kernel / block size and lane count
+    gives the same links and measurements bit for bit; choices a group's
+    chains do not allow fall back to the default."""
     base, th0, m0 = _batch_run(ctx)
     assert [g[2] for g in base.layout()] == [3]  # one group holding 6^4 chains: one site per thread
     layouts = [(4, ()),  # 4 MiB groups, default kernels
@@ -288,8 +290,9 @@ def test_batch_layouts_bit_identical(ctx):
                # 2 MiB: the last group mixes 12^3x8 and 6^4 chains, which refuse (5, 128)
                (2, ((5, 128), (1, 64), (3, 256), (5, 64), (5, 128))),
                (64, ((3, 128),))]
-    for layout in layouts:
-        b, th, m = _batch_run(ctx, layout)
+    for layout, lanes in [(lay, ln) for lay in layouts for ln in (1, 2)]:
+        b, th, m = _batch_run(ctx, layout, lanes=lanes)
+        assert b.lanes == lanes
         lay = b.layout()
         if layout[0] == 1:
             assert [(g[2], g[3]) for g in lay] == list(layout[1])
@@ -301,13 +304,14 @@ def test_batch_layouts_bit_identical(ctx):
             for c in range(c0, c1):
                 h = TUNE_SET[c][1][0] // 2
                 assert (v != 5 or h % 4 == 0) and (v != 1 or h % 2 == 0)
-        assert np.array_equal(th, th0), layout
-        assert np.array_equal(m, m0, equal_nan=True), layout
+        assert np.array_equal(th, th0), (layout, lanes)
+        assert np.array_equal(m, m0, equal_nan=True), (layout, lanes)
+        assert b.pass_count() == base.pass_count(), (layout, lanes)
 
 
 def test_batch_tune_and_cache(ctx, monkeypatch, tmp_path):
-    """u1_batch_tune picks a group size and a per-group kernel / block size,
-    keeps the Markov chains bit for bit, and caches the result in
+    """u1_batch_tune picks a group size, a lane count and a per-group kernel /
+    block size, keeps the Markov chains bit for bit, and caches the result in
     $U1_RESOURCE_PATH; a second batch of the same extents applies it."""
     monkeypatch.setenv("U1_RESOURCE_PATH", str(tmp_path))
     _, th0, m0 = _batch_run(ctx)
@@ -319,9 +323,11 @@ def test_batch_tune_and_cache(ctx, monkeypatch, tmp_path):
     rows = [r.split("\t") for r in f.read_text().splitlines() if r and not r.startswith("#")]
     assert len(rows) == 1 and int(rows[0][1]) in (32, 48, 64, 80, 96)
     assert rows[0][2] == ",".join(f"{v}:{t}" for _, _, v, t in lay)
+    assert int(rows[0][4]) == b.lanes in (1, 2)
     b2 = Batch(ctx, TUNE_SET, seed=5)
+    b2.set_lanes(3 - b.lanes)
     assert b2.tune() == int(rows[0][1])
-    assert b2.layout() == lay
+    assert b2.layout() == lay and b2.lanes == b.lanes
     assert len([r for r in f.read_text().splitlines() if r]) == 1  # applied from the cache, not re-tuned
 
 

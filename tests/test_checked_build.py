@@ -12,7 +12,8 @@ phase-dependency check.
   passes; an odd extent, which u1_geom_validate refuses, is shown to break
   the decomposition.
 * checked build (GPU, child process with U1_CHECKED=1): every update
-  variant, the batched kernels, the measuring phases, windowed Metropolis,
+  variant, the batched kernels (two lanes of chain groups), the measuring
+  phases, windowed Metropolis,
   multilevel sub-updates and full-size four-site phases (32^4 in one wave,
   40^4 in several) run with bounds, alignment and race checks on
   every link access; no violation and no race may occur, the phase count
@@ -46,7 +47,7 @@ GEOMS = [
     (2, (16, 0, 0, 12), 2.0, 1.0),
 ]
 BATCH = [(4, (8, 8, 8, 8), 1.0, 1.0), (4, (16, 4, 4, 4), 1.1, 1.0), (4, (6, 4, 4, 8), 0.9, 1.2),
-         (4, (4, 2, 2, 6), 1.0, 2.0)]
+         (4, (4, 2, 2, 6), 1.0, 2.0)] + [(4, (16, 16, 16, 16), 0.95, 1.0)] * 3  # 2 MiB groups: 4 groups, 2 lanes
 SWEEPS = ((1, 4), (2, 0), (0, 3))
 
 
@@ -227,6 +228,8 @@ def run_workload(out: Path) -> dict:
         report["multilevel"] = _lib.check_report(ctx.handle, reset=True)
     # batched chains (four-, two- and one-site groups)
     b = Batch(ctx, BATCH, seed=21)
+    b.configure(2)
+    assert b.groups >= 3 and b.lanes == 2
     b.hot_start()
     b.update(1, 4, measure=True)
     b.update(0, 2)
