@@ -307,6 +307,9 @@ def test_batch_layouts_bit_identical(ctx):
         assert np.array_equal(th, th0), (layout, lanes)
         assert np.array_equal(m, m0, equal_nan=True), (layout, lanes)
         assert b.pass_count() == base.pass_count(), (layout, lanes)
+    for bad in (0, 3):
+        with pytest.raises(U1Error):
+            base.set_lanes(bad)
 
 
 def test_batch_tune_and_cache(ctx, monkeypatch, tmp_path):
