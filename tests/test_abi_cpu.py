@@ -94,3 +94,23 @@ def test_null_arguments_return_invalid():
     assert _lib.lib.u1_update(None, None, 1, 4) == _lib.U1_ERR_INVALID
     assert _lib.lib.u1_measure(None, None) == _lib.U1_ERR_INVALID
     assert _lib.lib.u1_multilevel(None, None, 1, 1, 1, 1, 1, 1, None, 0) == _lib.U1_ERR_INVALID
+
+
+def test_integration_example_compiles(tmp_path):
+    """The C ABI example of INTEGRATION.md compiles against include/u1_b200.h
+    (g++ -fsyntax-only; no device needed)."""
+    import shutil
+    import subprocess
+    root = Path(__file__).resolve().parents[1]
+    text = (root / "INTEGRATION.md").read_text()
+    m = re.search(r"```c\+\+\n(.*?)```", text, re.S)
+    assert m, "no C++ example in INTEGRATION.md"
+    body = m.group(1).replace('#include "u1_b200.h"', "")
+    src = tmp_path / "example.cpp"
+    src.write_text('#include "u1_b200.h"\nint main() {\n' + body + "return 0;\n}\n")
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("g++ not found")
+    r = subprocess.run([gxx, "-std=c++17", "-fsyntax-only", "-Wall", "-I" + str(root / "include"), str(src)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
