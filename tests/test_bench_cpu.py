@@ -53,3 +53,23 @@ def test_traffic_figures_follow_the_profiled_kernel(tmp_path):
     per_link, note = b.ncu_batch_traffic_per_link_sweep(32, 2)
     assert per_link is None and "64 MiB" in note
     assert b.KERNEL_OF_VARIANT[5] == "k_update_quad" and b.KERNEL_OF_VARIANT[1] == "k_update_pair"
+
+
+def test_reference_arm_line():
+    """`bench.py --impl reference` (the reference's own FP64 CPU code when
+    oracle/_ref is built, else the oracle port) prints one JSON line with
+    the contract's keys, on the host only."""
+    import json
+    import subprocess
+    import sys
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--L", "8", "--steps", "2",
+                        "--warmup", "3"], cwd=str(ROOT), capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1])
+    for key in ("impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+                "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert key in line, key
+    assert line["impl"] == "reference" and line["value"] > 0 and line["steps"] == 2
+    assert line["cpu_baseline"]["kind"] in ("reference", "port") and line["cpu_baseline"]["value"] == line["value"]
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+    assert "8^4" in line["metric"]
