@@ -48,10 +48,10 @@ def test_traffic_figures_follow_the_profiled_kernel(tmp_path):
     f.write_text("kernel: k_update_quad\nsource_digest: 0000000000000000\ndram_bytes_per_launch: 12345\n")
     value, note = b.ncu_traffic_per_launch((32, 32, 32, 32), "k_update_quad", tmp_path)
     assert value is None and "stale" in note
-    per_link, note = b.ncu_batch_traffic_per_link_sweep(64, 1)  # the layout the summary was made with
+    per_link, note = b.ncu_batch_traffic_per_link_sweep(32, 2)  # the layout the summary was made with
     assert per_link is not None and 0 < per_link < 72 * 5, note
-    per_link, note = b.ncu_batch_traffic_per_link_sweep(32, 2)
-    assert per_link is None and "64 MiB" in note
+    per_link, note = b.ncu_batch_traffic_per_link_sweep(64, 1)
+    assert per_link is None and "32 MiB" in note
     assert b.KERNEL_OF_VARIANT[5] == "k_update_quad" and b.KERNEL_OF_VARIANT[1] == "k_update_pair"
 
 
